@@ -1,0 +1,156 @@
+/* ybgpu: B200-native factor-once / solve-many sparse triangular solves.
+ *
+ * C ABI of libybgpu.so. It mirrors the public API of ybus's `ybus_cuda` crate
+ * (ybus_cuda/src/lib.rs:73-75 re-exports `Gpu`, `GpuFactor`, `Timings`, `Pair`, `PairUpdate`,
+ * `ColumnMax`, `GpuBlock`, `GpuOperator`) one entry point per method, in the conventions of
+ * ybus's own C ABI (`ybus_ffi`): an int32 status per call (0 = success), a thread-local message
+ * for the last failure, and opaque handles made by `_new` and released by `_free`
+ * (ybus_ffi/src/lib.rs:44-73, ybus_ffi/src/status.rs:10-60).
+ *
+ * Contract violations that ybus_cuda answers with a panic (`assert!`) are reported here as
+ * YB_ERROR_INVALID_ARGUMENT instead; nothing in this library aborts the caller.
+ *
+ * Arrays of right-hand sides and solutions are column-major: column k of an n-row array starts
+ * at element k*n. Indices are int64 at the boundary and must fit 32 bits on the device
+ * (YB_ERROR_TOO_LARGE otherwise, as ybus_cuda's `CudaError::TooLarge`, ybus_cuda/src/lib.rs:98).
+ * A row index of -1 means "none" wherever ybus_cuda takes an `Option<usize>`.
+ */
+#ifndef YBGPU_H
+#define YBGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (ybus_cuda's `CudaError` variants, ybus_cuda/src/lib.rs:89-124) ---------- */
+#define YB_OK 0
+#define YB_ERROR_INVALID_ARGUMENT 1 /* a contract violation (ybus_cuda panics) */
+#define YB_ERROR_SHAPE_MISMATCH 2   /* CudaError::ShapeMismatch */
+#define YB_ERROR_TOO_LARGE 3        /* CudaError::TooLarge */
+#define YB_ERROR_NOT_POSITIVE_DEFINITE 4
+#define YB_ERROR_SINGULAR 5
+#define YB_NO_DEVICE 6              /* Gpu::new() -> Ok(None) */
+#define YB_ERROR_CUDA 7             /* CudaError::Driver */
+#define YB_ERROR_NOT_SYMMETRIC 8
+#define YB_ERROR_DEVICE_TIMEOUT 9   /* a bounded device wait gave up */
+#define YB_ERROR_INTERNAL 10
+
+#define YB_CHOLESKY 1
+#define YB_LU 2
+
+#define YB_ORDER_NATURAL 0
+#define YB_ORDER_AMD 1
+#define YB_ORDER_COLAMD 3
+
+/* The message of the calling thread's last failure, NUL-terminated and truncated to `length`;
+ * returns the length needed including the NUL. */
+int32_t yb_last_error_message(char *buffer, size_t length);
+
+/* ---- host factor producer (the ybus_sparse calls whose results ybus_cuda uploads) --------- */
+typedef struct yb_matrix yb_matrix;
+typedef struct yb_host_factor yb_host_factor;
+
+/* A compressed matrix from triplets, duplicates summed in input order
+ * (ybus_sparse/src/compressed_matrix.rs:254-330). `by_rows` = 1 for CSR, 0 for CSC. Complex
+ * values are interleaved (re, im), 2*count doubles. */
+int32_t yb_matrix_from_triplets(int64_t rows, int64_t cols, int64_t count, const int64_t *row_idx,
+                                const int64_t *col_idx, const double *values, int32_t by_rows,
+                                int32_t is_complex, yb_matrix **out);
+/* Rows and columns in the given orders (ybus_sparse/src/compressed_matrix/access.rs:175-216). */
+int32_t yb_matrix_select(const yb_matrix *m, int64_t n_rows, const int64_t *rows, int64_t n_cols,
+                         const int64_t *cols, yb_matrix **out);
+/* The other orientation of the same matrix (to_csc / to_csr). */
+int32_t yb_matrix_reorient(const yb_matrix *m, yb_matrix **out);
+int32_t yb_matrix_info(const yb_matrix *m, int64_t *rows, int64_t *cols, int64_t *stored,
+                       int32_t *by_rows, int32_t *is_complex);
+int32_t yb_matrix_export(const yb_matrix *m, int64_t *ptr, int64_t *idx, double *values);
+void yb_matrix_free(yb_matrix *m);
+/* A fill-reducing ordering (ybus_sparse/src/compressed_matrix/ordering.rs:46-64). */
+int32_t yb_ordering(const yb_matrix *m, int32_t ordering, int64_t *perm);
+
+/* `CsrMatrix::analyze_cholesky(ordering)` then `factor` (cholesky.rs:50-311): P A Pᵀ = L Lᵀ. */
+int32_t yb_host_cholesky(const yb_matrix *csr, int32_t ordering, yb_host_factor **out);
+/* `CscMatrix::analyze_lu(ordering)` then `factor` with the pivot threshold (lu.rs:142-247). */
+int32_t yb_host_lu(const yb_matrix *csc, int32_t ordering, double pivot_threshold, yb_host_factor **out);
+int32_t yb_host_factor_info(const yb_host_factor *f, int32_t *kind, int32_t *is_complex, int64_t *n,
+                            int64_t *lower_stored, int64_t *upper_stored);
+/* Cholesky: lower = L (CSR, diagonal last), upper = Lᵀ (CSR, diagonal first), both perms = P.
+ * LU: lower = L (CSC, unit diagonal first), upper = U (CSC, diagonal last), row_perm = P,
+ * col_perm = Q. Any output may be NULL. */
+int32_t yb_host_factor_export(const yb_host_factor *f, int64_t *lower_ptr, int64_t *lower_idx,
+                              double *lower_val, int64_t *upper_ptr, int64_t *upper_idx,
+                              double *upper_val, int64_t *row_perm, int64_t *col_perm);
+int32_t yb_host_etree(const yb_host_factor *f, int64_t *parent);
+void yb_host_factor_free(yb_host_factor *f);
+
+
+/* ---- the GPU (ybus_cuda `Gpu`, ybus_cuda/src/lib.rs:168-219) ----------------------------- */
+typedef struct yb_gpu yb_gpu;
+typedef struct yb_factor yb_factor;
+
+#define YB_FP64 0 /* substitutions in double */
+#define YB_FP32 1 /* substitutions in float (no refinement) */
+
+/* `Gpu::new()`: device `device`, or YB_NO_DEVICE where there is none (ybus returns Ok(None)). */
+int32_t yb_gpu_new(int32_t device, yb_gpu **out);
+void yb_gpu_free(yb_gpu *gpu);
+/* `Gpu::name()` (lib.rs:210-212). */
+int32_t yb_gpu_name(const yb_gpu *gpu, char *buffer, size_t length);
+/* `Gpu::memory()`: free and total device memory in bytes (lib.rs:214-218). */
+int32_t yb_gpu_memory(const yb_gpu *gpu, uint64_t *free_bytes, uint64_t *total_bytes);
+/* No ybus counterpart: SM count, compute capability and L2 size, for sizing launches. */
+int32_t yb_gpu_properties(const yb_gpu *gpu, int32_t *sm_count, int32_t *major, int32_t *minor, int64_t *l2_bytes);
+/* The stream the host-array calls of this GPU run on (a cudaStream_t). */
+void *yb_gpu_stream(const yb_gpu *gpu);
+/* Waits for `stream` (NULL for the GPU's own) to finish; reports any asynchronous CUDA error. */
+int32_t yb_gpu_synchronize(const yb_gpu *gpu, void *stream);
+
+/* ---- an uploaded factorization (ybus_cuda `GpuFactor`, ybus_cuda/src/factor.rs) ------------ */
+/* `GpuFactor::from_cholesky` (factor.rs:103-119): P A Pᵀ = L Lᵀ with L in CSR, each row's
+ * diagonal last, and perm = P (row i of P A Pᵀ is row perm[i] of A). */
+int32_t yb_factor_from_cholesky(yb_gpu *gpu, int64_t n, const int64_t *l_ptr, const int64_t *l_idx,
+                                const double *l_val, const int64_t *perm, yb_factor **out);
+/* `GpuFactor::from_lu` (factor.rs:123-133): P A Q = L U with L unit lower in CSC (diagonal
+ * first), U upper in CSC (diagonal last), row_perm = P, col_perm = Q. */
+int32_t yb_factor_from_lu(yb_gpu *gpu, int64_t n, const int64_t *l_ptr, const int64_t *l_idx,
+                          const double *l_val, const int64_t *u_ptr, const int64_t *u_idx,
+                          const double *u_val, const int64_t *row_perm, const int64_t *col_perm,
+                          yb_factor **out);
+void yb_factor_free(yb_factor *f);
+/* `GpuFactor::dim` and `block_width` (factor.rs:181-190); -1 for a null factor. */
+int64_t yb_factor_dim(const yb_factor *f);
+int64_t yb_factor_block_width(const yb_factor *f);
+/* `GpuFactor::set_block_width` (factor.rs:192-201): at least 1, at most 64 for one row. */
+int32_t yb_factor_set_block_width(yb_factor *f, int64_t width);
+/* `GpuFactor::timings` / `reset_timings` (factor.rs:203-210), in seconds. */
+int32_t yb_factor_timings(const yb_factor *f, double *upload_s, double *solve_s, double *download_s,
+                          int64_t *blocks);
+int32_t yb_factor_reset_timings(yb_factor *f);
+/* No ybus counterpart (cuSPARSE's analysis is opaque there): the level schedule's shape. */
+int32_t yb_factor_plan_info(const yb_factor *f, int32_t *fwd_levels, int32_t *bwd_levels,
+                            int64_t *fwd_entries, int64_t *bwd_entries, int32_t *fwd_widest,
+                            int32_t *bwd_widest);
+/* No ybus counterpart: the tile solve's launch shape for a precision (tile width 1..32, a power
+ * of two; threads a multiple of 32 up to 512; resident blocks per SM 1..8). */
+int32_t yb_factor_set_tile(yb_factor *f, int32_t precision, int32_t tile_width, int32_t threads,
+                           int32_t blocks_per_sm);
+int32_t yb_factor_get_tile(const yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *threads,
+                           int32_t *blocks_per_sm);
+
+/* `GpuFactor::solve_many` (factor.rs:234-289) with host arrays: `count` right-hand sides,
+ * column-major n x count in the caller's order, solutions likewise, in FP64. Pinned (page-locked)
+ * caller memory is copied directly; pageable memory goes through a pinned staging buffer. */
+int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count, double *out);
+/* The same solve on device arrays (leading dimensions ldb, ldx >= n) on `stream` (a
+ * cudaStream_t, NULL for the GPU's own), asynchronous, in YB_FP64 or YB_FP32 substitution. */
+int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
+                             int64_t count, int32_t precision, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YBGPU_H */

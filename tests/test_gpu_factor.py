@@ -1,0 +1,171 @@
+"""GPU solves against the oracle's CPU solves (ybus_cuda/tests/gpu_factor_test.rs): SPD (Cholesky)
+and unsymmetric (LU with pivoting) factors, 2x2 blocks, a single row, block widths narrower and
+wider than the number of right-hand sides, every tile width, repeated runs bit for bit, and the
+full 10,000-bus PTDF block. All calls go through the C ABI."""
+import numpy as np
+import pytest
+
+import oracle.oracle as orc
+from fixtures import random_spd, random_square, right_hand_sides, two_by_two_blocks, worst_relative_difference
+from ybus_b200 import FP32, FP64, GpuFactor, ShapeMismatch, grids, host
+
+pytestmark = pytest.mark.gpu
+
+# The GPU's solutions agree with the CPU's to within rounding (gpu_factor_test.rs:16)
+BAR = 1e-12
+
+
+def upload(gpu, f):
+    return GpuFactor.from_cholesky(gpu, f) if isinstance(f, host.HostCholesky) else GpuFactor.from_lu(gpu, f)
+
+
+def test_cholesky_solves_match_the_cpu_at_every_block_width(gpu):
+    chol = host.cholesky(random_spd(300, 3, 7))
+    rhs = right_hand_sides(300, 37, 11)
+    cpu = orc.solve_many(chol, rhs)
+    factor = upload(gpu, chol)
+    for width in [1, 5, 37, 64, 1024, 4096]:
+        factor.set_block_width(width)
+        solved = factor.solve_many(rhs)
+        d = worst_relative_difference(solved, cpu)
+        assert d < BAR, f"width {width}: {d:e}"
+
+
+@pytest.mark.parametrize("tile", [1, 2, 4, 8, 16, 32])
+@pytest.mark.parametrize("threads", [64, 256, 512])
+def test_every_tile_width_and_block_size(gpu, tile, threads):
+    chol = host.cholesky(random_spd(300, 3, 7))
+    rhs = right_hand_sides(300, 37, 11)
+    cpu = orc.solve_many(chol, rhs)
+    factor = upload(gpu, chol)
+    factor.set_tile(FP64, tile, threads, 2)
+    d = worst_relative_difference(factor.solve_many(rhs), cpu)
+    assert d < BAR, f"tile {tile} threads {threads}: {d:e}"
+
+
+def test_lu_solves_match_the_cpu_with_pivoting(gpu):
+    lu = host.lu(random_square(250, 4, 3))
+    assert any(i != p for i, p in enumerate(lu.row_perm)), "the fixture should pivot off the diagonal"
+    rhs = right_hand_sides(250, 20, 5)
+    cpu = orc.solve_many(lu, rhs)
+    factor = upload(gpu, lu)
+    factor.set_block_width(8)
+    d = worst_relative_difference(factor.solve_many(rhs), cpu)
+    assert d < BAR, f"{d:e}"
+
+
+def test_two_by_two_blocks_and_a_single_row(gpu):
+    lu = host.lu(two_by_two_blocks(40))
+    rhs = right_hand_sides(80, 3, 1)
+    factor = upload(gpu, lu)
+    d = worst_relative_difference(factor.solve_many(rhs), orc.solve_many(lu, rhs))
+    assert d < BAR, f"{d:e}"
+    # A single row, bit for bit, at block widths on both sides of 64
+    one = host.lu(host.Matrix.from_triplets(1, 1, [0], [0], [3.0], by_rows=False))
+    rhs = np.array([[j - 70.5] for j in range(200)])
+    factor = upload(gpu, one)
+    for width in [1, 64, 65, 1024]:
+        factor.set_block_width(width)
+        assert factor.block_width() == min(width, 64)
+        assert np.array_equal(factor.solve_many(rhs), orc.solve_many(one, rhs))
+
+
+def test_repeated_solves_give_the_same_bits(gpu):
+    chol = host.cholesky(random_spd(500, 2, 13))
+    rhs = right_hand_sides(500, 50, 17)
+    factor = upload(gpu, chol)
+    factor.set_block_width(16)
+    first = factor.solve_many(rhs)
+    factor.set_block_width(7)
+    factor.set_block_width(16)
+    for _ in range(3):
+        again = factor.solve_many(rhs)
+        assert np.array_equal(again.view(np.uint64), first.view(np.uint64))
+
+
+def test_empty_and_mismatched_right_hand_sides(gpu):
+    chol = host.cholesky(random_spd(10, 20, 1))
+    factor = upload(gpu, chol)
+    assert factor.solve_many([]).shape[0] == 0
+    with pytest.raises(ShapeMismatch) as e:
+        factor.solve_many([np.zeros(10), np.zeros(9)])
+    assert (e.value.expected, e.value.found) == (10, 9)
+    assert factor.timings().blocks == 0
+    factor.solve_many([np.ones(10)])
+    assert factor.timings().blocks == 1
+    factor.reset_timings()
+    assert factor.timings().blocks == 0
+
+
+def test_device_api_on_torch_memory_and_stream(gpu):
+    import torch
+    chol = host.cholesky(random_spd(300, 3, 7))
+    rhs = right_hand_sides(300, 40, 11)
+    cpu = orc.solve_many(chol, rhs)
+    factor = upload(gpu, chol)
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream().cuda_stream
+    factor.solve_many_device(b.data_ptr(), x.data_ptr(), 40, FP64, stream)
+    torch.cuda.current_stream().synchronize()
+    assert worst_relative_difference(x.cpu().numpy(), cpu) < BAR
+    # and on the library's own stream
+    x.zero_()
+    torch.cuda.synchronize()
+    factor.solve_many_device(b.data_ptr(), x.data_ptr(), 40, FP64, None)
+    gpu.synchronize()
+    assert worst_relative_difference(x.cpu().numpy(), cpu) < BAR
+
+
+def test_fp32_substitution_is_close(gpu):
+    import torch
+    chol = host.cholesky(random_spd(300, 3, 7))
+    rhs = right_hand_sides(300, 40, 11)
+    cpu = orc.solve_many(chol, rhs)
+    factor = upload(gpu, chol)
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    torch.cuda.synchronize()
+    for tile in [4, 8, 16, 32]:
+        factor.set_tile(FP32, tile, 512, 1)
+        factor.solve_many_device(b.data_ptr(), x.data_ptr(), 40, FP32, None)
+        gpu.synchronize()
+        d = worst_relative_difference(x.cpu().numpy(), cpu)
+        assert d < 1e-4, f"tile {tile}: {d:e}"
+
+
+def _ptdf_case(n_bus, extra, seed):
+    g = grids.make_grid(n_bus, extra, seed)
+    r, c, v = grids.bbus_triplets(g)
+    bbus = host.Matrix.from_triplets(n_bus, n_bus, r, c, v)
+    keep = np.arange(1, n_bus)
+    bp = bbus.select(keep, keep)
+    chol = host.cholesky(bp)
+    # RHS_k = b_k (e_f - e_t) over the non-slack buses
+    rhs = np.zeros((g.n_branch, n_bus))
+    k = np.arange(g.n_branch)
+    rhs[k, g.frm] += g.susceptance
+    rhs[k, g.to] -= g.susceptance
+    return g, bp, chol, np.ascontiguousarray(rhs[:, 1:])
+
+
+def test_full_ptdf_block_on_the_10k_grid(gpu):
+    import torch
+    g, bp, chol, rhs = _ptdf_case(10000, 3500, grids.SEED_BASE + 2)
+    assert rhs.shape == (13499, 9999)
+    factor = upload(gpu, chol)
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    torch.cuda.synchronize()
+    factor.solve_many_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], FP64, None)
+    gpu.synchronize()
+    xs = x.cpu().numpy()
+    sample = np.random.default_rng(0).choice(rhs.shape[0], 96, replace=False)
+    cpu = orc.solve_many(chol, rhs[sample], threads=8)
+    d = worst_relative_difference(xs[sample], cpu)
+    assert d < BAR, f"{d:e}"
+    # every column: relative residual at FP64 rounding level
+    p, i, v = bp.arrays()
+    worst = max(orc.relative_residual(p, i, v, xs[k], rhs[k]) for k in range(0, rhs.shape[0], 7))
+    assert worst < 1e-11, worst

@@ -1,0 +1,119 @@
+"""ctypes binding of libybgpu.so (the C ABI declared in include/ybgpu.h).
+
+The library is loaded from this package's directory. There is no fallback: if it is missing or
+fails to load, every call raises, so nothing silently runs on the CPU instead.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libybgpu.so"
+
+i32, i64, u64, dbl, vp = C.c_int32, C.c_int64, C.c_uint64, C.c_double, C.c_void_p
+P_i64 = C.POINTER(C.c_int64)
+P_i32 = C.POINTER(C.c_int32)
+P_dbl = C.POINTER(C.c_double)
+
+YB_OK = 0
+YB_ERROR_INVALID_ARGUMENT = 1
+YB_ERROR_SHAPE_MISMATCH = 2
+YB_ERROR_TOO_LARGE = 3
+YB_ERROR_NOT_POSITIVE_DEFINITE = 4
+YB_ERROR_SINGULAR = 5
+YB_NO_DEVICE = 6
+YB_ERROR_CUDA = 7
+YB_ERROR_NOT_SYMMETRIC = 8
+YB_ERROR_DEVICE_TIMEOUT = 9
+YB_ERROR_INTERNAL = 10
+YB_CHOLESKY = 1
+YB_LU = 2
+YB_ORDER_NATURAL = 0
+YB_ORDER_AMD = 1
+YB_ORDER_COLAMD = 3
+YB_FP64 = 0
+YB_FP32 = 1
+
+# name -> (restype, argtypes)
+SIGNATURES: dict[str, tuple] = {
+    "yb_last_error_message": (i32, [C.c_char_p, C.c_size_t]),
+    "yb_matrix_from_triplets": (i32, [i64, i64, i64, vp, vp, vp, i32, i32, C.POINTER(vp)]),
+    "yb_matrix_select": (i32, [vp, i64, vp, i64, vp, C.POINTER(vp)]),
+    "yb_matrix_reorient": (i32, [vp, C.POINTER(vp)]),
+    "yb_matrix_info": (i32, [vp, P_i64, P_i64, P_i64, P_i32, P_i32]),
+    "yb_matrix_export": (i32, [vp, vp, vp, vp]),
+    "yb_matrix_free": (None, [vp]),
+    "yb_ordering": (i32, [vp, i32, vp]),
+    "yb_host_cholesky": (i32, [vp, i32, C.POINTER(vp)]),
+    "yb_host_lu": (i32, [vp, i32, dbl, C.POINTER(vp)]),
+    "yb_host_factor_info": (i32, [vp, P_i32, P_i32, P_i64, P_i64, P_i64]),
+    "yb_host_factor_export": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "yb_host_etree": (i32, [vp, vp]),
+    "yb_host_factor_free": (None, [vp]),
+    "yb_gpu_new": (i32, [i32, C.POINTER(vp)]),
+    "yb_gpu_free": (None, [vp]),
+    "yb_gpu_name": (i32, [vp, C.c_char_p, C.c_size_t]),
+    "yb_gpu_memory": (i32, [vp, C.POINTER(u64), C.POINTER(u64)]),
+    "yb_gpu_properties": (i32, [vp, P_i32, P_i32, P_i32, P_i64]),
+    "yb_gpu_stream": (vp, [vp]),
+    "yb_gpu_synchronize": (i32, [vp, vp]),
+    "yb_factor_from_cholesky": (i32, [vp, i64, vp, vp, vp, vp, C.POINTER(vp)]),
+    "yb_factor_from_lu": (i32, [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]),
+    "yb_factor_free": (None, [vp]),
+    "yb_factor_dim": (i64, [vp]),
+    "yb_factor_block_width": (i64, [vp]),
+    "yb_factor_set_block_width": (i32, [vp, i64]),
+    "yb_factor_timings": (i32, [vp, P_dbl, P_dbl, P_dbl, P_i64]),
+    "yb_factor_reset_timings": (i32, [vp]),
+    "yb_factor_plan_info": (i32, [vp, P_i32, P_i32, P_i64, P_i64, P_i32, P_i32]),
+    "yb_factor_set_tile": (i32, [vp, i32, i32, i32, i32]),
+    "yb_factor_get_tile": (i32, [vp, i32, P_i32, P_i32, P_i32]),
+    "yb_solve_many": (i32, [vp, vp, i64, vp]),
+    "yb_solve_many_device": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
+}
+
+_lib: C.CDLL | None = None
+
+
+class YbError(RuntimeError):
+    """A failed libybgpu call: `status` is the YB_* code, the message the library's."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+        self.message = message
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is not built: run `python -c 'import __graft_entry__ as g; g.build()'`")
+        handle = C.CDLL(str(LIB_PATH), mode=os.RTLD_LOCAL)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().yb_last_error_message(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> int:
+    if status != YB_OK:
+        raise YbError(status, last_error())
+    return status
+
+
+def ptr(array) -> int | None:
+    """The data pointer of a numpy array (or None for None)."""
+    if array is None:
+        return None
+    return array.ctypes.data

@@ -1,0 +1,442 @@
+// C ABI of the GPU path: the device (`Gpu`), an uploaded factorization (`GpuFactor`) and its
+// block solves, mirroring ybus_cuda (ybus_cuda/src/lib.rs:168-219, ybus_cuda/src/factor.rs).
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "../../include/ybgpu.h"
+#include "capi_common.hpp"
+#include "device.cuh"
+#include "factor_state.cuh"
+#include "solve.cuh"
+
+using namespace yb;
+
+// ---------------------------------------------------------------------------------------------
+// Gpu
+// ---------------------------------------------------------------------------------------------
+
+extern "C" int32_t yb_gpu_new(int32_t device, yb_gpu **out) {
+  return guard([&] {
+    require(out != nullptr, "out is null");
+    *out = nullptr;
+    int count = 0;
+    const cudaError_t err = cudaGetDeviceCount(&count);
+    if (err == cudaErrorNoDevice || err == cudaErrorInsufficientDriver || count == 0) {
+      cudaGetLastError();
+      set_last_error("no CUDA device");
+      return YB_NO_DEVICE;
+    }
+    cuda_check(err, "cudaGetDeviceCount");
+    require(device >= 0 && device < count, "no such device");
+    auto g = std::make_unique<yb_gpu>();
+    g->device = device;
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    cudaDeviceProp prop{};
+    cuda_check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    g->name = prop.name;
+    g->sm_count = prop.multiProcessorCount;
+    g->major = prop.major;
+    g->minor = prop.minor;
+    g->l2_bytes = prop.l2CacheSize;
+    cuda_check(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    *out = g.release();
+    return YB_OK;
+  });
+}
+
+extern "C" void yb_gpu_free(yb_gpu *gpu) {
+  if (!gpu) return;
+  cudaSetDevice(gpu->device);
+  if (gpu->stream) cudaStreamDestroy(gpu->stream);
+  delete gpu;
+}
+
+extern "C" int32_t yb_gpu_name(const yb_gpu *gpu, char *buffer, size_t length) {
+  return guard([&] {
+    require(gpu && buffer && length, "null argument");
+    const size_t copy = std::min(length - 1, gpu->name.size());
+    std::memcpy(buffer, gpu->name.data(), copy);
+    buffer[copy] = '\0';
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_gpu_memory(const yb_gpu *gpu, uint64_t *free_bytes, uint64_t *total_bytes) {
+  return guard([&] {
+    require(gpu != nullptr, "null gpu");
+    cuda_check(cudaSetDevice(gpu->device), "cudaSetDevice");
+    size_t f = 0, t = 0;
+    cuda_check(cudaMemGetInfo(&f, &t), "cudaMemGetInfo");
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_gpu_properties(const yb_gpu *gpu, int32_t *sm_count, int32_t *major, int32_t *minor,
+                                     int64_t *l2_bytes) {
+  return guard([&] {
+    require(gpu != nullptr, "null gpu");
+    if (sm_count) *sm_count = gpu->sm_count;
+    if (major) *major = gpu->major;
+    if (minor) *minor = gpu->minor;
+    if (l2_bytes) *l2_bytes = gpu->l2_bytes;
+    return YB_OK;
+  });
+}
+
+extern "C" void *yb_gpu_stream(const yb_gpu *gpu) { return gpu ? (void *)gpu->stream : nullptr; }
+
+extern "C" int32_t yb_gpu_synchronize(const yb_gpu *gpu, void *stream) {
+  return guard([&] {
+    require(gpu != nullptr, "null gpu");
+    cuda_check(cudaSetDevice(gpu->device), "cudaSetDevice");
+    cuda_check(cudaStreamSynchronize(stream ? (cudaStream_t)stream : gpu->stream), "cudaStreamSynchronize");
+    return YB_OK;
+  });
+}
+
+// ---------------------------------------------------------------------------------------------
+// GpuFactor
+// ---------------------------------------------------------------------------------------------
+
+namespace {
+
+host::Compressed<double> csr_from_arrays(int64_t n, const int64_t *ptr, const int64_t *idx, const double *val,
+                                         bool by_rows) {
+  require(ptr != nullptr, "null pointer array");
+  host::Compressed<double> m;
+  m.rows = m.cols = n;
+  m.by_rows = by_rows;
+  m.ptr.assign(ptr, ptr + n + 1);
+  require(m.ptr[0] == 0, "pointers must start at 0");
+  for (int64_t i = 0; i < n; ++i) require(m.ptr[i + 1] >= m.ptr[i], "pointers must not decrease");
+  const int64_t nnz = m.ptr[n];
+  require(nnz == 0 || (idx && val), "null index or value array");
+  m.idx.assign(idx, idx + nnz);
+  m.val.assign(val, val + nnz);
+  for (int64_t v : m.idx) require(v >= 0 && v < n, "an index is out of range");
+  return m;
+}
+
+// The transpose of a square CSR matrix, in CSR form: its CSC arrays read by rows.
+host::Compressed<double> transpose_as_csr(const host::Compressed<double> &m) {
+  host::Compressed<double> t = host::reorient(m);
+  t.by_rows = true;
+  return t;
+}
+
+yb_factor *make_factor(yb_gpu *gpu, int64_t n, host::Compressed<double> lower, bool unit_lower,
+                       host::Compressed<double> upper, std::vector<int64_t> in_perm, std::vector<int64_t> out_perm,
+                       int kind) {
+  auto f = std::make_unique<yb_factor>();
+  f->gpu = gpu;
+  f->n = n;
+  f->kind = kind;
+  cuda_check(cudaSetDevice(gpu->device), "cudaSetDevice");
+  f->plan = build_plan<double>(n, lower, unit_lower, upper, in_perm, out_perm);
+  if (n == 1) {
+    // ybus_cuda solves a single-row factor on the host (ybus_cuda/src/factor.rs:244-248): the
+    // two triangles' diagonals, divided in the CPU's order
+    f->single = true;
+    f->single_lower = unit_lower ? 1.0 : lower.val[lower.ptr[1] - 1];
+    for (int64_t p = upper.ptr[0]; p < upper.ptr[1]; ++p)
+      if (upper.idx[p] == 0) f->single_upper = upper.val[p];
+  }
+  cudaStream_t s = gpu->stream;
+  f->in_slot.upload(f->plan.in_slot, s);
+  f->out_slot.upload(f->plan.out_slot, s);
+  upload_sweep(f->fwd64, f->plan.fwd, f->plan.n, s);
+  upload_sweep(f->bwd64, f->plan.bwd, f->plan.n, s);
+  upload_sweep(f->fwd32, f->plan.fwd, f->plan.n, s);
+  upload_sweep(f->bwd32, f->plan.bwd, f->plan.n, s);
+  cuda_check(cudaStreamSynchronize(s), "upload");
+  // Default block width as ybus_cuda chooses it: two n-column blocks of doubles per right-hand
+  // side in a quarter of the free memory (ybus_cuda/src/factor.rs:157-160), capped higher here
+  // because a block is one launch over all SMs rather than one SpSM call
+  size_t free_bytes = 0, total = 0;
+  cuda_check(cudaMemGetInfo(&free_bytes, &total), "cudaMemGetInfo");
+  const int64_t width = (int64_t)(free_bytes / 4 / (2 * 8 * (size_t)std::max<int64_t>(n, 1)));
+  f->width = std::max<int64_t>(1, std::min<int64_t>(width, kMaxDefaultWidth));
+  if (n == 1) f->width = std::min<int64_t>(f->width, kSingleRowWidth);
+  return f.release();
+}
+
+}  // namespace
+
+extern "C" int32_t yb_factor_from_cholesky(yb_gpu *gpu, int64_t n, const int64_t *l_ptr, const int64_t *l_idx,
+                                           const double *l_val, const int64_t *perm, yb_factor **out) {
+  return guard([&] {
+    require(gpu && out, "null argument");
+    require(n >= 0, "negative order");
+    require(n == 0 || perm, "null permutation");
+    auto lower = csr_from_arrays(n, l_ptr, l_idx, l_val, true);
+    auto upper = transpose_as_csr(lower);  // Lᵀ in CSR, each row's diagonal first
+    std::vector<int64_t> p(perm, perm + n);
+    *out = make_factor(gpu, n, std::move(lower), false, std::move(upper), p, p, YB_CHOLESKY);
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_from_lu(yb_gpu *gpu, int64_t n, const int64_t *l_ptr, const int64_t *l_idx,
+                                     const double *l_val, const int64_t *u_ptr, const int64_t *u_idx,
+                                     const double *u_val, const int64_t *row_perm, const int64_t *col_perm,
+                                     yb_factor **out) {
+  return guard([&] {
+    require(gpu && out, "null argument");
+    require(n >= 0, "negative order");
+    require(n == 0 || (row_perm && col_perm), "null permutation");
+    auto l_csc = csr_from_arrays(n, l_ptr, l_idx, l_val, false);
+    auto u_csc = csr_from_arrays(n, u_ptr, u_idx, u_val, false);
+    auto lower = host::reorient(l_csc);
+    auto upper = host::reorient(u_csc);
+    std::vector<int64_t> p(row_perm, row_perm + n), q(col_perm, col_perm + n);
+    *out = make_factor(gpu, n, std::move(lower), true, std::move(upper), p, q, YB_LU);
+    return YB_OK;
+  });
+}
+
+extern "C" void yb_factor_free(yb_factor *f) {
+  if (!f) return;
+  cudaSetDevice(f->gpu->device);
+  cudaStreamSynchronize(f->gpu->stream);
+  delete f;
+}
+
+extern "C" int64_t yb_factor_dim(const yb_factor *f) { return f ? f->n : -1; }
+extern "C" int64_t yb_factor_block_width(const yb_factor *f) { return f ? f->width : -1; }
+
+extern "C" int32_t yb_factor_set_block_width(yb_factor *f, int64_t width) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    const int64_t most = f->n == 1 ? kSingleRowWidth : INT64_MAX;
+    f->width = std::max<int64_t>(1, std::min<int64_t>(width, most));
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_timings(const yb_factor *f, double *upload_s, double *solve_s, double *download_s,
+                                     int64_t *blocks) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    if (upload_s) *upload_s = f->timings.upload;
+    if (solve_s) *solve_s = f->timings.solve;
+    if (download_s) *download_s = f->timings.download;
+    if (blocks) *blocks = f->timings.blocks;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_reset_timings(yb_factor *f) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    f->timings = Timings{};
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_plan_info(const yb_factor *f, int32_t *fwd_levels, int32_t *bwd_levels,
+                                       int64_t *fwd_entries, int64_t *bwd_entries, int32_t *fwd_widest,
+                                       int32_t *bwd_widest) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    if (fwd_levels) *fwd_levels = f->plan.fwd.levels;
+    if (bwd_levels) *bwd_levels = f->plan.bwd.levels;
+    if (fwd_entries) *fwd_entries = f->plan.fwd.entries();
+    if (bwd_entries) *bwd_entries = f->plan.bwd.entries();
+    if (fwd_widest) *fwd_widest = f->plan.fwd.widest;
+    if (bwd_widest) *bwd_widest = f->plan.bwd.widest;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_set_tile(yb_factor *f, int32_t precision, int32_t tile_width, int32_t threads,
+                                      int32_t blocks_per_sm) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(tile_width == 1 || tile_width == 2 || tile_width == 4 || tile_width == 8 || tile_width == 16 ||
+                tile_width == 32,
+            "the tile width must be a power of two up to 32");
+    require(threads >= 32 && threads <= 512 && threads % 32 == 0, "threads must be a multiple of 32 up to 512");
+    require(blocks_per_sm >= 1 && blocks_per_sm <= 8, "blocks per SM must be 1 to 8");
+    TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
+    t.width = tile_width;
+    t.threads = threads;
+    t.blocks_per_sm = blocks_per_sm;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_get_tile(const yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *threads,
+                                      int32_t *blocks_per_sm) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    const TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
+    if (tile_width) *tile_width = t.width;
+    if (threads) *threads = t.threads;
+    if (blocks_per_sm) *blocks_per_sm = t.blocks_per_sm;
+    return YB_OK;
+  });
+}
+
+// ---------------------------------------------------------------------------------------------
+// Launches
+// ---------------------------------------------------------------------------------------------
+
+namespace yb {
+
+template <class T, int W, Load LOAD, Store STORE>
+void launch_tiles_w(yb_factor *f, TileArgs<T> a, const TileConfig &cfg, cudaStream_t stream, DeviceArray<T> &scratch) {
+  if (a.count <= 0) return;
+  a.tiles = (a.count + W - 1) / W;
+  const int64_t grid = std::min<int64_t>(a.tiles, (int64_t)f->gpu->sm_count * cfg.blocks_per_sm);
+  scratch.reserve((size_t)grid * a.n * W);
+  a.scratch = scratch.get();
+  tile_solve_kernel<T, W, LOAD, STORE><<<(unsigned)grid, cfg.threads, 0, stream>>>(a);
+  cuda_check(cudaGetLastError(), "tile_solve_kernel launch");
+}
+
+template <class T, Load LOAD, Store STORE>
+void launch_tiles(yb_factor *f, TileArgs<T> a, const TileConfig &cfg, cudaStream_t stream, DeviceArray<T> &scratch) {
+  switch (cfg.width) {
+    case 1: return launch_tiles_w<T, 1, LOAD, STORE>(f, a, cfg, stream, scratch);
+    case 2: return launch_tiles_w<T, 2, LOAD, STORE>(f, a, cfg, stream, scratch);
+    case 4: return launch_tiles_w<T, 4, LOAD, STORE>(f, a, cfg, stream, scratch);
+    case 8: return launch_tiles_w<T, 8, LOAD, STORE>(f, a, cfg, stream, scratch);
+    case 16: return launch_tiles_w<T, 16, LOAD, STORE>(f, a, cfg, stream, scratch);
+    case 32: return launch_tiles_w<T, 32, LOAD, STORE>(f, a, cfg, stream, scratch);
+    default: throw host::Error(host::kInvalidArgument, "unsupported tile width");
+  }
+}
+
+template <class T> TileArgs<T> base_args(yb_factor *f, const DeviceSweep<T> &fwd, const DeviceSweep<T> &bwd) {
+  TileArgs<T> a{};
+  a.n = (int32_t)f->n;
+  a.in_slot = f->in_slot.get();
+  a.out_slot = f->out_slot.get();
+  a.fwd = view(fwd);
+  a.bwd = view(bwd);
+  return a;
+}
+
+// Solves `count` right-hand sides already on the device, in `precision`, on `stream`.
+void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count, int precision,
+                  cudaStream_t stream) {
+  if (count <= 0 || f->n == 0) return;
+  if (precision == YB_FP64) {
+    auto a = base_args<double>(f, f->fwd64, f->bwd64);
+    a.b = b, a.ldb = ldb, a.x = x, a.ldx = ldx, a.count = count;
+    launch_tiles<double, Load::Dense, Store::Dense>(f, a, f->tile64, stream, f->scratch64);
+  } else {
+    auto a = base_args<float>(f, f->fwd32, f->bwd32);
+    a.b = b, a.ldb = ldb, a.x = x, a.ldx = ldx, a.count = count;
+    launch_tiles<float, Load::Dense, Store::Dense>(f, a, f->tile32, stream, f->scratch32);
+  }
+}
+
+}  // namespace yb
+
+extern "C" int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
+                                        int64_t count, int32_t precision, void *stream) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(count >= 0, "negative count");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(count == 0 || (d_rhs && d_out), "null device array");
+    require(ldb >= f->n && ldx >= f->n, "a leading dimension is below the factor's order");
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    cudaStream_t s = stream ? (cudaStream_t)stream : f->gpu->stream;
+    if (f->single && count > 0) {
+      // One row: x = b / lower / upper, elementwise
+      solve_single_row_device(f, d_rhs, ldb, d_out, ldx, count, s);
+      return YB_OK;
+    }
+    solve_device(f, d_rhs, ldb, d_out, ldx, count, precision, s);
+    return YB_OK;
+  });
+}
+
+// `solve_many` (ybus_cuda/src/factor.rs:234-289) with host arrays: right-hand sides column-major
+// n x count in the caller's order, solutions likewise. Blocks of `block_width` columns go up,
+// are solved and come down; pinned caller memory is copied directly, pageable memory through a
+// pinned staging buffer.
+extern "C" int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count, double *out) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(count >= 0, "negative count");
+    const int64_t n = f->n;
+    if (n == 0 || count == 0) return YB_OK;
+    require(rhs && out, "null array");
+    if (f->single) {
+      for (int64_t k = 0; k < count; ++k) out[k] = rhs[k] / f->single_lower / f->single_upper;
+      return YB_OK;
+    }
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    cudaStream_t s = f->gpu->stream;
+    const int64_t width = f->width;
+    const int64_t chunk = std::min(width, count);
+    f->dev_b.reserve((size_t)(n * chunk));
+    f->dev_x.reserve((size_t)(n * chunk));
+    auto is_pinned = [](const void *p) {
+      cudaPointerAttributes attr{};
+      if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+      return attr.type == cudaMemoryTypeHost;
+    };
+    const bool pinned_in = is_pinned(rhs), pinned_out = is_pinned(out);
+    double *stage = (!pinned_in || !pinned_out) ? (double *)f->staging.get((size_t)(n * chunk) * sizeof(double)) : nullptr;
+    using clock = std::chrono::steady_clock;
+    for (int64_t k0 = 0; k0 < count; k0 += width) {
+      const int64_t cols = std::min(width, count - k0);
+      const size_t bytes = (size_t)(n * cols) * sizeof(double);
+      const double *src = rhs + k0 * n;
+      if (!pinned_in) {
+        std::memcpy(stage, src, bytes);
+        src = stage;
+      }
+      const auto t0 = clock::now();
+      cuda_check(cudaMemcpyAsync(f->dev_b.get(), src, bytes, cudaMemcpyHostToDevice, s), "upload");
+      cuda_check(cudaStreamSynchronize(s), "upload");
+      const auto t1 = clock::now();
+      solve_device(f, f->dev_b.get(), n, f->dev_x.get(), n, cols, YB_FP64, s);
+      cuda_check(cudaStreamSynchronize(s), "solve");
+      const auto t2 = clock::now();
+      double *dst = pinned_out ? out + k0 * n : stage;
+      cuda_check(cudaMemcpyAsync(dst, f->dev_x.get(), bytes, cudaMemcpyDeviceToHost, s), "download");
+      cuda_check(cudaStreamSynchronize(s), "download");
+      const auto t3 = clock::now();
+      if (!pinned_out) std::memcpy(out + k0 * n, stage, bytes);
+      f->timings.upload += std::chrono::duration<double>(t1 - t0).count();
+      f->timings.solve += std::chrono::duration<double>(t2 - t1).count();
+      f->timings.download += std::chrono::duration<double>(t3 - t2).count();
+      f->timings.blocks += 1;
+    }
+    return YB_OK;
+  });
+}
+
+namespace yb {
+
+namespace {
+__global__ void single_row_kernel(const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count, double lower,
+                                  double upper) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < count) x[k * ldx] = b[k * ldb] / lower / upper;
+}
+}  // namespace
+
+void solve_single_row_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
+                             cudaStream_t stream) {
+  const int threads = 256;
+  const int64_t blocks = (count + threads - 1) / threads;
+  single_row_kernel<<<(unsigned)blocks, threads, 0, stream>>>(b, ldb, x, ldx, count, f->single_lower, f->single_upper);
+  cuda_check(cudaGetLastError(), "single_row_kernel launch");
+}
+
+}  // namespace yb

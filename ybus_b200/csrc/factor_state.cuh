@@ -1,0 +1,66 @@
+// The state behind the C ABI's opaque handles `yb_gpu` and `yb_factor`.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/ybgpu.h"
+#include "device.cuh"
+#include "plan.hpp"
+
+// The widest block `yb_factor` chooses by itself. ybus_cuda caps its default at 1,024 because each
+// block is one cuSPARSE SpSM call (ybus_cuda/src/factor.rs:12); here a block is one persistent
+// launch that needs at least one tile per SM to fill the GPU, so the cap is higher.
+constexpr int64_t kMaxDefaultWidth = 65536;
+// The widest block a single-row factor uses (ybus_cuda/src/factor.rs:14-16): kept for API parity.
+constexpr int64_t kSingleRowWidth = 64;
+
+struct yb_gpu {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0, major = 0, minor = 0;
+  int64_t l2_bytes = 0;
+  std::string name;
+};
+
+namespace yb {
+
+// Seconds spent in `yb_solve_many`'s stages (ybus_cuda/src/factor.rs:22-31).
+struct Timings {
+  double upload = 0, solve = 0, download = 0;
+  int64_t blocks = 0;
+};
+
+// The launch shape of the tile solve for one precision.
+struct TileConfig {
+  int width = 8;          // right-hand sides per tile
+  int threads = 512;      // threads per block
+  int blocks_per_sm = 1;  // resident blocks per SM the grid is sized for
+};
+
+}  // namespace yb
+
+struct yb_factor {
+  yb_gpu *gpu = nullptr;
+  int64_t n = 0;
+  int kind = 0;
+  yb::Plan<double> plan;
+  yb::DeviceArray<int32_t> in_slot, out_slot;
+  yb::DeviceSweep<double> fwd64, bwd64;
+  yb::DeviceSweep<float> fwd32, bwd32;
+  yb::TileConfig tile64{8, 512, 1}, tile32{8, 512, 1};
+  yb::DeviceArray<double> scratch64;
+  yb::DeviceArray<float> scratch32;
+  yb::DeviceArray<double> dev_b, dev_x;
+  yb::PinnedBuffer staging;
+  int64_t width = 1;
+  yb::Timings timings;
+  bool single = false;
+  double single_lower = 1.0, single_upper = 1.0;
+};
+
+namespace yb {
+void solve_single_row_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
+                             cudaStream_t stream);
+}

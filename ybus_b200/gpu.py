@@ -1,0 +1,192 @@
+"""The GPU path's host API, mirroring ybus_cuda (ybus_cuda/src/lib.rs, factor.rs, pairs.rs).
+
+`Gpu.new()` is `Gpu::new()`: a device, or None where there is none. `GpuFactor` is an uploaded
+factorization whose `solve_many` solves many right-hand sides at once on the device. Every call
+goes through libybgpu's C ABI; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import YbError, check, lib, ptr
+from .host import HostCholesky, HostLu
+
+FP64 = _lib.YB_FP64
+FP32 = _lib.YB_FP32
+
+
+class CudaError(YbError):
+    """An error from the GPU path (ybus_cuda's `CudaError`, ybus_cuda/src/lib.rs:89-124)."""
+
+
+class ShapeMismatch(CudaError):
+    """A right-hand side doesn't have one entry per row (`CudaError::ShapeMismatch`)."""
+
+    def __init__(self, expected: int, found: int):
+        super().__init__(_lib.YB_ERROR_SHAPE_MISMATCH,
+                         f"a right-hand side has {found} entries, but the factorization has {expected} rows")
+        self.expected = expected
+        self.found = found
+
+
+def _check(status: int) -> None:
+    if status != _lib.YB_OK:
+        raise CudaError(status, _lib.last_error())
+
+
+@dataclass
+class Timings:
+    """Time spent by `GpuFactor.solve_many`, by stage (ybus_cuda/src/factor.rs:22-31), seconds."""
+    upload: float = 0.0
+    solve: float = 0.0
+    download: float = 0.0
+    blocks: int = 0
+
+
+class Gpu:
+    """A CUDA device and its stream (ybus_cuda's `Gpu`)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def new(cls, device: int = 0) -> "Gpu | None":
+        out = C.c_void_p()
+        status = lib().yb_gpu_new(device, C.byref(out))
+        if status == _lib.YB_NO_DEVICE:
+            return None
+        _check(status)
+        return cls(out.value)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().yb_gpu_free(h)
+            self._h = None
+
+    def name(self) -> str:
+        buf = C.create_string_buffer(256)
+        _check(lib().yb_gpu_name(self._h, buf, len(buf)))
+        return buf.value.decode()
+
+    def memory(self) -> tuple[int, int]:
+        free, total = C.c_uint64(), C.c_uint64()
+        _check(lib().yb_gpu_memory(self._h, C.byref(free), C.byref(total)))
+        return free.value, total.value
+
+    def properties(self) -> dict:
+        sm, major, minor, l2 = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int64()
+        _check(lib().yb_gpu_properties(self._h, C.byref(sm), C.byref(major), C.byref(minor), C.byref(l2)))
+        return {"sm_count": sm.value, "cc": (major.value, minor.value), "l2_bytes": l2.value}
+
+    def synchronize(self, stream: int | None = None) -> None:
+        _check(lib().yb_gpu_synchronize(self._h, stream))
+
+    @property
+    def stream(self) -> int:
+        return lib().yb_gpu_stream(self._h) or 0
+
+
+def _rhs_array(rhs, n: int) -> np.ndarray:
+    """Right-hand sides as a C-contiguous (count, n) array (column-major n x count)."""
+    if isinstance(rhs, np.ndarray):
+        if rhs.ndim != 2:
+            raise ValueError("right-hand sides are a (count, n) array")
+        if rhs.shape[1] != n and rhs.shape[0] > 0:
+            raise ShapeMismatch(n, rhs.shape[1])
+        return np.ascontiguousarray(rhs, dtype=np.float64)
+    rows = list(rhs)
+    for b in rows:
+        if len(b) != n:
+            raise ShapeMismatch(n, len(b))
+    if not rows:
+        return np.zeros((0, n))
+    return np.ascontiguousarray(np.array(rows, dtype=np.float64).reshape(len(rows), n))
+
+
+class GpuFactor:
+    """A factorization uploaded once, solving blocks of right-hand sides (ybus_cuda's `GpuFactor`)."""
+
+    def __init__(self, gpu: Gpu, handle: int):
+        self.gpu = gpu
+        self._h = C.c_void_p(handle)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().yb_factor_free(h)
+            self._h = None
+
+    @classmethod
+    def from_cholesky(cls, gpu: Gpu, chol: HostCholesky) -> "GpuFactor":
+        out = C.c_void_p()
+        l = chol.l
+        _check(lib().yb_factor_from_cholesky(gpu._h, chol.n, ptr(l.ptr), ptr(l.idx), ptr(np.ascontiguousarray(l.val)),
+                                             ptr(chol.perm), C.byref(out)))
+        return cls(gpu, out.value)
+
+    @classmethod
+    def from_lu(cls, gpu: Gpu, f: HostLu) -> "GpuFactor":
+        if f.is_complex:
+            raise CudaError(_lib.YB_ERROR_INVALID_ARGUMENT, "a complex factor uploads with from_lu_complex")
+        out = C.c_void_p()
+        _check(lib().yb_factor_from_lu(gpu._h, f.n, ptr(f.l.ptr), ptr(f.l.idx), ptr(f.l.val), ptr(f.u.ptr),
+                                       ptr(f.u.idx), ptr(f.u.val), ptr(f.row_perm), ptr(f.col_perm), C.byref(out)))
+        return cls(gpu, out.value)
+
+    def dim(self) -> int:
+        return lib().yb_factor_dim(self._h)
+
+    def block_width(self) -> int:
+        return lib().yb_factor_block_width(self._h)
+
+    def set_block_width(self, width: int) -> None:
+        _check(lib().yb_factor_set_block_width(self._h, width))
+
+    def timings(self) -> Timings:
+        u, s, d, b = C.c_double(), C.c_double(), C.c_double(), C.c_int64()
+        _check(lib().yb_factor_timings(self._h, C.byref(u), C.byref(s), C.byref(d), C.byref(b)))
+        return Timings(u.value, s.value, d.value, b.value)
+
+    def reset_timings(self) -> None:
+        _check(lib().yb_factor_reset_timings(self._h))
+
+    def plan_info(self) -> dict:
+        fl, bl, fe, be, fw, bw = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32()
+        _check(lib().yb_factor_plan_info(self._h, C.byref(fl), C.byref(bl), C.byref(fe), C.byref(be), C.byref(fw),
+                                         C.byref(bw)))
+        return {"fwd_levels": fl.value, "bwd_levels": bl.value, "fwd_entries": fe.value, "bwd_entries": be.value,
+                "fwd_widest": fw.value, "bwd_widest": bw.value}
+
+    def set_tile(self, precision: int, width: int, threads: int = 512, blocks_per_sm: int = 1) -> None:
+        _check(lib().yb_factor_set_tile(self._h, precision, width, threads, blocks_per_sm))
+
+    def tile(self, precision: int) -> tuple[int, int, int]:
+        w, t, b = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().yb_factor_get_tile(self._h, precision, C.byref(w), C.byref(t), C.byref(b)))
+        return w.value, t.value, b.value
+
+    def solve_many(self, rhs) -> np.ndarray:
+        """Solves A x = b for each right-hand side (a (count, n) array or a list of vectors) and
+        returns the solutions as a (count, n) array, in order (factor.rs:234-289)."""
+        n = self.dim()
+        b = _rhs_array(rhs, n)
+        out = np.empty_like(b)
+        if b.shape[0] == 0 or n == 0:
+            return out
+        _check(lib().yb_solve_many(self._h, ptr(b), b.shape[0], ptr(out)))
+        return out
+
+    def solve_many_into(self, b: np.ndarray, out: np.ndarray) -> None:
+        """`solve_many` into a caller's (count, n) buffer (pinned buffers are copied directly)."""
+        _check(lib().yb_solve_many(self._h, b.ctypes.data, b.shape[0], out.ctypes.data))
+
+    def solve_many_device(self, d_rhs: int, d_out: int, count: int, precision: int = FP64, stream: int | None = None,
+                          ldb: int | None = None, ldx: int | None = None) -> None:
+        """The solve on device pointers (column-major n x count), asynchronous on `stream`."""
+        n = self.dim()
+        _check(lib().yb_solve_many_device(self._h, d_rhs, ldb or n, d_out, ldx or n, count, precision, stream))
