@@ -211,7 +211,10 @@ def main():
 
     d_b = torch.from_numpy(rhs).cuda()
     d_x = torch.empty_like(d_b)
-    stream = torch.cuda.current_stream()
+    # A stream of our own: the current (legacy default) stream's handle is 0, which the C ABI
+    # reads as the library's own stream
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
 
     def step():

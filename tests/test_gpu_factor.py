@@ -106,9 +106,11 @@ def test_device_api_on_torch_memory_and_stream(gpu):
     b = torch.from_numpy(rhs).cuda()
     x = torch.empty_like(b)
     torch.cuda.synchronize()
-    stream = torch.cuda.current_stream().cuda_stream
-    factor.solve_many_device(b.data_ptr(), x.data_ptr(), 40, FP64, stream)
-    torch.cuda.current_stream().synchronize()
+    # a torch stream of its own (the legacy default stream's handle is 0, which means the
+    # library's own stream at the C ABI)
+    side = torch.cuda.Stream()
+    factor.solve_many_device(b.data_ptr(), x.data_ptr(), 40, FP64, side.cuda_stream)
+    side.synchronize()
     assert worst_relative_difference(x.cpu().numpy(), cpu) < BAR
     # and on the library's own stream
     x.zero_()
