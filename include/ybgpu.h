@@ -137,6 +137,10 @@ int32_t yb_factor_plan_info(const yb_factor *f, int32_t *fwd_levels, int32_t *bw
  * of two; threads a multiple of 32 up to 512; resident blocks per SM 1..8). */
 int32_t yb_factor_set_tile(yb_factor *f, int32_t precision, int32_t tile_width, int32_t threads,
                            int32_t blocks_per_sm);
+/* No ybus counterpart: which tile solve runs for a precision: 0 automatic (the shared-memory
+ * solve at the widest tile that fits, else the global-scratch solve), 1 the shared-memory solve
+ * (YB_ERROR_INVALID_ARGUMENT at launch if the tile does not fit), 2 the global-scratch solve. */
+int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int32_t kind);
 int32_t yb_factor_get_tile(const yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *threads,
                            int32_t *blocks_per_sm);
 

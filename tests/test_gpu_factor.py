@@ -31,16 +31,34 @@ def test_cholesky_solves_match_the_cpu_at_every_block_width(gpu):
         assert d < BAR, f"width {width}: {d:e}"
 
 
+SHARED, GLOBAL = 1, 2
+
+
+@pytest.mark.parametrize("kind", [SHARED, GLOBAL])
 @pytest.mark.parametrize("tile", [1, 2, 4, 8, 16, 32])
 @pytest.mark.parametrize("threads", [64, 256, 512])
-def test_every_tile_width_and_block_size(gpu, tile, threads):
+def test_every_tile_width_and_block_size(gpu, kind, tile, threads):
     chol = host.cholesky(random_spd(300, 3, 7))
     rhs = right_hand_sides(300, 37, 11)
     cpu = orc.solve_many(chol, rhs)
     factor = upload(gpu, chol)
-    factor.set_tile(FP64, tile, threads, 2)
+    factor.set_tile(FP64, tile, threads, 1 if kind == SHARED else 2)
+    factor.set_tile_kind(FP64, kind)
     d = worst_relative_difference(factor.solve_many(rhs), cpu)
-    assert d < BAR, f"tile {tile} threads {threads}: {d:e}"
+    assert d < BAR, f"kind {kind} tile {tile} threads {threads}: {d:e}"
+
+
+@pytest.mark.parametrize("kind", [SHARED, GLOBAL])
+def test_lu_with_both_tile_solves(gpu, kind):
+    lu = host.lu(random_square(250, 4, 3))
+    rhs = right_hand_sides(250, 45, 5)
+    cpu = orc.solve_many(lu, rhs)
+    factor = upload(gpu, lu)
+    for tile in (1, 4, 16):
+        factor.set_tile(FP64, tile, 256, 1)
+        factor.set_tile_kind(FP64, kind)
+        d = worst_relative_difference(factor.solve_many(rhs), cpu)
+        assert d < BAR, f"kind {kind} tile {tile}: {d:e}"
 
 
 def test_lu_solves_match_the_cpu_with_pivoting(gpu):
@@ -129,12 +147,14 @@ def test_fp32_substitution_is_close(gpu):
     b = torch.from_numpy(rhs).cuda()
     x = torch.empty_like(b)
     torch.cuda.synchronize()
-    for tile in [4, 8, 16, 32]:
-        factor.set_tile(FP32, tile, 512, 1)
-        factor.solve_many_device(b.data_ptr(), x.data_ptr(), 40, FP32, None)
-        gpu.synchronize()
-        d = worst_relative_difference(x.cpu().numpy(), cpu)
-        assert d < 1e-4, f"tile {tile}: {d:e}"
+    for kind in (SHARED, GLOBAL):
+        for tile in [1, 4, 8, 16, 32]:
+            factor.set_tile(FP32, tile, 512, 1)
+            factor.set_tile_kind(FP32, kind)
+            factor.solve_many_device(b.data_ptr(), x.data_ptr(), 40, FP32, None)
+            gpu.synchronize()
+            d = worst_relative_difference(x.cpu().numpy(), cpu)
+            assert d < 1e-4, f"kind {kind} tile {tile}: {d:e}"
 
 
 def _ptdf_case(n_bus, extra, seed):
@@ -160,8 +180,12 @@ def test_full_ptdf_block_on_the_10k_grid(gpu):
     b = torch.from_numpy(rhs).cuda()
     x = torch.empty_like(b)
     torch.cuda.synchronize()
-    factor.solve_many_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], FP64, None)
-    gpu.synchronize()
+    for kind in (GLOBAL, 0):
+        factor.set_tile_kind(FP64, kind)
+        x.zero_()
+        torch.cuda.synchronize()
+        factor.solve_many_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], FP64, None)
+        gpu.synchronize()
     xs = x.cpu().numpy()
     sample = np.random.default_rng(0).choice(rhs.shape[0], 96, replace=False)
     cpu = orc.solve_many(chol, rhs[sample], threads=8)

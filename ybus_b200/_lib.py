@@ -70,6 +70,7 @@ SIGNATURES: dict[str, tuple] = {
     "yb_factor_plan_info": (i32, [vp, P_i32, P_i32, P_i64, P_i64, P_i32, P_i32]),
     "yb_factor_set_tile": (i32, [vp, i32, i32, i32, i32]),
     "yb_factor_get_tile": (i32, [vp, i32, P_i32, P_i32, P_i32]),
+    "yb_factor_set_tile_kind": (i32, [vp, i32, i32]),
     "yb_solve_many": (i32, [vp, vp, i64, vp]),
     "yb_solve_many_device": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
 }
@@ -89,7 +90,7 @@ class YbError(RuntimeError):
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
+        if LIB_PATH is None or not LIB_PATH.exists():
             raise RuntimeError(f"{LIB_PATH} is not built: run `python -c 'import __graft_entry__ as g; g.build()'`")
         handle = C.CDLL(str(LIB_PATH), mode=os.RTLD_LOCAL)
         for name, (res, args) in SIGNATURES.items():

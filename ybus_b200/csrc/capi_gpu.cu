@@ -9,6 +9,7 @@
 #include "capi_common.hpp"
 #include "device.cuh"
 #include "factor_state.cuh"
+#include "smem_solve.cuh"
 #include "solve.cuh"
 
 using namespace yb;
@@ -40,6 +41,8 @@ extern "C" int32_t yb_gpu_new(int32_t device, yb_gpu **out) {
     g->major = prop.major;
     g->minor = prop.minor;
     g->l2_bytes = prop.l2CacheSize;
+    g->smem_optin = prop.sharedMemPerBlockOptin;
+    g->smem_per_sm = prop.sharedMemPerMultiprocessor;
     cuda_check(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     *out = g.release();
     return YB_OK;
@@ -270,6 +273,16 @@ extern "C" int32_t yb_factor_set_tile(yb_factor *f, int32_t precision, int32_t t
   });
 }
 
+extern "C" int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int32_t kind) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(kind >= kTileAuto && kind <= kTileGlobal, "unknown tile kind");
+    (precision == YB_FP64 ? f->tile64 : f->tile32).kind = kind;
+    return YB_OK;
+  });
+}
+
 extern "C" int32_t yb_factor_get_tile(const yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *threads,
                                       int32_t *blocks_per_sm) {
   return guard([&] {
@@ -313,6 +326,94 @@ void launch_tiles(yb_factor *f, TileArgs<T> a, const TileConfig &cfg, cudaStream
   }
 }
 
+template <class T> void upload_slices(DeviceSlices<T> &d, const SliceSweep<double> &s, cudaStream_t stream) {
+  d.levels = s.levels;
+  d.slices = s.slices();
+  d.entries = (int64_t)s.col.size();
+  d.level_slice.upload(s.level_slice, stream);
+  std::vector<int2> span(s.offset.size());
+  for (size_t i = 0; i < span.size(); ++i) span[i] = make_int2(s.offset[i], s.length[i]);
+  d.span.upload(span, stream);
+  d.row.upload(s.row, stream);
+  d.col.upload(s.col, stream);
+  d.dinv.upload(convert<T>(s.dinv), stream);
+  d.val.upload(convert<T>(s.val), stream);
+}
+
+template <class T>
+DeviceSlices<T> *slices_for(yb_factor *f, std::map<int, std::unique_ptr<DeviceSlices<T>[]>> &cache, int W,
+                            cudaStream_t stream) {
+  auto it = cache.find(W);
+  if (it != cache.end()) return it->second.get();
+  std::unique_ptr<DeviceSlices<T>[]> pair(new DeviceSlices<T>[2]);
+  upload_slices(pair[0], slice_sweep(f->plan.fwd, f->plan.n, 32 / W), stream);
+  upload_slices(pair[1], slice_sweep(f->plan.bwd, f->plan.n, 32 / W), stream);
+  auto *out = pair.get();
+  cache.emplace(W, std::move(pair));
+  return out;
+}
+
+template <class T> SliceView<T> slice_view(const DeviceSlices<T> &d) {
+  return SliceView<T>{d.levels, d.level_slice.get(), d.span.get(), d.row.get(), d.dinv.get(), d.col.get(), d.val.get()};
+}
+
+template <class T> size_t smem_bytes(const yb_factor *f, int W) { return (size_t)(f->n + 2) * W * sizeof(T); }
+
+template <class T> bool smem_fits(const yb_factor *f, const TileConfig &cfg) {
+  return smem_bytes<T>(f, cfg.width) <= (size_t)f->gpu->smem_optin &&
+         smem_bytes<T>(f, cfg.width) * cfg.blocks_per_sm <= (size_t)f->gpu->smem_per_sm;
+}
+
+template <class T, int W>
+void launch_smem_w(yb_factor *f, SmemArgs<T> a, const TileConfig &cfg, cudaStream_t stream,
+                   std::map<int, std::unique_ptr<DeviceSlices<T>[]>> &cache) {
+  // entries prefetched per slice: as many as keep the kernel within 128 registers
+  constexpr int CH = sizeof(T) == 8 ? 4 : 8;
+  DeviceSlices<T> *sl = slices_for<T>(f, cache, W, stream);
+  a.fwd = slice_view(sl[0]);
+  a.bwd = slice_view(sl[1]);
+  a.tiles = (a.count + W - 1) / W;
+  const size_t smem = smem_bytes<T>(f, W);
+  cuda_check(cudaFuncSetAttribute(smem_tile_kernel<T, W, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  const int64_t grid = std::min<int64_t>(a.tiles, (int64_t)f->gpu->sm_count * cfg.blocks_per_sm);
+  smem_tile_kernel<T, W, CH><<<(unsigned)grid, cfg.threads, smem, stream>>>(a);
+  cuda_check(cudaGetLastError(), "smem_tile_kernel launch");
+}
+
+template <class T>
+void launch_smem(yb_factor *f, SmemArgs<T> a, const TileConfig &cfg, cudaStream_t stream,
+                 std::map<int, std::unique_ptr<DeviceSlices<T>[]>> &cache) {
+  switch (cfg.width) {
+    case 1: return launch_smem_w<T, 1>(f, a, cfg, stream, cache);
+    case 2: return launch_smem_w<T, 2>(f, a, cfg, stream, cache);
+    case 4: return launch_smem_w<T, 4>(f, a, cfg, stream, cache);
+    case 8: return launch_smem_w<T, 8>(f, a, cfg, stream, cache);
+    case 16: return launch_smem_w<T, 16>(f, a, cfg, stream, cache);
+    case 32: return launch_smem_w<T, 32>(f, a, cfg, stream, cache);
+    default: throw host::Error(host::kInvalidArgument, "unsupported tile width");
+  }
+}
+
+// The shape the auto kind runs: the widest tile whose working vector fits in shared memory at
+// one block per SM, else the global-scratch kernel with the configured shape.
+template <class T> TileConfig resolve(const yb_factor *f, TileConfig cfg) {
+  if (cfg.kind == kTileGlobal) return cfg;
+  if (cfg.kind == kTileShared) {
+    if (!smem_fits<T>(f, cfg)) throw host::Error(host::kInvalidArgument, "the tile does not fit in shared memory");
+    return cfg;
+  }
+  for (int w = 32; w >= 1; w /= 2) {
+    TileConfig c = cfg;
+    c.width = w;
+    c.blocks_per_sm = 1;
+    c.kind = kTileShared;
+    if (smem_fits<T>(f, c)) return c;
+  }
+  cfg.kind = kTileGlobal;
+  return cfg;
+}
+
 template <class T> TileArgs<T> base_args(yb_factor *f, const DeviceSweep<T> &fwd, const DeviceSweep<T> &bwd) {
   TileArgs<T> a{};
   a.n = (int32_t)f->n;
@@ -327,15 +428,27 @@ template <class T> TileArgs<T> base_args(yb_factor *f, const DeviceSweep<T> &fwd
 void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count, int precision,
                   cudaStream_t stream) {
   if (count <= 0 || f->n == 0) return;
-  if (precision == YB_FP64) {
-    auto a = base_args<double>(f, f->fwd64, f->bwd64);
-    a.b = b, a.ldb = ldb, a.x = x, a.ldx = ldx, a.count = count;
-    launch_tiles<double, Load::Dense, Store::Dense>(f, a, f->tile64, stream, f->scratch64);
-  } else {
-    auto a = base_args<float>(f, f->fwd32, f->bwd32);
-    a.b = b, a.ldb = ldb, a.x = x, a.ldx = ldx, a.count = count;
-    launch_tiles<float, Load::Dense, Store::Dense>(f, a, f->tile32, stream, f->scratch32);
-  }
+  auto run = [&](auto zero, const TileConfig &configured, auto &fwd, auto &bwd, auto &scratch, auto &cache) {
+    using T = decltype(zero);
+    const TileConfig cfg = resolve<T>(f, configured);
+    if (cfg.kind == kTileShared) {
+      SmemArgs<T> a{};
+      a.n = (int32_t)f->n;
+      a.count = count;
+      a.b = b, a.ldb = ldb, a.x = x, a.ldx = ldx;
+      a.in_slot = f->in_slot.get();
+      a.out_slot = f->out_slot.get();
+      launch_smem<T>(f, a, cfg, stream, cache);
+    } else {
+      auto a = base_args<T>(f, fwd, bwd);
+      a.b = b, a.ldb = ldb, a.x = x, a.ldx = ldx, a.count = count;
+      launch_tiles<T, Load::Dense, Store::Dense>(f, a, cfg, stream, scratch);
+    }
+  };
+  if (precision == YB_FP64)
+    run(0.0, f->tile64, f->fwd64, f->bwd64, f->scratch64, f->slices64);
+  else
+    run(0.0f, f->tile32, f->fwd32, f->bwd32, f->scratch32, f->slices32);
 }
 
 }  // namespace yb

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
+#include <memory>
 #include <string>
 
 #include "../../include/ybgpu.h"
@@ -21,6 +23,8 @@ struct yb_gpu {
   cudaStream_t stream = nullptr;
   int sm_count = 0, major = 0, minor = 0;
   int64_t l2_bytes = 0;
+  int64_t smem_optin = 0;       // largest dynamic shared memory a block may opt into
+  int64_t smem_per_sm = 0;
   std::string name;
 };
 
@@ -32,11 +36,25 @@ struct Timings {
   int64_t blocks = 0;
 };
 
+// Which tile solve runs: the shared-memory one (the tile's working vector in shared memory) when
+// it fits, or the one whose working vectors live in a global scratch buffer.
+enum TileKind : int { kTileAuto = 0, kTileShared = 1, kTileGlobal = 2 };
+
 // The launch shape of the tile solve for one precision.
 struct TileConfig {
   int width = 8;          // right-hand sides per tile
   int threads = 512;      // threads per block
   int blocks_per_sm = 1;  // resident blocks per SM the grid is sized for
+  int kind = kTileAuto;
+};
+
+// A sliced sweep on the device (SliceSweep in plan.hpp), at value type T.
+template <class T> struct DeviceSlices {
+  int32_t levels = 0;
+  int64_t slices = 0, entries = 0;
+  DeviceArray<int32_t> level_slice, row, col;
+  DeviceArray<int2> span;
+  DeviceArray<T> dinv, val;
 };
 
 }  // namespace yb
@@ -50,6 +68,9 @@ struct yb_factor {
   yb::DeviceSweep<double> fwd64, bwd64;
   yb::DeviceSweep<float> fwd32, bwd32;
   yb::TileConfig tile64{8, 512, 1}, tile32{8, 512, 1};
+  // sliced sweeps per tile width (built on first use): [width] -> {forward, backward}
+  std::map<int, std::unique_ptr<yb::DeviceSlices<double>[]>> slices64;
+  std::map<int, std::unique_ptr<yb::DeviceSlices<float>[]>> slices32;
   yb::DeviceArray<double> scratch64;
   yb::DeviceArray<float> scratch32;
   yb::DeviceArray<double> dev_b, dev_x;

@@ -127,6 +127,59 @@ Plan<T> build_plan(int64_t n, const host::Compressed<T> &lower, bool unit_lower,
   return plan;
 }
 
+template <class T> SliceSweep<T> slice_sweep(const Sweep<T> &s, int32_t n, int32_t G) {
+  if (G < 1 || G > 32) throw Error(host::kInvalidArgument, "slice width must be 1 to 32");
+  SliceSweep<T> out;
+  out.G = G;
+  out.levels = s.levels;
+  out.level_slice.assign(1, 0);
+  std::vector<int32_t> rows;
+  for (int32_t l = 0; l < s.levels; ++l) {
+    rows.assign(s.row.begin() + s.level_ptr[l], s.row.begin() + s.level_ptr[l + 1]);
+    // positions k of this level, longest rows first (stable by position)
+    std::vector<int32_t> ks(rows.size());
+    for (size_t t = 0; t < ks.size(); ++t) ks[t] = s.level_ptr[l] + (int32_t)t;
+    std::stable_sort(ks.begin(), ks.end(), [&](int32_t a, int32_t b) {
+      return (s.ptr[a + 1] - s.ptr[a]) > (s.ptr[b + 1] - s.ptr[b]);
+    });
+    for (size_t t0 = 0; t0 < ks.size(); t0 += G) {
+      const size_t t1 = std::min(ks.size(), t0 + (size_t)G);
+      int32_t len = 0;
+      for (size_t t = t0; t < t1; ++t) len = std::max(len, s.ptr[ks[t] + 1] - s.ptr[ks[t]]);
+      out.offset.push_back((int32_t)out.col.size());
+      out.length.push_back(len);
+      for (int32_t g = 0; g < G; ++g) {
+        const size_t t = t0 + g;
+        if (t < t1) {
+          out.row.push_back(s.row[ks[t]]);
+          out.dinv.push_back(s.dinv[ks[t]]);
+        } else {
+          out.row.push_back(n + 1);
+          out.dinv.push_back(T(0));
+        }
+      }
+      for (int32_t q = 0; q < len; ++q)
+        for (int32_t g = 0; g < G; ++g) {
+          const size_t t = t0 + g;
+          if (t < t1 && q < s.ptr[ks[t] + 1] - s.ptr[ks[t]]) {
+            const int32_t p = s.ptr[ks[t]] + q;
+            out.col.push_back(s.col[p]);
+            out.val.push_back(s.val[p]);
+          } else {
+            out.col.push_back(n);
+            out.val.push_back(T(0));
+          }
+        }
+      if ((int64_t)out.col.size() > std::numeric_limits<int32_t>::max())
+        throw Error(host::kTooLarge, "the sliced factor has too many entries for 32-bit offsets");
+    }
+    out.level_slice.push_back((int32_t)out.offset.size());
+  }
+  return out;
+}
+
+template SliceSweep<double> slice_sweep(const Sweep<double> &, int32_t, int32_t);
+
 template Plan<double> build_plan(int64_t, const host::Compressed<double> &, bool, const host::Compressed<double> &,
                                  const std::vector<int64_t> &, const std::vector<int64_t> &);
 template Plan<host::c128> build_plan(int64_t, const host::Compressed<host::c128> &, bool,

@@ -34,6 +34,25 @@ template <class T> struct Sweep {
   int64_t entries() const { return (int64_t)col.size(); }
 };
 
+// A sweep cut into slices for the shared-memory tile solve: each level's rows, longest first,
+// taken G at a time (one row per lane group of a warp). A slice's entries are stored entry-major
+// (entry q of its G rows contiguous), so a warp reads entry q of all its rows in one coalesced
+// access with no dependent index loads. Short rows are padded with (col = n, val = 0), which
+// reads an always-zero slot; missing rows of a level's last slice write to slot n + 1.
+template <class T> struct SliceSweep {
+  int32_t G = 0, levels = 0;
+  std::vector<int32_t> level_slice;  // [levels + 1] slice ranges
+  std::vector<int32_t> offset, length;  // [slices] entry offset and padded row length
+  std::vector<int32_t> row;          // [slices * G]
+  std::vector<T> dinv;               // [slices * G]
+  std::vector<int32_t> col;          // [entries]
+  std::vector<T> val;                // [entries]
+  int64_t slices() const { return (int64_t)offset.size(); }
+};
+
+// Cuts `s` into slices of G rows for a factor of order n.
+template <class T> SliceSweep<T> slice_sweep(const Sweep<T> &s, int32_t n, int32_t G);
+
 template <class T> struct Plan {
   int32_t n = 0;
   std::vector<int32_t> in_slot, out_slot;   // [n]

@@ -65,7 +65,10 @@ class Gpu:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib().yb_gpu_free(h)
+            try:
+                lib().yb_gpu_free(h)
+            except Exception:
+                pass
             self._h = None
 
     def name(self) -> str:
@@ -118,7 +121,10 @@ class GpuFactor:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib().yb_factor_free(h)
+            try:
+                lib().yb_factor_free(h)
+            except Exception:
+                pass
             self._h = None
 
     @classmethod
@@ -164,6 +170,10 @@ class GpuFactor:
 
     def set_tile(self, precision: int, width: int, threads: int = 512, blocks_per_sm: int = 1) -> None:
         _check(lib().yb_factor_set_tile(self._h, precision, width, threads, blocks_per_sm))
+
+    def set_tile_kind(self, precision: int, kind: int) -> None:
+        """0 automatic, 1 shared-memory tile solve, 2 global-scratch tile solve."""
+        _check(lib().yb_factor_set_tile_kind(self._h, precision, kind))
 
     def tile(self, precision: int) -> tuple[int, int, int]:
         w, t, b = C.c_int32(), C.c_int32(), C.c_int32()

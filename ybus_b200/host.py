@@ -28,7 +28,10 @@ class Matrix:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib().yb_matrix_free(h)
+            try:
+                lib().yb_matrix_free(h)
+            except Exception:
+                pass
             self._h = None
 
     @classmethod
