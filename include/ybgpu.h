@@ -137,10 +137,24 @@ int32_t yb_factor_plan_info(const yb_factor *f, int32_t *fwd_levels, int32_t *bw
  * of two; threads a multiple of 32 up to 512; resident blocks per SM 1..8). */
 int32_t yb_factor_set_tile(yb_factor *f, int32_t precision, int32_t tile_width, int32_t threads,
                            int32_t blocks_per_sm);
-/* No ybus counterpart: which tile solve runs for a precision: 0 automatic (the shared-memory
- * solve at the widest tile that fits, else the global-scratch solve), 1 the shared-memory solve
- * (YB_ERROR_INVALID_ARGUMENT at launch if the tile does not fit), 2 the global-scratch solve. */
+/* No ybus counterpart: which tile solve runs for a precision: 0 automatic (the streamed solve at
+ * the widest tile that fits in shared memory, else the global-scratch solve), 1 the level-sliced
+ * shared-memory solve, 2 the global-scratch solve, 3 the streamed solve (1 and 3 give
+ * YB_ERROR_INVALID_ARGUMENT at launch if the tile does not fit in shared memory). */
 int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int32_t kind);
+/* No ybus counterpart: the streamed solve's shape for a precision: warps per block (1..16), pages
+ * in flight per warp (2..16), page bytes (512..16384, a multiple of 16), and the row count under
+ * which a level is taken by one warp alone (0: twice a slice's rows). */
+int32_t yb_factor_set_stream(yb_factor *f, int32_t precision, int32_t warps, int32_t ring,
+                             int32_t page_bytes, int32_t narrow_rows);
+/* No ybus counterpart: the streamed layout the automatic choice runs for a precision (building it
+ * if needed); YB_ERROR_INVALID_ARGUMENT if that choice is not the streamed solve. */
+int32_t yb_factor_stream_info(yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *stages,
+                              int64_t *records, int64_t *bytes, int32_t *fwd_wide, int32_t *bwd_wide,
+                              int32_t *narrow_rows);
+/* Waits for the device and reports YB_ERROR_DEVICE_TIMEOUT (clearing it) if a bounded wait in a
+ * kernel of this factor ran out since the last check; the host-array calls check by themselves. */
+int32_t yb_factor_check_error(yb_factor *f);
 int32_t yb_factor_get_tile(const yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *threads,
                            int32_t *blocks_per_sm);
 

@@ -31,7 +31,7 @@ def test_cholesky_solves_match_the_cpu_at_every_block_width(gpu):
         assert d < BAR, f"width {width}: {d:e}"
 
 
-SHARED, GLOBAL = 1, 2
+SHARED, GLOBAL, STREAM = 1, 2, 3
 
 
 @pytest.mark.parametrize("kind", [SHARED, GLOBAL])
@@ -48,8 +48,31 @@ def test_every_tile_width_and_block_size(gpu, kind, tile, threads):
     assert d < BAR, f"kind {kind} tile {tile} threads {threads}: {d:e}"
 
 
-@pytest.mark.parametrize("kind", [SHARED, GLOBAL])
-def test_lu_with_both_tile_solves(gpu, kind):
+@pytest.mark.parametrize("tile", [1, 2, 4, 8, 16, 32])
+@pytest.mark.parametrize("warps,ring,page,narrow", [(8, 4, 2048, 0), (4, 2, 512, 0), (1, 3, 1024, 0),
+                                                    (8, 4, 512, 100000), (8, 4, 2048, 1), (16, 2, 768, 3)])
+def test_streamed_solve_every_layout(gpu, tile, warps, ring, page, narrow):
+    # small pages force chunked records; narrow=100000 puts every level on warp 0 (split rows),
+    # narrow=1 none; 2,000 right-hand sides make several tiles per block at tile width 1
+    chol = host.cholesky(random_spd(300, 3, 7))
+    rhs = right_hand_sides(300, 37, 11)
+    cpu = orc.solve_many(chol, rhs)
+    factor = upload(gpu, chol)
+    factor.set_tile(FP64, tile, 256, 1)
+    factor.set_tile_kind(FP64, STREAM)
+    factor.set_stream(FP64, warps, ring, page, narrow)
+    d = worst_relative_difference(factor.solve_many(rhs), cpu)
+    assert d < BAR, f"tile {tile}: {d:e}"
+    if tile == 1:
+        many = right_hand_sides(300, 400, 3)
+        many = np.concatenate([many] * 5)
+        d = worst_relative_difference(factor.solve_many(many), orc.solve_many(chol, many))
+        assert d < BAR, f"many tiles: {d:e}"
+    factor.check_error()
+
+
+@pytest.mark.parametrize("kind", [SHARED, GLOBAL, STREAM])
+def test_lu_with_every_tile_solve(gpu, kind):
     lu = host.lu(random_square(250, 4, 3))
     rhs = right_hand_sides(250, 45, 5)
     cpu = orc.solve_many(lu, rhs)
@@ -147,7 +170,7 @@ def test_fp32_substitution_is_close(gpu):
     b = torch.from_numpy(rhs).cuda()
     x = torch.empty_like(b)
     torch.cuda.synchronize()
-    for kind in (SHARED, GLOBAL):
+    for kind in (SHARED, GLOBAL, STREAM):
         for tile in [1, 4, 8, 16, 32]:
             factor.set_tile(FP32, tile, 512, 1)
             factor.set_tile_kind(FP32, kind)

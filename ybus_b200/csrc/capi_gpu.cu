@@ -10,6 +10,7 @@
 #include "device.cuh"
 #include "factor_state.cuh"
 #include "smem_solve.cuh"
+#include "stream_solve.cuh"
 #include "solve.cuh"
 
 using namespace yb;
@@ -155,6 +156,8 @@ yb_factor *make_factor(yb_gpu *gpu, int64_t n, host::Compressed<double> lower, b
   upload_sweep(f->bwd64, f->plan.bwd, f->plan.n, s);
   upload_sweep(f->fwd32, f->plan.fwd, f->plan.n, s);
   upload_sweep(f->bwd32, f->plan.bwd, f->plan.n, s);
+  f->error.resize(1);
+  cuda_check(cudaMemsetAsync(f->error.get(), 0, sizeof(int32_t), s), "cudaMemsetAsync");
   cuda_check(cudaStreamSynchronize(s), "upload");
   // Default block width as ybus_cuda chooses it: two n-column blocks of doubles per right-hand
   // side in a quarter of the free memory (ybus_cuda/src/factor.rs:157-160), capped higher here
@@ -277,8 +280,38 @@ extern "C" int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int3
   return guard([&] {
     require(f != nullptr, "null factor");
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
-    require(kind >= kTileAuto && kind <= kTileGlobal, "unknown tile kind");
+    require(kind >= kTileAuto && kind <= kTileStream, "unknown tile kind");
     (precision == YB_FP64 ? f->tile64 : f->tile32).kind = kind;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_set_stream(yb_factor *f, int32_t precision, int32_t warps, int32_t ring,
+                                        int32_t page_bytes, int32_t narrow_rows) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(warps >= 1 && warps <= 16, "warps must be 1 to 16");
+    require(ring >= 2 && ring <= 16, "the ring holds 2 to 16 pages");
+    require(page_bytes >= 512 && page_bytes <= 16384 && page_bytes % 16 == 0,
+            "page bytes must be a multiple of 16 from 512 to 16384");
+    require(narrow_rows >= 0, "narrow rows must not be negative");
+    TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
+    t.stream_warps = warps, t.ring = ring, t.page_bytes = page_bytes, t.narrow_rows = narrow_rows;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_check_error(yb_factor *f) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    int32_t word = 0;
+    cuda_check(cudaMemcpy(&word, f->error.get(), sizeof word, cudaMemcpyDeviceToHost), "read error word");
+    if (word != 0) {
+      cuda_check(cudaMemset(f->error.get(), 0, sizeof word), "clear error word");
+      throw host::Error(host::kDeviceTimeout, "a bounded device wait ran out in the streamed solve");
+    }
     return YB_OK;
   });
 }
@@ -395,10 +428,93 @@ void launch_smem(yb_factor *f, SmemArgs<T> a, const TileConfig &cfg, cudaStream_
   }
 }
 
-// The shape the auto kind runs: the widest tile whose working vector fits in shared memory at
-// one block per SM, else the global-scratch kernel with the configured shape.
+template <class T> size_t stream_smem_bytes(const yb_factor *f, const TileConfig &cfg, int W) {
+  const size_t y = (((size_t)(f->n + 2) * W * sizeof(T)) + 127) & ~(size_t)127;
+  return y + (size_t)cfg.stream_warps * cfg.ring * cfg.page_bytes + (size_t)cfg.stream_warps * cfg.ring * 8;
+}
+
+template <class T> bool stream_fits(const yb_factor *f, const TileConfig &cfg, int W) {
+  return stream_smem_bytes<T>(f, cfg, W) <= (size_t)f->gpu->smem_optin;
+}
+
+template <class T> DeviceStream *stream_for(yb_factor *f, const TileConfig &cfg, int W, cudaStream_t stream) {
+  const int narrow = cfg.narrow_rows > 0 ? cfg.narrow_rows : 2 * (32 / W);
+  const auto key = std::make_tuple((int)sizeof(T), W, cfg.stream_warps, cfg.page_bytes, narrow);
+  auto it = f->streams.find(key);
+  if (it != f->streams.end()) return it->second.get();
+  const StreamLayout lay = stream_layout(f->plan, W, (int)sizeof(T), cfg.stream_warps, cfg.page_bytes, narrow);
+  auto d = std::make_unique<DeviceStream>();
+  d->stages = lay.stages;
+  d->G = lay.G;
+  d->records = lay.records;
+  d->bytes = (int64_t)lay.blob.size();
+  d->fwd_wide = lay.fwd_wide, d->bwd_wide = lay.bwd_wide;
+  d->fwd_narrow_rows = lay.fwd_narrow_rows, d->bwd_narrow_rows = lay.bwd_narrow_rows;
+  d->blob.upload(lay.blob, stream);
+  d->warp_page.upload(lay.warp_page, stream);
+  std::vector<uint8_t> scale(lay.load_scale.size() * sizeof(T));
+  for (size_t i = 0; i < lay.load_scale.size(); ++i) {
+    const T v = (T)lay.load_scale[i];
+    std::memcpy(scale.data() + i * sizeof(T), &v, sizeof(T));
+  }
+  d->load_scale.upload(scale, stream);
+  cuda_check(cudaStreamSynchronize(stream), "stream layout upload");
+  auto *out = d.get();
+  f->streams.emplace(key, std::move(d));
+  return out;
+}
+
+template <class T, int W>
+void launch_stream_w(yb_factor *f, StreamArgs a, const TileConfig &cfg, cudaStream_t stream) {
+  DeviceStream *d = stream_for<T>(f, cfg, W, stream);
+  a.tiles = (a.count + W - 1) / W;
+  a.blob = d->blob.get();
+  a.warp_page = d->warp_page.get();
+  a.load_scale = d->load_scale.get();
+  a.page_bytes = cfg.page_bytes;
+  a.ring = cfg.ring;
+  a.stages = d->stages;
+  a.error = f->error.get();
+  const size_t smem = stream_smem_bytes<T>(f, cfg, W);
+  cuda_check(cudaFuncSetAttribute(stream_tile_kernel<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  const int64_t grid = std::min<int64_t>(a.tiles, (int64_t)f->gpu->sm_count * cfg.blocks_per_sm);
+  stream_tile_kernel<T, W><<<(unsigned)grid, cfg.stream_warps * 32, smem, stream>>>(a);
+  cuda_check(cudaGetLastError(), "stream_tile_kernel launch");
+}
+
+template <class T> void launch_stream(yb_factor *f, StreamArgs a, const TileConfig &cfg, cudaStream_t stream) {
+  switch (cfg.width) {
+    case 1: return launch_stream_w<T, 1>(f, a, cfg, stream);
+    case 2: return launch_stream_w<T, 2>(f, a, cfg, stream);
+    case 4: return launch_stream_w<T, 4>(f, a, cfg, stream);
+    case 8: return launch_stream_w<T, 8>(f, a, cfg, stream);
+    case 16: return launch_stream_w<T, 16>(f, a, cfg, stream);
+    case 32: return launch_stream_w<T, 32>(f, a, cfg, stream);
+    default: throw host::Error(host::kInvalidArgument, "unsupported tile width");
+  }
+}
+
+// The shape the auto kind runs: the streamed solve at the widest tile whose working vector and
+// page rings fit in shared memory (one block per SM), else the global-scratch kernel.
 template <class T> TileConfig resolve(const yb_factor *f, TileConfig cfg) {
   if (cfg.kind == kTileGlobal) return cfg;
+  if (cfg.kind == kTileStream) {
+    if (!stream_fits<T>(f, cfg, cfg.width)) throw host::Error(host::kInvalidArgument, "the tile does not fit in shared memory");
+    return cfg;
+  }
+  if (cfg.kind == kTileAuto) {
+    for (int w = 32; w >= 1; w /= 2)
+      if (stream_fits<T>(f, cfg, w)) {
+        TileConfig c = cfg;
+        c.width = w;
+        c.blocks_per_sm = 1;
+        c.kind = kTileStream;
+        return c;
+      }
+    cfg.kind = kTileGlobal;
+    return cfg;
+  }
   if (cfg.kind == kTileShared) {
     if (!smem_fits<T>(f, cfg)) throw host::Error(host::kInvalidArgument, "the tile does not fit in shared memory");
     return cfg;
@@ -431,7 +547,15 @@ void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t
   auto run = [&](auto zero, const TileConfig &configured, auto &fwd, auto &bwd, auto &scratch, auto &cache) {
     using T = decltype(zero);
     const TileConfig cfg = resolve<T>(f, configured);
-    if (cfg.kind == kTileShared) {
+    if (cfg.kind == kTileStream) {
+      StreamArgs a{};
+      a.n = (int32_t)f->n;
+      a.count = count;
+      a.b = b, a.ldb = ldb, a.x = x, a.ldx = ldx;
+      a.in_slot = f->in_slot.get();
+      a.out_slot = f->out_slot.get();
+      launch_stream<T>(f, a, cfg, stream);
+    } else if (cfg.kind == kTileShared) {
       SmemArgs<T> a{};
       a.n = (int32_t)f->n;
       a.count = count;
@@ -519,6 +643,14 @@ extern "C" int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count,
       const auto t1 = clock::now();
       solve_device(f, f->dev_b.get(), n, f->dev_x.get(), n, cols, YB_FP64, s);
       cuda_check(cudaStreamSynchronize(s), "solve");
+      {
+        int32_t word = 0;
+        cuda_check(cudaMemcpy(&word, f->error.get(), sizeof word, cudaMemcpyDeviceToHost), "read error word");
+        if (word != 0) {
+          cuda_check(cudaMemset(f->error.get(), 0, sizeof word), "clear error word");
+          throw host::Error(host::kDeviceTimeout, "a bounded device wait ran out in the streamed solve");
+        }
+      }
       const auto t2 = clock::now();
       double *dst = pinned_out ? out + k0 * n : stage;
       cuda_check(cudaMemcpyAsync(dst, f->dev_x.get(), bytes, cudaMemcpyDeviceToHost, s), "download");
@@ -553,3 +685,31 @@ void solve_single_row_device(yb_factor *f, const double *b, int64_t ldb, double 
 }
 
 }  // namespace yb
+
+extern "C" int32_t yb_factor_stream_info(yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *stages,
+                                         int64_t *records, int64_t *bytes, int32_t *fwd_wide, int32_t *bwd_wide,
+                                         int32_t *narrow_rows) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    const TileConfig &configured = precision == YB_FP64 ? f->tile64 : f->tile32;
+    TileConfig cfg;
+    DeviceStream *d = nullptr;
+    if (precision == YB_FP64) {
+      cfg = resolve<double>(f, configured);
+      if (cfg.kind == kTileStream) d = stream_for<double>(f, cfg, cfg.width, f->gpu->stream);
+    } else {
+      cfg = resolve<float>(f, configured);
+      if (cfg.kind == kTileStream) d = stream_for<float>(f, cfg, cfg.width, f->gpu->stream);
+    }
+    if (tile_width) *tile_width = cfg.width;
+    if (stages) *stages = d ? d->stages : 0;
+    if (records) *records = d ? d->records : 0;
+    if (bytes) *bytes = d ? d->bytes : 0;
+    if (fwd_wide) *fwd_wide = d ? d->fwd_wide : 0;
+    if (bwd_wide) *bwd_wide = d ? d->bwd_wide : 0;
+    if (narrow_rows) *narrow_rows = d ? d->fwd_narrow_rows + d->bwd_narrow_rows : 0;
+    return d ? (int32_t)YB_OK : (int32_t)YB_ERROR_INVALID_ARGUMENT;
+  });
+}
+

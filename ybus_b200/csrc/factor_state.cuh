@@ -6,6 +6,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 
 #include "../../include/ybgpu.h"
 #include "device.cuh"
@@ -38,7 +39,7 @@ struct Timings {
 
 // Which tile solve runs: the shared-memory one (the tile's working vector in shared memory) when
 // it fits, or the one whose working vectors live in a global scratch buffer.
-enum TileKind : int { kTileAuto = 0, kTileShared = 1, kTileGlobal = 2 };
+enum TileKind : int { kTileAuto = 0, kTileShared = 1, kTileGlobal = 2, kTileStream = 3 };
 
 // The launch shape of the tile solve for one precision.
 struct TileConfig {
@@ -46,6 +47,19 @@ struct TileConfig {
   int threads = 512;      // threads per block
   int blocks_per_sm = 1;  // resident blocks per SM the grid is sized for
   int kind = kTileAuto;
+  // the streamed solve's shape: warps per block, pages in flight per warp, page bytes, and the
+  // row count under which a level goes to warp 0 (0: twice the rows of a slice)
+  int stream_warps = 8, ring = 4, page_bytes = 2048, narrow_rows = 0;
+};
+
+// A streamed layout on the device (StreamLayout in plan.hpp).
+struct DeviceStream {
+  int32_t stages = 0, G = 0;
+  int64_t records = 0, bytes = 0;
+  int32_t fwd_wide = 0, bwd_wide = 0, fwd_narrow_rows = 0, bwd_narrow_rows = 0;
+  DeviceArray<uint8_t> blob;
+  DeviceArray<int32_t> warp_page;
+  DeviceArray<uint8_t> load_scale;
 };
 
 // A sliced sweep on the device (SliceSweep in plan.hpp), at value type T.
@@ -71,6 +85,9 @@ struct yb_factor {
   // sliced sweeps per tile width (built on first use): [width] -> {forward, backward}
   std::map<int, std::unique_ptr<yb::DeviceSlices<double>[]>> slices64;
   std::map<int, std::unique_ptr<yb::DeviceSlices<float>[]>> slices32;
+  // streamed layouts by shape (precision, width, warps, page bytes, narrow rows)
+  std::map<std::tuple<int, int, int, int, int>, std::unique_ptr<yb::DeviceStream>> streams;
+  yb::DeviceArray<int32_t> error;  // the device error word (a bounded wait that ran out)
   yb::DeviceArray<double> scratch64;
   yb::DeviceArray<float> scratch32;
   yb::DeviceArray<double> dev_b, dev_x;

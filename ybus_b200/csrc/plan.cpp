@@ -1,6 +1,9 @@
 #include "plan.hpp"
 
+#include <complex>
+#include <cstring>
 #include <limits>
+#include <memory>
 #include <string>
 
 namespace yb {
@@ -185,5 +188,222 @@ template Plan<double> build_plan(int64_t, const host::Compressed<double> &, bool
 template Plan<host::c128> build_plan(int64_t, const host::Compressed<host::c128> &, bool,
                                      const host::Compressed<host::c128> &, const std::vector<int64_t> &,
                                      const std::vector<int64_t> &);
+
+}  // namespace yb
+
+namespace yb {
+
+namespace {
+
+inline int64_t align16(int64_t v) { return (v + 15) & ~int64_t(15); }
+
+// Appends records to one warp's pages.
+struct PageWriter {
+  int32_t page_bytes;
+  std::vector<uint8_t> &blob;
+  int64_t page_start = -1, pos = 0;
+  int32_t pages = 0;
+  PageWriter(int32_t pb, std::vector<uint8_t> &b) : page_bytes(pb), blob(b) {}
+  void close_page() {
+    if (page_start < 0) return;
+    if (pos + 16 <= page_bytes) {
+      int32_t end[4] = {kRecordEnd, 0, 0, 0};
+      std::memcpy(blob.data() + page_start + pos, end, 16);
+    }
+    page_start = -1;
+  }
+  uint8_t *reserve(int64_t bytes) {
+    if (bytes > page_bytes) throw Error(host::kInternal, "a stream record does not fit a page");
+    if (page_start < 0 || pos + bytes > page_bytes) {
+      close_page();
+      page_start = (int64_t)blob.size();
+      blob.resize(blob.size() + page_bytes, 0);
+      pos = 0;
+      ++pages;
+    }
+    uint8_t *p = blob.data() + page_start + pos;
+    pos += bytes;
+    return p;
+  }
+};
+
+template <class V> void put(uint8_t *&p, const V *v, int64_t count) {
+  std::memcpy(p, v, sizeof(V) * count);
+  p += align16(sizeof(V) * count);
+}
+
+}  // namespace
+
+template <class T>
+StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, int32_t warps, int32_t page_bytes,
+                           int32_t narrow_rows) {
+  if (W < 1 || W > 32 || 32 % W) throw Error(host::kInvalidArgument, "tile width must divide 32");
+  if (value_bytes != 8 && value_bytes != 4) throw Error(host::kInvalidArgument, "values are 4 or 8 bytes");
+  if (warps < 1 || page_bytes < 256 || page_bytes % 16) throw Error(host::kInvalidArgument, "bad stream shape");
+  const int32_t n = plan.n, G = 32 / W;
+  StreamLayout out;
+  out.G = G;
+  out.warps = warps;
+  out.page_bytes = page_bytes;
+  out.load_scale.assign(n, 1.0);
+  // values written at value_bytes: double or float
+  auto put_values = [&](uint8_t *&p, const std::vector<double> &v) {
+    if (value_bytes == 8) {
+      put(p, v.data(), (int64_t)v.size());
+    } else {
+      std::vector<float> f(v.begin(), v.end());
+      put(p, f.data(), (int64_t)f.size());
+    }
+  };
+  const int64_t head = 16;
+  const int64_t slice_fixed = head + align16(4 * G) + align16((int64_t)value_bytes * G);
+  // entries per record so a chunk fits a page (both arrays padded to 16 bytes)
+  const int64_t slice_len_max = (page_bytes - slice_fixed - 32) / ((int64_t)G * (4 + value_bytes));
+  const int64_t split_fixed = head + 16 + 16;
+  const int64_t split_ent_max = ((page_bytes - split_fixed - 32) / (4 + value_bytes)) / G * G;
+  if (slice_len_max < 1 || split_ent_max < G) throw Error(host::kInvalidArgument, "pages too small for the tile width");
+
+  std::vector<std::unique_ptr<PageWriter>> writers;
+  std::vector<std::vector<uint8_t>> blobs(warps);
+  for (int32_t w = 0; w < warps; ++w) writers.emplace_back(new PageWriter(page_bytes, blobs[w]));
+
+  // A slice record (chunked): rows ks (positions of sweep s), entries q in [q0, q1)
+  auto emit_slice = [&](int32_t w, const Sweep<T> &s, const std::vector<int32_t> &ks, int32_t stage) {
+    int32_t len = 0;
+    for (int32_t k : ks) len = std::max(len, s.ptr[k + 1] - s.ptr[k]);
+    std::vector<int32_t> rows(G, n + 1);
+    std::vector<double> dinv(G, 0.0);
+    for (size_t g = 0; g < ks.size(); ++g) {
+      rows[g] = s.row[ks[g]];
+      dinv[g] = (double)std::real(s.dinv[ks[g]]);
+    }
+    int32_t q0 = 0;
+    do {
+      const int32_t q1 = (int32_t)std::min<int64_t>(len, q0 + slice_len_max);
+      const int32_t m = q1 - q0;
+      const int64_t bytes = slice_fixed + align16(4LL * m * G) + align16((int64_t)value_bytes * m * G);
+      uint8_t *p = writers[w]->reserve(bytes);
+      int32_t hdr[4] = {kRecordSlice, stage, m, (q0 == 0 ? kRecordFirst : 0) | (q1 == len ? kRecordLast : 0)};
+      put(p, hdr, 4);
+      put(p, rows.data(), G);
+      put_values(p, dinv);
+      std::vector<int32_t> col((size_t)m * G, n);
+      std::vector<double> val((size_t)m * G, 0.0);
+      for (int32_t q = q0; q < q1; ++q)
+        for (size_t g = 0; g < ks.size(); ++g) {
+          const int32_t k = ks[g];
+          if (q < s.ptr[k + 1] - s.ptr[k]) {
+            col[(size_t)(q - q0) * G + g] = s.col[s.ptr[k] + q];
+            val[(size_t)(q - q0) * G + g] = (double)std::real(s.val[s.ptr[k] + q]);
+          }
+        }
+      put(p, col.data(), (int64_t)col.size());
+      put_values(p, val);
+      ++out.records;
+      q0 = q1;
+    } while (q0 < len);
+  };
+  // A split-row record (chunked): one row's entries spread over the G lane groups
+  auto emit_split = [&](int32_t w, const Sweep<T> &s, int32_t k, int32_t stage) {
+    const int32_t len = s.ptr[k + 1] - s.ptr[k];
+    int32_t e0 = 0;
+    do {
+      const int32_t e1 = (int32_t)std::min<int64_t>(len, e0 + split_ent_max);
+      const int32_t m = (int32_t)(((e1 - e0) + G - 1) / G * G);
+      const int64_t bytes = split_fixed + align16(4LL * m) + align16((int64_t)value_bytes * m);
+      uint8_t *p = writers[w]->reserve(bytes);
+      int32_t hdr[4] = {kRecordSplit, stage, m, (e0 == 0 ? kRecordFirst : 0) | (e1 == len ? kRecordLast : 0)};
+      put(p, hdr, 4);
+      int32_t row[4] = {s.row[k], 0, 0, 0};
+      put(p, row, 4);
+      std::vector<double> dv(16 / value_bytes, 0.0);
+      dv[0] = (double)std::real(s.dinv[k]);
+      put_values(p, dv);
+      std::vector<int32_t> col(m, n);
+      std::vector<double> val(m, 0.0);
+      for (int32_t e = e0; e < e1; ++e) {
+        col[e - e0] = s.col[s.ptr[k] + e];
+        val[e - e0] = (double)std::real(s.val[s.ptr[k] + e]);
+      }
+      put(p, col.data(), m);
+      put_values(p, val);
+      ++out.records;
+      e0 = e1;
+    } while (e0 < len);
+  };
+  auto sorted_level = [](const Sweep<T> &s, int32_t l) {
+    std::vector<int32_t> ks;
+    for (int32_t k = s.level_ptr[l]; k < s.level_ptr[l + 1]; ++k) ks.push_back(k);
+    std::stable_sort(ks.begin(), ks.end(),
+                     [&](int32_t a, int32_t b) { return (s.ptr[a + 1] - s.ptr[a]) > (s.ptr[b + 1] - s.ptr[b]); });
+    return ks;
+  };
+  auto rows_of = [](const Sweep<T> &s, int32_t l) { return s.level_ptr[l + 1] - s.level_ptr[l]; };
+  // Narrow levels: the forward sweep's suffix and the backward sweep's prefix of levels with
+  // fewer than `narrow_rows` rows
+  const Sweep<T> &F = plan.fwd, &B = plan.bwd;
+  int32_t f_first_narrow = F.levels;
+  while (f_first_narrow > 1 && rows_of(F, f_first_narrow - 1) < narrow_rows) --f_first_narrow;
+  int32_t b_narrow = 0;
+  while (b_narrow < B.levels && rows_of(B, b_narrow) < narrow_rows) ++b_narrow;
+
+  // Forward level 0: no entries, folded into the load
+  if (F.levels > 0)
+    for (int32_t k = F.level_ptr[0]; k < F.level_ptr[1]; ++k) {
+      if (F.ptr[k + 1] != F.ptr[k]) throw Error(host::kInternal, "a level-0 row has entries");
+      out.load_scale[plan.in_row[F.row[k]]] = (double)std::real(F.dinv[k]);
+    }
+  int32_t stage = 0;
+  auto deal_level = [&](const Sweep<T> &s, int32_t l, int32_t st) {
+    const auto ks = sorted_level(s, l);
+    int32_t slice = 0;
+    for (size_t t0 = 0; t0 < ks.size(); t0 += G, ++slice) {
+      std::vector<int32_t> part(ks.begin() + t0, ks.begin() + std::min(ks.size(), t0 + (size_t)G));
+      emit_slice((slice + l) % warps, s, part, st);
+    }
+  };
+  // forward wide levels 1 .. f_first_narrow - 1
+  for (int32_t l = 1; l < f_first_narrow; ++l) {
+    deal_level(F, l, stage);
+    ++stage;
+    ++out.fwd_wide;
+  }
+  // narrow levels of both sweeps: warp 0
+  auto narrow_level = [&](const Sweep<T> &s, int32_t l, int32_t st) {
+    const auto ks = sorted_level(s, l);
+    if ((int32_t)ks.size() * 2 >= G) {
+      for (size_t t0 = 0; t0 < ks.size(); t0 += G) {
+        std::vector<int32_t> part(ks.begin() + t0, ks.begin() + std::min(ks.size(), t0 + (size_t)G));
+        emit_slice(0, s, part, st);
+      }
+    } else {
+      for (int32_t k : ks) emit_split(0, s, k, st);
+    }
+  };
+  for (int32_t l = std::max(f_first_narrow, 1); l < F.levels; ++l) {
+    narrow_level(F, l, stage);
+    out.fwd_narrow_rows += rows_of(F, l);
+  }
+  for (int32_t l = 0; l < b_narrow; ++l) {
+    narrow_level(B, l, stage);
+    out.bwd_narrow_rows += rows_of(B, l);
+  }
+  ++stage;
+  for (int32_t l = b_narrow; l < B.levels; ++l) {
+    deal_level(B, l, stage);
+    ++stage;
+    ++out.bwd_wide;
+  }
+  out.stages = stage;
+  out.warp_page.assign(1, 0);
+  for (int32_t w = 0; w < warps; ++w) {
+    writers[w]->close_page();
+    out.warp_page.push_back(out.warp_page.back() + writers[w]->pages);
+    out.blob.insert(out.blob.end(), blobs[w].begin(), blobs[w].end());
+  }
+  return out;
+}
+
+template StreamLayout stream_layout(const Plan<double> &, int32_t, int32_t, int32_t, int32_t, int32_t);
 
 }  // namespace yb

@@ -53,6 +53,33 @@ template <class T> struct SliceSweep {
 // Cuts `s` into slices of G rows for a factor of order n.
 template <class T> SliceSweep<T> slice_sweep(const Sweep<T> &s, int32_t n, int32_t G);
 
+// The factor of both sweeps as per-warp streams of records in fixed-size pages, for the streamed
+// tile solve. A record is a slice of up to G rows of one level (one row per lane group), or one
+// long row split over the lane groups, or a chunk of either (entries that do not fit one page
+// continue in the next record). Each record carries the number of block barriers that must have
+// passed before it runs (its stage). Levels with many rows ("wide") are dealt over all warps with a
+// block barrier after each; the narrow levels at the top of the tree, at the end of the forward
+// sweep and the start of the backward one, all go to warp 0, which takes them back to back with
+// only warp-level synchronisation. Forward rows with no entries need no record: the load of b
+// scales them by their diagonal (load_scale).
+struct StreamLayout {
+  int32_t G = 0, warps = 0, page_bytes = 0, stages = 0;
+  int32_t fwd_wide = 0, bwd_wide = 0, fwd_narrow_rows = 0, bwd_narrow_rows = 0;
+  int64_t records = 0;
+  std::vector<uint8_t> blob;        // pages of all warps
+  std::vector<int32_t> warp_page;   // [warps + 1] page ranges in the blob
+  std::vector<double> load_scale;   // [n] by row of b: the forward diagonal's reciprocal, or 1
+};
+
+enum RecordKind : int32_t { kRecordEnd = -1, kRecordSlice = 0, kRecordSplit = 1 };
+enum RecordFlags : int32_t { kRecordFirst = 1, kRecordLast = 2 };
+
+// Builds the streams of a plan's sweeps for values of `value_bytes` (8 or 4) and tile width W.
+template <class T> struct Plan;
+template <class T>
+StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, int32_t warps, int32_t page_bytes,
+                           int32_t narrow_rows);
+
 template <class T> struct Plan {
   int32_t n = 0;
   std::vector<int32_t> in_slot, out_slot;   // [n]

@@ -1,0 +1,220 @@
+// The streamed tile solve: a tile's working vector lives in shared memory, and each warp reads its
+// share of the factor as a stream of fixed-size pages that TMA bulk copies bring into a per-warp
+// shared-memory ring several pages ahead of use (see StreamLayout in plan.hpp).
+//
+// Shared memory of a block:
+//   Ys[(n + 2) * W]            the tile, slot-major; slot n stays zero, slot n + 1 absorbs padding
+//   ring[warps][S][page]       each warp's pages in flight
+//   full[warps][S]             one mbarrier per ring slot: the bulk copy's completion
+//
+// Lane 0 of a warp issues `cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes`
+// for page k + S once page k is consumed; the warp waits on the slot's mbarrier with
+// `mbarrier.try_wait.parity`, a bounded number of times (a wait that runs out sets the error word
+// and the kernel carries on to its end, so no barrier is left unmatched). A page's records are
+// walked in order: before a record of stage s the warp takes block barriers until s have passed;
+// slice records give each lane group a row, split records spread one row over the lane groups and
+// reduce with shuffles. The stream is the same for every tile, so the prefetch runs on from one
+// tile into the next.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device.cuh"
+#include "plan.hpp"
+
+namespace yb {
+
+struct StreamArgs {
+  int32_t n;
+  int64_t count, tiles;
+  const double *__restrict__ b;
+  int64_t ldb;
+  double *__restrict__ x;
+  int64_t ldx;
+  const int32_t *__restrict__ in_slot;
+  const int32_t *__restrict__ out_slot;
+  const void *__restrict__ load_scale;  // [n] T, by row of b
+  const uint8_t *__restrict__ blob;
+  const int32_t *__restrict__ warp_page;  // [warps + 1]
+  int32_t page_bytes, ring, stages;
+  int32_t *error;  // set to 1 if a wait ran out
+};
+
+constexpr long kWaitLimit = 1L << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void bulk_page(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for a slot's copy; gives up after kWaitLimit tries, recording the failure. Returns
+// whether the copy completed.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int32_t *error) {
+  long tries = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if (++tries >= kWaitLimit) {
+      atomicExch(error, 1);
+      return false;
+    }
+  }
+  return true;
+}
+
+// Orders this thread's earlier shared-memory accesses before later async-proxy (bulk copy) writes.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+template <class T, int W>
+__global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
+  static_assert(32 % W == 0, "W divides a warp");
+  constexpr int G = 32 / W;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int n = a.n;
+  T *Ys = reinterpret_cast<T *>(smem_raw);
+  const size_t y_bytes = (((size_t)(n + 2) * W * sizeof(T)) + 127) & ~(size_t)127;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  const int g = lane / W, c = lane % W;
+  const int S = a.ring, PB = a.page_bytes;
+  uint8_t *ring = smem_raw + y_bytes + (size_t)warp * S * PB;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + y_bytes + (size_t)warps * S * PB) + warp * S;
+  const T *scale = reinterpret_cast<const T *>(a.load_scale);
+
+  if (threadIdx.x < 2 * W) Ys[n * W + threadIdx.x] = T(0);
+  if (lane == 0)
+    for (int s = 0; s < S; ++s) mbar_init(full + s, 1);
+  mbar_fence_init();
+  __syncthreads();
+
+  const int p0 = __ldg(a.warp_page + warp), np = __ldg(a.warp_page + warp + 1) - p0;
+  const int64_t my_tiles = blockIdx.x < a.tiles ? (a.tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int64_t total_pages = (int64_t)np * my_tiles;
+  // Pages of this warp's stream, numbered across all its tiles: page k is stream page k % np
+  auto issue = [&](int64_t k) {
+    if (k < total_pages) {
+      fence_proxy_async();
+      const int slot = (int)(k % S);
+      bulk_page(ring + (size_t)slot * PB, a.blob + (size_t)(p0 + (int)(k % np)) * PB, (uint32_t)PB, full + slot);
+    }
+  };
+  if (lane == 0)
+    for (int64_t k = 0; k < S; ++k) issue(k);
+  __syncwarp();
+
+  int64_t k = 0;  // next page to consume
+  for (int64_t tile = blockIdx.x; tile < a.tiles; tile += gridDim.x) {
+    const int64_t col0 = tile * W;
+    // b's columns into slots, leaves (no forward entries) scaled by their diagonal
+#pragma unroll 1
+    for (int cc = 0; cc < W; ++cc) {
+      const int64_t col = col0 + cc;
+      if (col < a.count) {
+        const double *bc = a.b + col * a.ldb;
+#pragma unroll 8
+        for (int r = threadIdx.x; r < n; r += blockDim.x)
+          Ys[__ldg(a.in_slot + r) * W + cc] = (T)__ldg(bc + r) * __ldg(scale + r);
+      } else {
+        for (int r = threadIdx.x; r < n; r += blockDim.x) Ys[r * W + cc] = T(0);
+      }
+    }
+    __syncthreads();
+
+    int done = 0;
+    T acc = T(0);
+    for (int j = 0; j < np; ++j, ++k) {
+      const int slot = (int)(k % S);
+      const bool ready = mbar_wait_bounded(full + slot, (uint32_t)((k / S) & 1), a.error);
+      const uint8_t *page = ring + (size_t)slot * PB;
+      int pos = ready ? 0 : PB;  // a page that never arrived is skipped
+      while (pos + 16 <= PB) {
+        const int4 hdr = *reinterpret_cast<const int4 *>(page + pos);
+        const int kind = hdr.x, len = hdr.z, flags = hdr.w;
+        const int stage = min(hdr.y, a.stages);
+        if (kind < 0 || len < 0 || len > PB) break;
+        while (done < stage) {
+          __syncthreads();
+          ++done;
+        }
+        const uint8_t *body = page + pos + 16;
+        if (kind == kRecordSlice) {
+          const int32_t *rows = reinterpret_cast<const int32_t *>(body);
+          const T *dinv = reinterpret_cast<const T *>(body + ((4 * G + 15) & ~15));
+          const uint8_t *ent = body + ((4 * G + 15) & ~15) + ((sizeof(T) * G + 15) & ~15);
+          const int32_t *col = reinterpret_cast<const int32_t *>(ent);
+          const T *val = reinterpret_cast<const T *>(ent + ((4 * len * G + 15) & ~15));
+          const int row = rows[g];
+          if (flags & kRecordFirst) acc = Ys[row * W + c];
+          for (int q = 0; q < len; ++q) acc -= val[q * G + g] * Ys[col[q * G + g] * W + c];
+          if (flags & kRecordLast) Ys[row * W + c] = acc * dinv[g];
+          pos += 16 + ((4 * G + 15) & ~15) + ((sizeof(T) * G + 15) & ~15) + ((4 * len * G + 15) & ~15) +
+                 ((sizeof(T) * len * G + 15) & ~15);
+        } else {
+          const int row = *reinterpret_cast<const int32_t *>(body);
+          const T dinv = *reinterpret_cast<const T *>(body + 16);
+          const int32_t *col = reinterpret_cast<const int32_t *>(body + 32);
+          const T *val = reinterpret_cast<const T *>(body + 32 + ((4 * len + 15) & ~15));
+          T part = T(0);
+          for (int e = g; e < len; e += G) part += val[e] * Ys[col[e] * W + c];
+#pragma unroll
+          for (int off = W; off < 32; off <<= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+          if (flags & kRecordFirst) acc = Ys[row * W + c];
+          acc -= part;
+          if ((flags & kRecordLast) && g == 0) Ys[row * W + c] = acc * dinv;
+          pos += 48 + ((4 * len + 15) & ~15) + ((sizeof(T) * len + 15) & ~15);
+        }
+        __syncwarp();
+      }
+      __syncwarp();
+      if (lane == 0) issue(k + S);
+    }
+    while (done < a.stages) {
+      __syncthreads();
+      ++done;
+    }
+    // slots into x's columns
+#pragma unroll 1
+    for (int cc = 0; cc < W; ++cc) {
+      const int64_t col = col0 + cc;
+      if (col >= a.count) break;
+      double *xc = a.x + col * a.ldx;
+#pragma unroll 8
+      for (int r = threadIdx.x; r < n; r += blockDim.x) xc[r] = (double)Ys[__ldg(a.out_slot + r) * W + cc];
+    }
+    __syncthreads();
+  }
+  // Every copy issued was waited for above; after a wait that ran out, wait (bounded) for the
+  // last copy into each slot before the block's shared memory is released
+  if (lane == 0 && total_pages > 0) {
+    const int64_t first = total_pages > S ? total_pages - S : 0;
+    for (int64_t kk = first; kk < total_pages; ++kk) {
+      long tries = 0;
+      while (!mbar_try_wait(full + (kk % S), (uint32_t)((kk / S) & 1)) && ++tries < kWaitLimit) {
+      }
+    }
+  }
+}
+
+}  // namespace yb

@@ -175,6 +175,21 @@ class GpuFactor:
         """0 automatic, 1 shared-memory tile solve, 2 global-scratch tile solve."""
         _check(lib().yb_factor_set_tile_kind(self._h, precision, kind))
 
+    def set_stream(self, precision: int, warps: int = 8, ring: int = 4, page_bytes: int = 2048,
+                   narrow_rows: int = 0) -> None:
+        _check(lib().yb_factor_set_stream(self._h, precision, warps, ring, page_bytes, narrow_rows))
+
+    def stream_info(self, precision: int) -> dict:
+        w, st, nf, nb, nr = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        rec, by = C.c_int64(), C.c_int64()
+        _check(lib().yb_factor_stream_info(self._h, precision, C.byref(w), C.byref(st), C.byref(rec), C.byref(by),
+                                           C.byref(nf), C.byref(nb), C.byref(nr)))
+        return {"tile": w.value, "stages": st.value, "records": rec.value, "bytes": by.value,
+                "fwd_wide_levels": nf.value, "bwd_wide_levels": nb.value, "narrow_rows": nr.value}
+
+    def check_error(self) -> None:
+        _check(lib().yb_factor_check_error(self._h))
+
     def tile(self, precision: int) -> tuple[int, int, int]:
         w, t, b = C.c_int32(), C.c_int32(), C.c_int32()
         _check(lib().yb_factor_get_tile(self._h, precision, C.byref(w), C.byref(t), C.byref(b)))
