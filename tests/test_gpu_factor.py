@@ -54,6 +54,8 @@ def test_every_tile_width_and_block_size(gpu, kind, tile, threads):
 def test_streamed_solve_every_layout(gpu, tile, warps, ring, page, narrow):
     # small pages force chunked records; narrow=100000 puts every level on warp 0 (split rows),
     # narrow=1 none; 2,000 right-hand sides make several tiles per block at tile width 1
+    if tile == 1 and page < 1024:
+        pytest.skip("a 32-row slice needs pages of at least 1 KiB")
     chol = host.cholesky(random_spd(300, 3, 7))
     rhs = right_hand_sides(300, 37, 11)
     cpu = orc.solve_many(chol, rhs)

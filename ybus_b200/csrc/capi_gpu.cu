@@ -302,6 +302,14 @@ extern "C" int32_t yb_factor_set_stream(yb_factor *f, int32_t precision, int32_t
   });
 }
 
+extern "C" int32_t yb_factor_set_phase_clock(yb_factor *f, void *d_clock) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    f->phase_clock = (long long *)d_clock;
+    return YB_OK;
+  });
+}
+
 extern "C" int32_t yb_factor_check_error(yb_factor *f) {
   return guard([&] {
     require(f != nullptr, "null factor");
@@ -475,6 +483,7 @@ void launch_stream_w(yb_factor *f, StreamArgs a, const TileConfig &cfg, cudaStre
   a.ring = cfg.ring;
   a.stages = d->stages;
   a.error = f->error.get();
+  a.phase_clock = f->phase_clock;
   const size_t smem = stream_smem_bytes<T>(f, cfg, W);
   cuda_check(cudaFuncSetAttribute(stream_tile_kernel<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "cudaFuncSetAttribute");

@@ -88,6 +88,7 @@ struct yb_factor {
   // streamed layouts by shape (precision, width, warps, page bytes, narrow rows)
   std::map<std::tuple<int, int, int, int, int>, std::unique_ptr<yb::DeviceStream>> streams;
   yb::DeviceArray<int32_t> error;  // the device error word (a bounded wait that ran out)
+  long long *phase_clock = nullptr;  // diagnostics buffer of the caller's, or null
   yb::DeviceArray<double> scratch64;
   yb::DeviceArray<float> scratch32;
   yb::DeviceArray<double> dev_b, dev_x;

@@ -40,6 +40,9 @@ struct StreamArgs {
   const int32_t *__restrict__ warp_page;  // [warps + 1]
   int32_t page_bytes, ring, stages;
   int32_t *error;  // set to 1 if a wait ran out
+  // diagnostics: if set, block 0 records clock64() at phase boundaries of its first tiles:
+  // [tile][warp][mark], marks 0 load done, 1 first record, 2 stage-barrier entries..., see kernel
+  long long *phase_clock;
 };
 
 constexpr long kWaitLimit = 1L << 24;
@@ -141,6 +144,9 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
       }
     }
     __syncthreads();
+    const int64_t it = (tile - blockIdx.x) / gridDim.x;
+    long long *pc = (a.phase_clock && blockIdx.x == 0 && it < 4 && lane == 0) ? a.phase_clock + (it * 16 + warp) * 8 : nullptr;
+    if (pc) pc[0] = clock64();
 
     int done = 0;
     T acc = T(0);
@@ -157,6 +163,7 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
         while (done < stage) {
           __syncthreads();
           ++done;
+          if (pc && done < 6) pc[2 + done] = clock64();
         }
         const uint8_t *body = page + pos + 16;
         if (kind == kRecordSlice) {
@@ -190,10 +197,12 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
       __syncwarp();
       if (lane == 0) issue(k + S);
     }
+    if (pc) pc[1] = clock64();
     while (done < a.stages) {
       __syncthreads();
       ++done;
     }
+    if (pc) pc[2] = clock64();
     // slots into x's columns
 #pragma unroll 1
     for (int cc = 0; cc < W; ++cc) {
@@ -204,6 +213,7 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
       for (int r = threadIdx.x; r < n; r += blockDim.x) xc[r] = (double)Ys[__ldg(a.out_slot + r) * W + cc];
     }
     __syncthreads();
+    if (pc) pc[3] = clock64();
   }
   // Every copy issued was waited for above; after a wait that ran out, wait (bounded) for the
   // last copy into each slot before the block's shared memory is released
