@@ -147,6 +147,9 @@ int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int32_t kind);
  * which a level is taken by one warp alone (0: twice a slice's rows). */
 int32_t yb_factor_set_stream(yb_factor *f, int32_t precision, int32_t warps, int32_t ring,
                              int32_t page_bytes, int32_t narrow_rows);
+/* No ybus counterpart: the forward level from which the streamed solve takes the top of the tree
+ * as one dense block through its explicit inverse (-1: chosen from the factor, 0: none). */
+int32_t yb_factor_set_tail_level(yb_factor *f, int32_t precision, int32_t tail_level);
 /* No ybus counterpart: the streamed layout the automatic choice runs for a precision (building it
  * if needed); YB_ERROR_INVALID_ARGUMENT if that choice is not the streamed solve. */
 int32_t yb_factor_stream_info(yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *stages,

@@ -73,6 +73,26 @@ def test_streamed_solve_every_layout(gpu, tile, warps, ring, page, narrow):
     factor.check_error()
 
 
+@pytest.mark.parametrize("tile", [1, 2, 4, 8, 16])
+@pytest.mark.parametrize("tail_level", [-1, 0, 1, 2, 5])
+def test_dense_tail_block(gpu, tile, tail_level):
+    # the top of the tree solved as one block by its explicit inverse, from level 1 (nearly the
+    # whole factor) to none, Cholesky (backward block too) and LU (where it may not close)
+    chol = host.cholesky(random_spd(300, 3, 7))
+    lu = host.lu(random_square(250, 4, 3))
+    for f, n in ((chol, 300), (lu, 250)):
+        rhs = right_hand_sides(n, 45, 11)
+        cpu = orc.solve_many(f, rhs)
+        factor = upload(gpu, f)
+        factor.set_tile(FP64, tile, 256, 1)
+        factor.set_tile_kind(FP64, STREAM)
+        factor.set_stream(FP64, 8, 4, 2048, 0)
+        factor.set_tail_level(FP64, tail_level)
+        d = worst_relative_difference(factor.solve_many(rhs), cpu)
+        assert d < BAR, f"tile {tile} tail {tail_level}: {d:e}"
+        factor.check_error()
+
+
 @pytest.mark.parametrize("kind", [SHARED, GLOBAL, STREAM])
 def test_lu_with_every_tile_solve(gpu, kind):
     lu = host.lu(random_square(250, 4, 3))

@@ -75,6 +75,7 @@ SIGNATURES: dict[str, tuple] = {
     "yb_factor_stream_info": (i32, [vp, i32, P_i32, P_i32, P_i64, P_i64, P_i32, P_i32, P_i32]),
     "yb_factor_check_error": (i32, [vp]),
     "yb_factor_set_phase_clock": (i32, [vp, vp]),
+    "yb_factor_set_tail_level": (i32, [vp, i32, i32]),
     "yb_solve_many": (i32, [vp, vp, i64, vp]),
     "yb_solve_many_device": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
 }

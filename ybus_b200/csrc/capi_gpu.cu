@@ -302,6 +302,16 @@ extern "C" int32_t yb_factor_set_stream(yb_factor *f, int32_t precision, int32_t
   });
 }
 
+extern "C" int32_t yb_factor_set_tail_level(yb_factor *f, int32_t precision, int32_t tail_level) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(tail_level >= -1, "the tail level is -1 (chosen), 0 (none) or a forward level");
+    (precision == YB_FP64 ? f->tile64 : f->tile32).tail_level = tail_level;
+    return YB_OK;
+  });
+}
+
 extern "C" int32_t yb_factor_set_phase_clock(yb_factor *f, void *d_clock) {
   return guard([&] {
     require(f != nullptr, "null factor");
@@ -436,9 +446,32 @@ void launch_smem(yb_factor *f, SmemArgs<T> a, const TileConfig &cfg, cudaStream_
   }
 }
 
+// The dense tail's first level: the shallowest forward level whose rows and above number at most
+// kTailRows (dense inverse entries grow as the square), or 0 for none.
+constexpr int kTailRows = 400;
+int32_t tail_level_for(const yb_factor *f, const TileConfig &cfg) {
+  if (cfg.tail_level >= 0) return cfg.tail_level;
+  const auto &F = f->plan.fwd;
+  int32_t level = F.levels, rows = 0;
+  while (level > 1 && rows + (F.level_ptr[level] - F.level_ptr[level - 1]) <= kTailRows) {
+    rows += F.level_ptr[level] - F.level_ptr[level - 1];
+    --level;
+  }
+  // worth it only when it removes a good number of levels
+  return (F.levels - level >= 8) ? level : 0;
+}
+
+int32_t tail_rows_for(const yb_factor *f, int32_t level) {
+  if (level <= 0 || level >= f->plan.fwd.levels) return 0;
+  return f->plan.fwd.level_ptr[f->plan.fwd.levels] - f->plan.fwd.level_ptr[level];
+}
+
 template <class T> size_t stream_smem_bytes(const yb_factor *f, const TileConfig &cfg, int W) {
   const size_t y = (((size_t)(f->n + 2) * W * sizeof(T)) + 127) & ~(size_t)127;
-  return y + (size_t)cfg.stream_warps * cfg.ring * cfg.page_bytes + (size_t)cfg.stream_warps * cfg.ring * 8;
+  const int m = tail_rows_for(f, tail_level_for(f, cfg));
+  const size_t tb = (((size_t)(m + 1) * W * sizeof(T)) + 15) & ~(size_t)15;
+  const size_t ts = (((size_t)(m + 1) * 4) + 127) & ~(size_t)127;
+  return y + tb + ts + (size_t)cfg.stream_warps * cfg.ring * cfg.page_bytes + (size_t)cfg.stream_warps * cfg.ring * 8;
 }
 
 template <class T> bool stream_fits(const yb_factor *f, const TileConfig &cfg, int W) {
@@ -447,10 +480,12 @@ template <class T> bool stream_fits(const yb_factor *f, const TileConfig &cfg, i
 
 template <class T> DeviceStream *stream_for(yb_factor *f, const TileConfig &cfg, int W, cudaStream_t stream) {
   const int narrow = cfg.narrow_rows > 0 ? cfg.narrow_rows : 2 * (32 / W);
-  const auto key = std::make_tuple((int)sizeof(T), W, cfg.stream_warps, cfg.page_bytes, narrow);
+  const int tail_level = tail_level_for(f, cfg);
+  const auto key = std::make_tuple((int)sizeof(T), W, cfg.stream_warps, cfg.page_bytes, narrow, tail_level);
   auto it = f->streams.find(key);
   if (it != f->streams.end()) return it->second.get();
-  const StreamLayout lay = stream_layout(f->plan, W, (int)sizeof(T), cfg.stream_warps, cfg.page_bytes, narrow);
+  const StreamLayout lay =
+      stream_layout(f->plan, W, (int)sizeof(T), cfg.stream_warps, cfg.page_bytes, narrow, tail_level);
   auto d = std::make_unique<DeviceStream>();
   d->stages = lay.stages;
   d->G = lay.G;
@@ -466,6 +501,8 @@ template <class T> DeviceStream *stream_for(yb_factor *f, const TileConfig &cfg,
     std::memcpy(scale.data() + i * sizeof(T), &v, sizeof(T));
   }
   d->load_scale.upload(scale, stream);
+  d->tail = lay.tail;
+  d->tail_slot.upload(lay.tail_slot.empty() ? std::vector<int32_t>{0} : lay.tail_slot, stream);
   cuda_check(cudaStreamSynchronize(stream), "stream layout upload");
   auto *out = d.get();
   f->streams.emplace(key, std::move(d));
@@ -482,6 +519,8 @@ void launch_stream_w(yb_factor *f, StreamArgs a, const TileConfig &cfg, cudaStre
   a.page_bytes = cfg.page_bytes;
   a.ring = cfg.ring;
   a.stages = d->stages;
+  a.tail = d->tail;
+  a.tail_slot = d->tail_slot.get();
   a.error = f->error.get();
   a.phase_clock = f->phase_clock;
   const size_t smem = stream_smem_bytes<T>(f, cfg, W);

@@ -50,6 +50,7 @@ struct TileConfig {
   // the streamed solve's shape: warps per block, pages in flight per warp, page bytes, and the
   // row count under which a level goes to warp 0 (0: twice the rows of a slice)
   int stream_warps = 8, ring = 4, page_bytes = 2048, narrow_rows = 0;
+  int tail_level = -1;  // forward level from which rows form the dense tail (0: none, -1: chosen)
 };
 
 // A streamed layout on the device (StreamLayout in plan.hpp).
@@ -60,6 +61,8 @@ struct DeviceStream {
   DeviceArray<uint8_t> blob;
   DeviceArray<int32_t> warp_page;
   DeviceArray<uint8_t> load_scale;
+  int32_t tail = 0;
+  DeviceArray<int32_t> tail_slot;
 };
 
 // A sliced sweep on the device (SliceSweep in plan.hpp), at value type T.
@@ -86,7 +89,7 @@ struct yb_factor {
   std::map<int, std::unique_ptr<yb::DeviceSlices<double>[]>> slices64;
   std::map<int, std::unique_ptr<yb::DeviceSlices<float>[]>> slices32;
   // streamed layouts by shape (precision, width, warps, page bytes, narrow rows)
-  std::map<std::tuple<int, int, int, int, int>, std::unique_ptr<yb::DeviceStream>> streams;
+  std::map<std::tuple<int, int, int, int, int, int>, std::unique_ptr<yb::DeviceStream>> streams;
   yb::DeviceArray<int32_t> error;  // the device error word (a bounded wait that ran out)
   long long *phase_clock = nullptr;  // diagnostics buffer of the caller's, or null
   yb::DeviceArray<double> scratch64;

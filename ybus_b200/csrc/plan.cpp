@@ -236,7 +236,7 @@ template <class V> void put(uint8_t *&p, const V *v, int64_t count) {
 
 template <class T>
 StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, int32_t warps, int32_t page_bytes,
-                           int32_t narrow_rows) {
+                           int32_t narrow_rows, int32_t tail_level) {
   if (W < 1 || W > 32 || 32 % W) throw Error(host::kInvalidArgument, "tile width must divide 32");
   if (value_bytes != 8 && value_bytes != 4) throw Error(host::kInvalidArgument, "values are 4 or 8 bytes");
   if (warps < 1 || page_bytes < 256 || page_bytes % 16) throw Error(host::kInvalidArgument, "bad stream shape");
@@ -267,23 +267,42 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
   std::vector<std::vector<uint8_t>> blobs(warps);
   for (int32_t w = 0; w < warps; ++w) writers.emplace_back(new PageWriter(page_bytes, blobs[w]));
 
-  // A slice record (chunked): rows ks (positions of sweep s), entries q in [q0, q1)
-  auto emit_slice = [&](int32_t w, const Sweep<T> &s, const std::vector<int32_t> &ks, int32_t stage) {
+  // Entries of position k of sweep s that a record takes: all, or (for the tail's partial sums)
+  // only those in columns outside the tail
+  std::vector<char> in_tail(n, 0);
+  auto entries_of = [&](const Sweep<T> &s, int32_t k, bool outside_tail) {
+    std::vector<int32_t> ps;
+    for (int32_t p = s.ptr[k]; p < s.ptr[k + 1]; ++p)
+      if (!outside_tail || !in_tail[s.col[p]]) ps.push_back(p);
+    return ps;
+  };
+  // A slice record (chunked): rows ks (positions of sweep s). to_tail: rows become tail indices
+  // `tail_index[g]`, only entries outside the tail are taken and the result is left unscaled.
+  auto emit_slice = [&](int32_t w, const Sweep<T> &s, const std::vector<int32_t> &ks, int32_t stage,
+                        const std::vector<int32_t> *tail_index = nullptr) {
+    const bool to_tail = tail_index != nullptr;
+    std::vector<std::vector<int32_t>> ents;
     int32_t len = 0;
-    for (int32_t k : ks) len = std::max(len, s.ptr[k + 1] - s.ptr[k]);
-    std::vector<int32_t> rows(G, n + 1);
+    for (int32_t k : ks) {
+      ents.push_back(entries_of(s, k, to_tail));
+      len = std::max(len, (int32_t)ents.back().size());
+    }
+    std::vector<int32_t> rows(G, to_tail ? 0 : n + 1);
     std::vector<double> dinv(G, 0.0);
     for (size_t g = 0; g < ks.size(); ++g) {
-      rows[g] = s.row[ks[g]];
-      dinv[g] = (double)std::real(s.dinv[ks[g]]);
+      rows[g] = to_tail ? (*tail_index)[g] : s.row[ks[g]];
+      dinv[g] = to_tail ? 1.0 : (double)std::real(s.dinv[ks[g]]);
     }
+    if (to_tail)  // padded rows of a tail record accumulate nothing into a spare tail entry
+      for (size_t g = ks.size(); g < (size_t)G; ++g) rows[g] = out.tail;
     int32_t q0 = 0;
     do {
       const int32_t q1 = (int32_t)std::min<int64_t>(len, q0 + slice_len_max);
       const int32_t m = q1 - q0;
       const int64_t bytes = slice_fixed + align16(4LL * m * G) + align16((int64_t)value_bytes * m * G);
       uint8_t *p = writers[w]->reserve(bytes);
-      int32_t hdr[4] = {kRecordSlice, stage, m, (q0 == 0 ? kRecordFirst : 0) | (q1 == len ? kRecordLast : 0)};
+      int32_t hdr[4] = {kRecordSlice, stage, m,
+                        (q0 == 0 ? kRecordFirst : 0) | (q1 == len ? kRecordLast : 0) | (to_tail ? kRecordToTail : 0)};
       put(p, hdr, 4);
       put(p, rows.data(), G);
       put_values(p, dinv);
@@ -291,10 +310,10 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
       std::vector<double> val((size_t)m * G, 0.0);
       for (int32_t q = q0; q < q1; ++q)
         for (size_t g = 0; g < ks.size(); ++g) {
-          const int32_t k = ks[g];
-          if (q < s.ptr[k + 1] - s.ptr[k]) {
-            col[(size_t)(q - q0) * G + g] = s.col[s.ptr[k] + q];
-            val[(size_t)(q - q0) * G + g] = (double)std::real(s.val[s.ptr[k] + q]);
+          if (q < (int32_t)ents[g].size()) {
+            const int32_t pp = ents[g][q];
+            col[(size_t)(q - q0) * G + g] = s.col[pp];
+            val[(size_t)(q - q0) * G + g] = (double)std::real(s.val[pp]);
           }
         }
       put(p, col.data(), (int64_t)col.size());
@@ -302,6 +321,35 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
       ++out.records;
       q0 = q1;
     } while (q0 < len);
+  };
+  // A copy marker: the warp copies its share of the tail's slots into the tail buffer
+  auto emit_marker = [&](int32_t w, int32_t kind, int32_t stage, int32_t sweep) {
+    uint8_t *p = writers[w]->reserve(16);
+    int32_t hdr[4] = {kind, stage, sweep, 0};
+    put(p, hdr, 4);
+    ++out.records;
+  };
+  // Dense rows of a tail inverse (chunked): row t, columns [j0, j0 + count) of `inv`, where
+  // packed(t, j) gives a value's index; the product with the tail buffer goes to t's slot
+  const int64_t dense_fixed = head + 16;
+  const int64_t dense_max = (page_bytes - dense_fixed - 16) / value_bytes / 4 * 4;
+  auto emit_dense_row = [&](int32_t w, const std::vector<double> &inv, int32_t t, int32_t j_first, int32_t count,
+                            auto packed, int32_t stage) {
+    int32_t e0 = 0;
+    do {
+      const int32_t e1 = (int32_t)std::min<int64_t>(count, e0 + dense_max);
+      const int32_t m = e1 - e0;
+      uint8_t *p = writers[w]->reserve(dense_fixed + align16((int64_t)value_bytes * m));
+      int32_t hdr[4] = {kRecordDense, stage, m, (e0 == 0 ? kRecordFirst : 0) | (e1 == count ? kRecordLast : 0)};
+      put(p, hdr, 4);
+      int32_t where[4] = {t, j_first + e0, 0, 0};
+      put(p, where, 4);
+      std::vector<double> v(m);
+      for (int32_t e = e0; e < e1; ++e) v[e - e0] = inv[packed(t, j_first + e)];
+      put_values(p, v);
+      ++out.records;
+      e0 = e1;
+    } while (e0 < count);
   };
   // A split-row record (chunked): one row's entries spread over the G lane groups
   auto emit_split = [&](int32_t w, const Sweep<T> &s, int32_t k, int32_t stage) {
@@ -339,13 +387,79 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
     return ks;
   };
   auto rows_of = [](const Sweep<T> &s, int32_t l) { return s.level_ptr[l + 1] - s.level_ptr[l]; };
-  // Narrow levels: the forward sweep's suffix and the backward sweep's prefix of levels with
-  // fewer than `narrow_rows` rows
   const Sweep<T> &F = plan.fwd, &B = plan.bwd;
-  int32_t f_first_narrow = F.levels;
-  while (f_first_narrow > 1 && rows_of(F, f_first_narrow - 1) < narrow_rows) --f_first_narrow;
-  int32_t b_narrow = 0;
-  while (b_narrow < B.levels && rows_of(B, b_narrow) < narrow_rows) ++b_narrow;
+  // The dense tail: rows at forward level >= tail_level
+  const bool dense_tail = tail_level > 0 && tail_level < F.levels;
+  std::vector<int32_t> tail_index(n, -1);
+  if (dense_tail) {
+    for (int32_t i = 0; i < n; ++i)
+      if (F.level_of[i] >= tail_level) {
+        tail_index[i] = (int32_t)out.tail_slot.size();
+        out.tail_slot.push_back(i);
+        in_tail[i] = 1;
+      }
+    out.tail = (int32_t)out.tail_slot.size();
+    // Backward closure: every upper-triangle dependency of a tail row is a tail row
+    out.tail_backward = true;
+    for (int32_t k = 0; k < n && out.tail_backward; ++k)
+      if (in_tail[B.row[k]])
+        for (int32_t p = B.ptr[k]; p < B.ptr[k + 1]; ++p)
+          if (!in_tail[B.col[p]]) {
+            out.tail_backward = false;
+            break;
+          }
+    // L_TT and U_TT (dense, in tail order, diagonal included) and their inverses in FP64
+    const int32_t m = out.tail;
+    std::vector<double> Lt((size_t)m * m, 0.0), Ut((size_t)m * m, 0.0);
+    for (int32_t k = 0; k < n; ++k) {
+      const int32_t i = F.row[k];
+      if (!in_tail[i]) continue;
+      const int32_t a = tail_index[i];
+      Lt[(size_t)a * m + a] = 1.0 / (double)std::real(F.dinv[k]);
+      for (int32_t p = F.ptr[k]; p < F.ptr[k + 1]; ++p)
+        if (in_tail[F.col[p]]) Lt[(size_t)a * m + tail_index[F.col[p]]] = (double)std::real(F.val[p]);
+    }
+    // inverse of a lower triangle by columns: solve L z = e_c
+    out.fwd_inv.assign((size_t)m * (m + 1) / 2, 0.0);
+    std::vector<double> z(m);
+    for (int32_t col = 0; col < m; ++col) {
+      std::fill(z.begin(), z.end(), 0.0);
+      for (int32_t i = col; i < m; ++i) {
+        double acc = (i == col) ? 1.0 : 0.0;
+        for (int32_t j = col; j < i; ++j) acc -= Lt[(size_t)i * m + j] * z[j];
+        z[i] = acc / Lt[(size_t)i * m + i];
+        out.fwd_inv[(size_t)i * (i + 1) / 2 + col] = z[i];
+      }
+    }
+    if (out.tail_backward) {
+      for (int32_t k = 0; k < n; ++k) {
+        const int32_t i = B.row[k];
+        if (!in_tail[i]) continue;
+        const int32_t a = tail_index[i];
+        Ut[(size_t)a * m + a] = 1.0 / (double)std::real(B.dinv[k]);
+        for (int32_t p = B.ptr[k]; p < B.ptr[k + 1]; ++p) Ut[(size_t)a * m + tail_index[B.col[p]]] = (double)std::real(B.val[p]);
+      }
+      // inverse of an upper triangle by columns: solve U z = e_c, rows from the last
+      out.bwd_inv.assign((size_t)m * (m + 1) / 2, 0.0);
+      auto up = [m](int32_t i, int32_t j) { return (size_t)i * m - (size_t)i * (i - 1) / 2 + (j - i); };
+      for (int32_t col = m - 1; col >= 0; --col) {
+        std::fill(z.begin(), z.end(), 0.0);
+        for (int32_t i = col; i >= 0; --i) {
+          double acc = (i == col) ? 1.0 : 0.0;
+          for (int32_t j = i + 1; j <= col; ++j) acc -= Ut[(size_t)i * m + j] * z[j];
+          z[i] = acc / Ut[(size_t)i * m + i];
+          out.bwd_inv[up(i, col)] = z[i];
+        }
+      }
+    }
+  }
+  // Narrow levels (taken by warp 0 alone): without a dense tail, the forward sweep's suffix of
+  // levels with fewer than `narrow_rows` rows; the backward sweep's prefix likewise
+  int32_t f_end = F.levels;  // forward levels handled by level (the rest are the tail)
+  if (dense_tail) f_end = tail_level;
+  int32_t f_first_narrow = f_end;
+  if (!dense_tail)
+    while (f_first_narrow > 1 && rows_of(F, f_first_narrow - 1) < narrow_rows) --f_first_narrow;
 
   // Forward level 0: no entries, folded into the load
   if (F.levels > 0)
@@ -354,45 +468,108 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
       out.load_scale[plan.in_row[F.row[k]]] = (double)std::real(F.dinv[k]);
     }
   int32_t stage = 0;
-  auto deal_level = [&](const Sweep<T> &s, int32_t l, int32_t st) {
-    const auto ks = sorted_level(s, l);
+  auto deal = [&](const Sweep<T> &s, std::vector<int32_t> ks, int32_t st, int32_t rot,
+                  const std::vector<int32_t> *tails = nullptr) {
+    std::stable_sort(ks.begin(), ks.end(),
+                     [&](int32_t a, int32_t b) { return (s.ptr[a + 1] - s.ptr[a]) > (s.ptr[b + 1] - s.ptr[b]); });
     int32_t slice = 0;
     for (size_t t0 = 0; t0 < ks.size(); t0 += G, ++slice) {
       std::vector<int32_t> part(ks.begin() + t0, ks.begin() + std::min(ks.size(), t0 + (size_t)G));
-      emit_slice((slice + l) % warps, s, part, st);
+      if (tails) {
+        std::vector<int32_t> ti;
+        for (int32_t k : part) ti.push_back(tail_index[s.row[k]]);
+        emit_slice((slice + rot) % warps, s, part, st, &ti);
+      } else {
+        emit_slice((slice + rot) % warps, s, part, st);
+      }
     }
   };
-  // forward wide levels 1 .. f_first_narrow - 1
+  auto level_positions = [](const Sweep<T> &s, int32_t l) {
+    std::vector<int32_t> ks;
+    for (int32_t k = s.level_ptr[l]; k < s.level_ptr[l + 1]; ++k) ks.push_back(k);
+    return ks;
+  };
+  // forward levels 1 .. f_first_narrow - 1, a barrier after each
   for (int32_t l = 1; l < f_first_narrow; ++l) {
-    deal_level(F, l, stage);
+    deal(F, level_positions(F, l), stage, l);
     ++stage;
     ++out.fwd_wide;
   }
-  // narrow levels of both sweeps: warp 0
-  auto narrow_level = [&](const Sweep<T> &s, int32_t l, int32_t st) {
-    const auto ks = sorted_level(s, l);
-    if ((int32_t)ks.size() * 2 >= G) {
-      for (size_t t0 = 0; t0 < ks.size(); t0 += G) {
-        std::vector<int32_t> part(ks.begin() + t0, ks.begin() + std::min(ks.size(), t0 + (size_t)G));
-        emit_slice(0, s, part, st);
-      }
-    } else {
-      for (int32_t k : ks) emit_split(0, s, k, st);
-    }
-  };
-  for (int32_t l = std::max(f_first_narrow, 1); l < F.levels; ++l) {
-    narrow_level(F, l, stage);
-    out.fwd_narrow_rows += rows_of(F, l);
-  }
-  for (int32_t l = 0; l < b_narrow; ++l) {
-    narrow_level(B, l, stage);
-    out.bwd_narrow_rows += rows_of(B, l);
-  }
-  ++stage;
-  for (int32_t l = b_narrow; l < B.levels; ++l) {
-    deal_level(B, l, stage);
+  if (dense_tail) {
+    // r_T = b_T - L_TB y_B into the tail buffer, then y_T = L_TT^-1 r_T into the slots
+    std::vector<int32_t> ks;
+    for (int32_t l = tail_level; l < F.levels; ++l)
+      for (int32_t k = F.level_ptr[l]; k < F.level_ptr[l + 1]; ++k) ks.push_back(k);
+    deal(F, ks, stage, 0, &ks);
     ++stage;
-    ++out.bwd_wide;
+    const int32_t m = out.tail;
+    auto lower_at = [](int32_t i, int32_t j) { return (size_t)i * (i + 1) / 2 + j; };
+    for (int32_t t = 0; t < m; ++t) emit_dense_row((t / 1) % warps, out.fwd_inv, t, 0, t + 1, lower_at, stage);
+    ++stage;
+    out.fwd_narrow_rows = out.tail;
+  } else {
+    auto narrow_level = [&](const Sweep<T> &s, int32_t l, int32_t st) {
+      const auto ks = sorted_level(s, l);
+      if ((int32_t)ks.size() * 2 >= G) {
+        for (size_t t0 = 0; t0 < ks.size(); t0 += G) {
+          std::vector<int32_t> part(ks.begin() + t0, ks.begin() + std::min(ks.size(), t0 + (size_t)G));
+          emit_slice(0, s, part, st);
+        }
+      } else {
+        for (int32_t k : ks) emit_split(0, s, k, st);
+      }
+    };
+    for (int32_t l = std::max(f_first_narrow, 1); l < F.levels; ++l) {
+      narrow_level(F, l, stage);
+      out.fwd_narrow_rows += rows_of(F, l);
+    }
+    // the backward prefix of narrow levels joins warp 0's run
+    int32_t b_narrow = 0;
+    while (b_narrow < B.levels && rows_of(B, b_narrow) < narrow_rows) ++b_narrow;
+    for (int32_t l = 0; l < b_narrow; ++l) {
+      narrow_level(B, l, stage);
+      out.bwd_narrow_rows += rows_of(B, l);
+    }
+    ++stage;
+    for (int32_t l = b_narrow; l < B.levels; ++l) {
+      deal(B, level_positions(B, l), stage, l);
+      ++stage;
+      ++out.bwd_wide;
+    }
+  }
+  if (dense_tail) {
+    std::vector<char> done_b(n, 0);
+    if (out.tail_backward) {
+      // x_T = U_TT^-1 y_T: copy y_T to the tail buffer, then the product into the slots
+      for (int32_t w = 0; w < warps; ++w) emit_marker(w, kRecordCopy, stage, 1);
+      ++stage;
+      const int32_t m = out.tail;
+      auto upper_at = [m](int32_t i, int32_t j) { return (size_t)i * m - (size_t)i * (i - 1) / 2 + (j - i); };
+      for (int32_t t = 0; t < m; ++t) emit_dense_row(t % warps, out.bwd_inv, t, t, m - t, upper_at, stage);
+      ++stage;
+      for (int32_t i = 0; i < n; ++i) done_b[i] = in_tail[i];
+      out.bwd_narrow_rows = out.tail;
+    }
+    // the remaining backward rows by levels counted over rows not yet done
+    std::vector<int32_t> lev(n, -1);
+    int32_t levels = 0;
+    for (int32_t k = 0; k < n; ++k) {  // B's positions are in topological order (level order)
+      const int32_t i = B.row[k];
+      if (done_b[i]) continue;
+      int32_t l = 0;
+      for (int32_t p = B.ptr[k]; p < B.ptr[k + 1]; ++p)
+        if (!done_b[B.col[p]]) l = std::max(l, lev[B.col[p]] + 1);
+      lev[i] = l;
+      levels = std::max(levels, l + 1);
+    }
+    std::vector<std::vector<int32_t>> by_level(levels);
+    for (int32_t k = 0; k < n; ++k)
+      if (!done_b[B.row[k]]) by_level[lev[B.row[k]]].push_back(k);
+    for (int32_t l = 0; l < levels; ++l) {
+      deal(B, by_level[l], stage, l);
+      ++stage;
+      ++out.bwd_wide;
+    }
   }
   out.stages = stage;
   out.warp_page.assign(1, 0);
@@ -404,6 +581,6 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
   return out;
 }
 
-template StreamLayout stream_layout(const Plan<double> &, int32_t, int32_t, int32_t, int32_t, int32_t);
+template StreamLayout stream_layout(const Plan<double> &, int32_t, int32_t, int32_t, int32_t, int32_t, int32_t);
 
 }  // namespace yb

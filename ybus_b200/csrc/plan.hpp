@@ -62,23 +62,37 @@ template <class T> SliceSweep<T> slice_sweep(const Sweep<T> &s, int32_t n, int32
 // sweep and the start of the backward one, all go to warp 0, which takes them back to back with
 // only warp-level synchronisation. Forward rows with no entries need no record: the load of b
 // scales them by their diagonal (load_scale).
+//
+// With a dense tail (tail_level K > 0), the rows T at forward levels K and above (the top of the
+// tree: every row that depends on a T row is in T) are solved as a block: forward, r_T = b_T −
+// L_TB y_B for all T rows at once, then y_T = L_TT⁻¹ r_T; backward (when T is closed under the
+// upper triangle's dependencies, as it is for a Cholesky factor), x_T = U_TT⁻¹ y_T first, then the
+// remaining rows by their levels counted without T. The inverses are computed here in FP64 and
+// applied as dense triangular matrix-vector products, which take one stage each instead of one
+// per level of the chain of narrow levels at the top of the tree.
 struct StreamLayout {
   int32_t G = 0, warps = 0, page_bytes = 0, stages = 0;
   int32_t fwd_wide = 0, bwd_wide = 0, fwd_narrow_rows = 0, bwd_narrow_rows = 0;
   int64_t records = 0;
+  int32_t tail = 0;                 // |T|, 0 for no dense tail
+  bool tail_backward = false;       // the backward sweep also takes T densely
+  std::vector<int32_t> tail_slot;   // [tail] the slot of each T row, increasing
+  std::vector<double> fwd_inv;      // packed lower triangle of L_TT⁻¹, row-major
+  std::vector<double> bwd_inv;      // packed upper triangle of U_TT⁻¹, row-major
   std::vector<uint8_t> blob;        // pages of all warps
   std::vector<int32_t> warp_page;   // [warps + 1] page ranges in the blob
   std::vector<double> load_scale;   // [n] by row of b: the forward diagonal's reciprocal, or 1
 };
 
-enum RecordKind : int32_t { kRecordEnd = -1, kRecordSlice = 0, kRecordSplit = 1 };
-enum RecordFlags : int32_t { kRecordFirst = 1, kRecordLast = 2 };
+enum RecordKind : int32_t { kRecordEnd = -1, kRecordSlice = 0, kRecordSplit = 1, kRecordDense = 2, kRecordCopy = 3 };
+// kRecordToTail: a slice whose rows are tail indices; its results (unscaled) go to the tail buffer
+enum RecordFlags : int32_t { kRecordFirst = 1, kRecordLast = 2, kRecordToTail = 4 };
 
 // Builds the streams of a plan's sweeps for values of `value_bytes` (8 or 4) and tile width W.
 template <class T> struct Plan;
 template <class T>
 StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, int32_t warps, int32_t page_bytes,
-                           int32_t narrow_rows);
+                           int32_t narrow_rows, int32_t tail_level = 0);
 
 template <class T> struct Plan {
   int32_t n = 0;

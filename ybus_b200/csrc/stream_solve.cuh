@@ -39,6 +39,8 @@ struct StreamArgs {
   const uint8_t *__restrict__ blob;
   const int32_t *__restrict__ warp_page;  // [warps + 1]
   int32_t page_bytes, ring, stages;
+  int32_t tail;                           // rows of the dense tail (0: none)
+  const int32_t *__restrict__ tail_slot;  // [tail] their slots
   int32_t *error;  // set to 1 if a wait ran out
   // diagnostics: if set, block 0 records clock64() at phase boundaries of its first tiles:
   // [tile][warp][mark], marks 0 load done, 1 first record, 2 stage-barrier entries..., see kernel
@@ -102,11 +104,19 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
   const int g = lane / W, c = lane % W;
   const int S = a.ring, PB = a.page_bytes;
-  uint8_t *ring = smem_raw + y_bytes + (size_t)warp * S * PB;
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + y_bytes + (size_t)warps * S * PB) + warp * S;
+  // the dense tail's buffer (tail + 1 rows) and slots (tail + 1: the spare maps to the zero slot)
+  const int m = a.tail;
+  T *Tb = reinterpret_cast<T *>(smem_raw + y_bytes);
+  const size_t tb_bytes = (((size_t)(m + 1) * W * sizeof(T)) + 15) & ~(size_t)15;
+  int32_t *tslot = reinterpret_cast<int32_t *>(smem_raw + y_bytes + tb_bytes);
+  const size_t ts_bytes = (((size_t)(m + 1) * 4) + 127) & ~(size_t)127;
+  uint8_t *ring = smem_raw + y_bytes + tb_bytes + ts_bytes + (size_t)warp * S * PB;
+  uint64_t *full =
+      reinterpret_cast<uint64_t *>(smem_raw + y_bytes + tb_bytes + ts_bytes + (size_t)warps * S * PB) + warp * S;
   const T *scale = reinterpret_cast<const T *>(a.load_scale);
 
   if (threadIdx.x < 2 * W) Ys[n * W + threadIdx.x] = T(0);
+  for (int t = threadIdx.x; t <= m; t += blockDim.x) tslot[t] = t < m ? __ldg(a.tail_slot + t) : n;
   if (lane == 0)
     for (int s = 0; s < S; ++s) mbar_init(full + s, 1);
   mbar_fence_init();
@@ -150,6 +160,9 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
 
     int done = 0;
     T acc = T(0);
+    T dacc[W];
+#pragma unroll
+    for (int cc = 0; cc < W; ++cc) dacc[cc] = T(0);
     for (int j = 0; j < np; ++j, ++k) {
       const int slot = (int)(k % S);
       const bool ready = mbar_wait_bounded(full + slot, (uint32_t)((k / S) & 1), a.error);
@@ -173,11 +186,45 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
           const int32_t *col = reinterpret_cast<const int32_t *>(ent);
           const T *val = reinterpret_cast<const T *>(ent + ((4 * len * G + 15) & ~15));
           const int row = rows[g];
-          if (flags & kRecordFirst) acc = Ys[row * W + c];
+          const bool to_tail = (flags & kRecordToTail) != 0;
+          if (flags & kRecordFirst) acc = Ys[(to_tail ? tslot[row] : row) * W + c];
           for (int q = 0; q < len; ++q) acc -= val[q * G + g] * Ys[col[q * G + g] * W + c];
-          if (flags & kRecordLast) Ys[row * W + c] = acc * dinv[g];
+          if (flags & kRecordLast) {
+            if (to_tail)
+              Tb[row * W + c] = acc;
+            else
+              Ys[row * W + c] = acc * dinv[g];
+          }
           pos += 16 + ((4 * G + 15) & ~15) + ((sizeof(T) * G + 15) & ~15) + ((4 * len * G + 15) & ~15) +
                  ((sizeof(T) * len * G + 15) & ~15);
+        } else if (kind == kRecordDense) {
+          // one chunk of a dense tail row: lanes split the columns, each lane keeps W sums
+          const int t = *reinterpret_cast<const int32_t *>(body);
+          const int j0 = *reinterpret_cast<const int32_t *>(body + 4);
+          const T *val = reinterpret_cast<const T *>(body + 16);
+          if (flags & kRecordFirst)
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) dacc[cc] = T(0);
+          for (int e = lane; e < len; e += 32) {
+            const T v = val[e];
+            const T *tb = Tb + (size_t)(j0 + e) * W;
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) dacc[cc] += v * tb[cc];
+          }
+          if (flags & kRecordLast) {
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+              T v = dacc[cc];
+#pragma unroll
+              for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+              if (lane == cc) Ys[tslot[t] * W + cc] = v;
+            }
+          }
+          pos += 32 + ((sizeof(T) * len + 15) & ~15);
+        } else if (kind == kRecordCopy) {
+          // this warp's share of the tail's slots into the tail buffer
+          for (int idx = warp * 32 + lane; idx < m * W; idx += warps * 32) Tb[idx] = Ys[tslot[idx / W] * W + idx % W];
+          pos += 16;
         } else {
           const int row = *reinterpret_cast<const int32_t *>(body);
           const T dinv = *reinterpret_cast<const T *>(body + 16);

@@ -187,6 +187,10 @@ class GpuFactor:
         return {"tile": w.value, "stages": st.value, "records": rec.value, "bytes": by.value,
                 "fwd_wide_levels": nf.value, "bwd_wide_levels": nb.value, "narrow_rows": nr.value}
 
+    def set_tail_level(self, precision: int, level: int) -> None:
+        """-1: chosen from the factor, 0: no dense tail, else the first forward level of the tail."""
+        _check(lib().yb_factor_set_tail_level(self._h, precision, level))
+
     def check_error(self) -> None:
         _check(lib().yb_factor_check_error(self._h))
 
