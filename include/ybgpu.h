@@ -161,7 +161,7 @@ int32_t yb_factor_check_error(yb_factor *f);
 /* No ybus counterpart, diagnostics: a device buffer of 512 int64 (or NULL to stop) into which block
  * 0 of the streamed solve writes clock64() at its phase boundaries for its first 4 tiles, as
  * [tile][warp < 16][8]: 0 tile loaded, 1 own records done, 2 all stages done, 3 tile stored,
- * 3 + s the s-th stage barrier passed (s < 3). */
+ * 4 cycles spent waiting for pages, 5 cycles spent in block barriers, 6 pages taken. */
 int32_t yb_factor_set_phase_clock(yb_factor *f, void *d_clock);
 int32_t yb_factor_get_tile(const yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *threads,
                            int32_t *blocks_per_sm);

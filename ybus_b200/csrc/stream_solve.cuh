@@ -159,13 +159,19 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
     if (pc) pc[0] = clock64();
 
     int done = 0;
+    long long wait_cycles = 0, barrier_cycles = 0, pages_seen = 0;
     T acc = T(0);
     T dacc[W];
 #pragma unroll
     for (int cc = 0; cc < W; ++cc) dacc[cc] = T(0);
     for (int j = 0; j < np; ++j, ++k) {
       const int slot = (int)(k % S);
+      const long long w0 = pc ? clock64() : 0;
       const bool ready = mbar_wait_bounded(full + slot, (uint32_t)((k / S) & 1), a.error);
+      if (pc) {
+        wait_cycles += clock64() - w0;
+        ++pages_seen;
+      }
       const uint8_t *page = ring + (size_t)slot * PB;
       int pos = ready ? 0 : PB;  // a page that never arrived is skipped
       while (pos + 16 <= PB) {
@@ -173,10 +179,13 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
         const int kind = hdr.x, len = hdr.z, flags = hdr.w;
         const int stage = min(hdr.y, a.stages);
         if (kind < 0 || len < 0 || len > PB) break;
-        while (done < stage) {
-          __syncthreads();
-          ++done;
-          if (pc && done < 6) pc[2 + done] = clock64();
+        if (done < stage) {
+          const long long b0 = pc ? clock64() : 0;
+          while (done < stage) {
+            __syncthreads();
+            ++done;
+          }
+          if (pc) barrier_cycles += clock64() - b0;
         }
         const uint8_t *body = page + pos + 16;
         if (kind == kRecordSlice) {
@@ -244,7 +253,12 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
       __syncwarp();
       if (lane == 0) issue(k + S);
     }
-    if (pc) pc[1] = clock64();
+    if (pc) {
+      pc[1] = clock64();
+      pc[4] = wait_cycles;
+      pc[5] = barrier_cycles;
+      pc[6] = pages_seen;
+    }
     while (done < a.stages) {
       __syncthreads();
       ++done;
