@@ -3,6 +3,7 @@
 #include <complex>
 #include <cstring>
 #include <limits>
+#include <functional>
 #include <memory>
 #include <string>
 
@@ -489,11 +490,89 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
     for (int32_t k = s.level_ptr[l]; k < s.level_ptr[l + 1]; ++k) ks.push_back(k);
     return ks;
   };
-  // forward levels 1 .. f_first_narrow - 1, a barrier after each
-  for (int32_t l = 1; l < f_first_narrow; ++l) {
-    deal(F, level_positions(F, l), stage, l);
+  // With a dense tail, the rows below it fall into independent groups (for a Cholesky factor,
+  // the subtrees hanging under the tail): each goes whole to one warp, balanced by work, which
+  // takes its rows level by level with only warp synchronisation
+  std::vector<int32_t> owner(n, -1);
+  bool by_warp = false;
+  if (dense_tail) {
+    std::vector<int32_t> parent_uf(n);
+    for (int32_t i = 0; i < n; ++i) parent_uf[i] = i;
+    std::function<int32_t(int32_t)> find = [&](int32_t x) {
+      while (parent_uf[x] != x) x = parent_uf[x] = parent_uf[parent_uf[x]];
+      return x;
+    };
+    auto join = [&](const Sweep<T> &s) {
+      for (int32_t k = 0; k < n; ++k) {
+        const int32_t i = s.row[k];
+        if (in_tail[i]) continue;
+        for (int32_t p = s.ptr[k]; p < s.ptr[k + 1]; ++p)
+          if (!in_tail[s.col[p]]) parent_uf[find(i)] = find(s.col[p]);
+      }
+    };
+    join(F);
+    if (out.tail_backward) join(B);
+    std::vector<int64_t> work(n, 0);
+    for (int32_t k = 0; k < n; ++k) {
+      if (!in_tail[F.row[k]]) work[find(F.row[k])] += 1 + F.ptr[k + 1] - F.ptr[k];
+      if (!in_tail[B.row[k]]) work[find(B.row[k])] += 1 + B.ptr[k + 1] - B.ptr[k];
+    }
+    std::vector<int32_t> roots;
+    for (int32_t i = 0; i < n; ++i)
+      if (!in_tail[i] && find(i) == i) roots.push_back(i);
+    std::stable_sort(roots.begin(), roots.end(), [&](int32_t a, int32_t b) { return work[a] > work[b]; });
+    std::vector<int64_t> load(warps, 0);
+    std::vector<int32_t> group_warp(n, -1);
+    for (int32_t r : roots) {
+      const int32_t w = (int32_t)(std::min_element(load.begin(), load.end()) - load.begin());
+      group_warp[r] = w;
+      load[w] += work[r];
+    }
+    for (int32_t i = 0; i < n; ++i)
+      if (!in_tail[i]) owner[i] = group_warp[find(i)];
+    by_warp = true;
+  }
+  // Emits positions `ks` of sweep s (in topological order, with their levels `lev`) as each
+  // owner warp's slices, one level after another, all at stage `st`
+  auto emit_owned = [&](const Sweep<T> &s, const std::vector<int32_t> &ks, const std::vector<int32_t> &lev,
+                        int32_t st) {
+    std::vector<std::vector<int32_t>> mine(warps);
+    for (int32_t k : ks) mine[owner[s.row[k]]].push_back(k);
+    for (int32_t w = 0; w < warps; ++w) {
+      auto &v = mine[w];
+      std::stable_sort(v.begin(), v.end(), [&](int32_t a, int32_t b) { return lev[s.row[a]] < lev[s.row[b]]; });
+      size_t i0 = 0;
+      while (i0 < v.size()) {
+        size_t i1 = i0;
+        while (i1 < v.size() && lev[s.row[v[i1]]] == lev[s.row[v[i0]]]) ++i1;
+        std::vector<int32_t> same(v.begin() + i0, v.begin() + i1);
+        std::stable_sort(same.begin(), same.end(), [&](int32_t a, int32_t b) {
+          return (s.ptr[a + 1] - s.ptr[a]) > (s.ptr[b + 1] - s.ptr[b]);
+        });
+        for (size_t t0 = 0; t0 < same.size(); t0 += G) {
+          std::vector<int32_t> part(same.begin() + t0, same.begin() + std::min(same.size(), t0 + (size_t)G));
+          emit_slice(w, s, part, st);
+        }
+        i0 = i1;
+      }
+    }
+  };
+  if (by_warp) {
+    // forward rows below the tail (level 0 is folded into the load)
+    std::vector<int32_t> ks;
+    for (int32_t l = 1; l < f_end; ++l)
+      for (int32_t k = F.level_ptr[l]; k < F.level_ptr[l + 1]; ++k) ks.push_back(k);
+    std::vector<int32_t> lev(F.level_of.begin(), F.level_of.end());
+    emit_owned(F, ks, lev, stage);
     ++stage;
-    ++out.fwd_wide;
+    out.fwd_wide = 1;
+  } else {
+    // forward levels 1 .. f_first_narrow - 1 dealt over the warps, a barrier after each
+    for (int32_t l = 1; l < f_first_narrow; ++l) {
+      deal(F, level_positions(F, l), stage, l);
+      ++stage;
+      ++out.fwd_wide;
+    }
   }
   if (dense_tail) {
     // r_T = b_T - L_TB y_B into the tail buffer, then y_T = L_TT^-1 r_T into the slots
@@ -504,7 +583,7 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
     ++stage;
     const int32_t m = out.tail;
     auto lower_at = [](int32_t i, int32_t j) { return (size_t)i * (i + 1) / 2 + j; };
-    for (int32_t t = 0; t < m; ++t) emit_dense_row((t / 1) % warps, out.fwd_inv, t, 0, t + 1, lower_at, stage);
+    for (int32_t t = 0; t < m; ++t) emit_dense_row(t % warps, out.fwd_inv, t, 0, t + 1, lower_at, stage);
     ++stage;
     out.fwd_narrow_rows = out.tail;
   } else {
@@ -562,13 +641,22 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
       lev[i] = l;
       levels = std::max(levels, l + 1);
     }
-    std::vector<std::vector<int32_t>> by_level(levels);
-    for (int32_t k = 0; k < n; ++k)
-      if (!done_b[B.row[k]]) by_level[lev[B.row[k]]].push_back(k);
-    for (int32_t l = 0; l < levels; ++l) {
-      deal(B, by_level[l], stage, l);
+    if (by_warp && out.tail_backward) {
+      std::vector<int32_t> ks;
+      for (int32_t k = 0; k < n; ++k)
+        if (!done_b[B.row[k]]) ks.push_back(k);
+      emit_owned(B, ks, lev, stage);
       ++stage;
-      ++out.bwd_wide;
+      out.bwd_wide = 1;
+    } else {
+      std::vector<std::vector<int32_t>> by_level(levels);
+      for (int32_t k = 0; k < n; ++k)
+        if (!done_b[B.row[k]]) by_level[lev[B.row[k]]].push_back(k);
+      for (int32_t l = 0; l < levels; ++l) {
+        deal(B, by_level[l], stage, l);
+        ++stage;
+        ++out.bwd_wide;
+      }
     }
   }
   out.stages = stage;
