@@ -49,13 +49,11 @@ def test_every_tile_width_and_block_size(gpu, kind, tile, threads):
 
 
 @pytest.mark.parametrize("tile", [1, 2, 4, 8, 16, 32])
-@pytest.mark.parametrize("warps,ring,page,narrow", [(8, 4, 2048, 0), (4, 2, 512, 0), (1, 3, 1024, 0),
-                                                    (8, 4, 512, 100000), (8, 4, 2048, 1), (16, 2, 768, 3)])
+@pytest.mark.parametrize("warps,ring,page,narrow", [(8, 4, 2048, 0), (4, 2, 1024, 0), (1, 3, 1024, 0),
+                                                    (8, 4, 1024, 100000), (8, 4, 2048, 1), (16, 2, 1536, 3)])
 def test_streamed_solve_every_layout(gpu, tile, warps, ring, page, narrow):
     # small pages force chunked records; narrow=100000 puts every level on warp 0 (split rows),
     # narrow=1 none; 2,000 right-hand sides make several tiles per block at tile width 1
-    if tile == 1 and page < 1024:
-        pytest.skip("a 32-row slice needs pages of at least 1 KiB")
     chol = host.cholesky(random_spd(300, 3, 7))
     rhs = right_hand_sides(300, 37, 11)
     cpu = orc.solve_many(chol, rhs)

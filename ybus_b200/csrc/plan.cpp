@@ -241,7 +241,7 @@ StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, 
   if (W < 1 || W > 32 || 32 % W) throw Error(host::kInvalidArgument, "tile width must divide 32");
   if (value_bytes != 8 && value_bytes != 4) throw Error(host::kInvalidArgument, "values are 4 or 8 bytes");
   if (warps < 1 || page_bytes < 256 || page_bytes % 16) throw Error(host::kInvalidArgument, "bad stream shape");
-  const int32_t n = plan.n, G = 32 / W;
+  const int32_t n = plan.n, G = 32;  // a slice: one row per lane, each lane holding all W sums
   StreamLayout out;
   out.G = G;
   out.warps = warps;

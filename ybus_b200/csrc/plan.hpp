@@ -54,8 +54,9 @@ template <class T> struct SliceSweep {
 template <class T> SliceSweep<T> slice_sweep(const Sweep<T> &s, int32_t n, int32_t G);
 
 // The factor of both sweeps as per-warp streams of records in fixed-size pages, for the streamed
-// tile solve. A record is a slice of up to G rows of one level (one row per lane group), or one
-// long row split over the lane groups, or a chunk of either (entries that do not fit one page
+// tile solve. A record is a slice of up to 32 rows of one level (one row per lane, each lane
+// keeping the tile's W sums in registers), or one long row split over the lanes, or a chunk of
+// either (entries that do not fit one page
 // continue in the next record). Each record carries the number of block barriers that must have
 // passed before it runs (its stage). Levels with many rows ("wide") are dealt over all warps with a
 // block barrier after each; the narrow levels at the top of the tree, at the end of the forward

@@ -93,16 +93,50 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 // Orders this thread's earlier shared-memory accesses before later async-proxy (bulk copy) writes.
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// A slot's W values to and from registers, in 16-byte (or narrower) shared-memory accesses.
+template <class T, int W> __device__ __forceinline__ void load_w(const T *p, T (&v)[W]) {
+  if constexpr (sizeof(T) * W % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) * W / 16); ++i) {
+      const int4 q = reinterpret_cast<const int4 *>(p)[i];
+      memcpy(&v[i * 16 / sizeof(T)], &q, 16);
+    }
+  } else if constexpr (sizeof(T) * W == 8) {
+    const int2 q = *reinterpret_cast<const int2 *>(p);
+    memcpy(&v[0], &q, 8);
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = p[i];
+  }
+}
+
+template <class T, int W> __device__ __forceinline__ void store_w(T *p, const T (&v)[W]) {
+  if constexpr (sizeof(T) * W % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) * W / 16); ++i) {
+      int4 q;
+      memcpy(&q, &v[i * 16 / sizeof(T)], 16);
+      reinterpret_cast<int4 *>(p)[i] = q;
+    }
+  } else if constexpr (sizeof(T) * W == 8) {
+    int2 q;
+    memcpy(&q, &v[0], 8);
+    *reinterpret_cast<int2 *>(p) = q;
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) p[i] = v[i];
+  }
+}
+
 template <class T, int W>
 __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
   static_assert(32 % W == 0, "W divides a warp");
-  constexpr int G = 32 / W;
+  constexpr int G = 32;  // rows of a slice record: one per lane
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int n = a.n;
   T *Ys = reinterpret_cast<T *>(smem_raw);
   const size_t y_bytes = (((size_t)(n + 2) * W * sizeof(T)) + 127) & ~(size_t)127;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  const int g = lane / W, c = lane % W;
   const int S = a.ring, PB = a.page_bytes;
   // the dense tail's buffer (tail + 1 rows) and slots (tail + 1: the spare maps to the zero slot)
   const int m = a.tail;
@@ -160,10 +194,9 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
 
     int done = 0;
     long long wait_cycles = 0, barrier_cycles = 0, pages_seen = 0;
-    T acc = T(0);
-    T dacc[W];
+    T acc[W];  // a row's W running sums (slice: this lane's row; split and dense: this lane's share)
 #pragma unroll
-    for (int cc = 0; cc < W; ++cc) dacc[cc] = T(0);
+    for (int cc = 0; cc < W; ++cc) acc[cc] = T(0);
     for (int j = 0; j < np; ++j, ++k) {
       const int slot = (int)(k % S);
       const long long w0 = pc ? clock64() : 0;
@@ -189,20 +222,31 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
         }
         const uint8_t *body = page + pos + 16;
         if (kind == kRecordSlice) {
+          // this lane's row: W sums in registers, one vector load per entry
           const int32_t *rows = reinterpret_cast<const int32_t *>(body);
           const T *dinv = reinterpret_cast<const T *>(body + ((4 * G + 15) & ~15));
           const uint8_t *ent = body + ((4 * G + 15) & ~15) + ((sizeof(T) * G + 15) & ~15);
           const int32_t *col = reinterpret_cast<const int32_t *>(ent);
           const T *val = reinterpret_cast<const T *>(ent + ((4 * len * G + 15) & ~15));
-          const int row = rows[g];
+          const int row = rows[lane];
           const bool to_tail = (flags & kRecordToTail) != 0;
-          if (flags & kRecordFirst) acc = Ys[(to_tail ? tslot[row] : row) * W + c];
-          for (int q = 0; q < len; ++q) acc -= val[q * G + g] * Ys[col[q * G + g] * W + c];
+          if (flags & kRecordFirst) load_w<T, W>(Ys + (to_tail ? tslot[row] : row) * W, acc);
+          for (int q = 0; q < len; ++q) {
+            const T v = val[q * G + lane];
+            T y[W];
+            load_w<T, W>(Ys + col[q * G + lane] * W, y);
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) acc[cc] -= v * y[cc];
+          }
           if (flags & kRecordLast) {
-            if (to_tail)
-              Tb[row * W + c] = acc;
-            else
-              Ys[row * W + c] = acc * dinv[g];
+            if (to_tail) {
+              store_w<T, W>(Tb + row * W, acc);
+            } else {
+              const T d = dinv[lane];
+#pragma unroll
+              for (int cc = 0; cc < W; ++cc) acc[cc] *= d;
+              store_w<T, W>(Ys + row * W, acc);
+            }
           }
           pos += 16 + ((4 * G + 15) & ~15) + ((sizeof(T) * G + 15) & ~15) + ((4 * len * G + 15) & ~15) +
                  ((sizeof(T) * len * G + 15) & ~15);
@@ -213,17 +257,18 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
           const T *val = reinterpret_cast<const T *>(body + 16);
           if (flags & kRecordFirst)
 #pragma unroll
-            for (int cc = 0; cc < W; ++cc) dacc[cc] = T(0);
+            for (int cc = 0; cc < W; ++cc) acc[cc] = T(0);
           for (int e = lane; e < len; e += 32) {
             const T v = val[e];
-            const T *tb = Tb + (size_t)(j0 + e) * W;
+            T y[W];
+            load_w<T, W>(Tb + (j0 + e) * W, y);
 #pragma unroll
-            for (int cc = 0; cc < W; ++cc) dacc[cc] += v * tb[cc];
+            for (int cc = 0; cc < W; ++cc) acc[cc] += v * y[cc];
           }
           if (flags & kRecordLast) {
 #pragma unroll
             for (int cc = 0; cc < W; ++cc) {
-              T v = dacc[cc];
+              T v = acc[cc];
 #pragma unroll
               for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
               if (lane == cc) Ys[tslot[t] * W + cc] = v;
@@ -235,17 +280,30 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
           for (int idx = warp * 32 + lane; idx < m * W; idx += warps * 32) Tb[idx] = Ys[tslot[idx / W] * W + idx % W];
           pos += 16;
         } else {
+          // one long row split over the lanes: each lane's share of the entries, then a reduction
           const int row = *reinterpret_cast<const int32_t *>(body);
           const T dinv = *reinterpret_cast<const T *>(body + 16);
           const int32_t *col = reinterpret_cast<const int32_t *>(body + 32);
           const T *val = reinterpret_cast<const T *>(body + 32 + ((4 * len + 15) & ~15));
-          T part = T(0);
-          for (int e = g; e < len; e += G) part += val[e] * Ys[col[e] * W + c];
+          if (flags & kRecordFirst)
 #pragma unroll
-          for (int off = W; off < 32; off <<= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
-          if (flags & kRecordFirst) acc = Ys[row * W + c];
-          acc -= part;
-          if ((flags & kRecordLast) && g == 0) Ys[row * W + c] = acc * dinv;
+            for (int cc = 0; cc < W; ++cc) acc[cc] = T(0);
+          for (int e = lane; e < len; e += 32) {
+            const T v = val[e];
+            T y[W];
+            load_w<T, W>(Ys + col[e] * W, y);
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) acc[cc] += v * y[cc];
+          }
+          if (flags & kRecordLast) {
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+              T v = acc[cc];
+#pragma unroll
+              for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+              if (lane == cc) Ys[row * W + cc] = (Ys[row * W + cc] - v) * dinv;
+            }
+          }
           pos += 48 + ((4 * len + 15) & ~15) + ((sizeof(T) * len + 15) & ~15);
         }
         __syncwarp();
