@@ -45,6 +45,7 @@ def parse():
     p.add_argument("--mode", default="auto", choices=["auto", "fp64", "fp32"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--rhs", type=int, default=0, help="solve only the first RHS (a smaller case for profiling)")
     return p.parse_args()
 
 
@@ -202,6 +203,8 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     g, bp, chol, rhs = workload()
+    if a.rhs > 0:
+        rhs = np.ascontiguousarray(rhs[: a.rhs])
     n, count = chol.n, rhs.shape[0]
     gpu = Gpu.new(local)
     factor = GpuFactor.from_cholesky(gpu, chol)

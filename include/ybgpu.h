@@ -137,10 +137,11 @@ int32_t yb_factor_plan_info(const yb_factor *f, int32_t *fwd_levels, int32_t *bw
  * of two; threads a multiple of 32 up to 512; resident blocks per SM 1..8). */
 int32_t yb_factor_set_tile(yb_factor *f, int32_t precision, int32_t tile_width, int32_t threads,
                            int32_t blocks_per_sm);
-/* No ybus counterpart: which tile solve runs for a precision: 0 automatic (the streamed solve at
- * the widest tile that fits in shared memory, else the global-scratch solve), 1 the level-sliced
- * shared-memory solve, 2 the global-scratch solve, 3 the streamed solve (1 and 3 give
- * YB_ERROR_INVALID_ARGUMENT at launch if the tile does not fit in shared memory). */
+/* No ybus counterpart: which tile solve runs for a precision: 0 automatic (the domain solve at the
+ * widest tile that fits in shared memory; else the streamed solve likewise; else the
+ * global-scratch solve), 1 the level-sliced shared-memory solve, 2 the global-scratch solve, 3 the
+ * streamed solve, 4 the domain solve (1, 3 and 4 give YB_ERROR_INVALID_ARGUMENT at launch if the
+ * tile does not fit in shared memory or, for 4, the factor admits no domain layout). */
 int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int32_t kind);
 /* No ybus counterpart: the streamed solve's shape for a precision: warps per block (1..16), pages
  * in flight per warp (2..16), page bytes (512..16384, a multiple of 16), and the row count under
@@ -155,13 +156,32 @@ int32_t yb_factor_set_tail_level(yb_factor *f, int32_t precision, int32_t tail_l
 int32_t yb_factor_stream_info(yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *stages,
                               int64_t *records, int64_t *bytes, int32_t *fwd_wide, int32_t *bwd_wide,
                               int32_t *narrow_rows);
+/* No ybus counterpart: the domain solve's shape for a precision: warps per block (1..16), pages in
+ * flight per warp (2..8), page bytes (512..16384, a multiple of 16), and the cut, the first forward
+ * level of the dense top block (-1: chosen by the layout's cost model). */
+int32_t yb_factor_set_domain(yb_factor *f, int32_t precision, int32_t warps, int32_t ring, int32_t page_bytes,
+                             int32_t cut);
+/* No ybus counterpart: the domain layout the automatic choice runs for a precision (building it if
+ * needed): tile width, cut, rows of the top block, records, bytes, shared memory per block and the
+ * cost model's cycles per tile; YB_ERROR_INVALID_ARGUMENT if that choice is not the domain solve. */
+int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *cut, int32_t *top_rows,
+                              int64_t *records, int64_t *bytes, int64_t *smem_bytes, double *model_cycles);
+/* No ybus counterpart, diagnostics on the host (no GPU needed): the domain layout a Cholesky factor
+ * given as to yb_factor_from_cholesky gets for `value_bytes` (8 or 4). info receives {cut, top
+ * rows, stages, warps, pages, records, entries, page bytes}; blob (pages * page_bytes bytes),
+ * warp_page (warps + 1) and top_slot (top rows) may be NULL, so a first call can size them. */
+int32_t yb_domain_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
+                                  const int64_t *perm, int32_t value_bytes, int32_t warps, int32_t page_bytes,
+                                  int32_t cut, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *top_slot);
 /* Waits for the device and reports YB_ERROR_DEVICE_TIMEOUT (clearing it) if a bounded wait in a
  * kernel of this factor ran out since the last check; the host-array calls check by themselves. */
 int32_t yb_factor_check_error(yb_factor *f);
 /* No ybus counterpart, diagnostics: a device buffer of 512 int64 (or NULL to stop) into which block
- * 0 of the streamed solve writes clock64() at its phase boundaries for its first 4 tiles, as
- * [tile][warp < 16][8]: 0 tile loaded, 1 own records done, 2 all stages done, 3 tile stored,
- * 4 cycles spent waiting for pages, 5 cycles spent in block barriers, 6 pages taken. */
+ * 0 of the streamed or domain solve writes clock64() marks for its first 4 tiles, as
+ * [tile][warp < 16][8]. Streamed solve: 0 tile loaded, 1 own records done, 2 all stages done,
+ * 3 tile stored, 4 cycles waiting for pages, 5 cycles in block barriers, 6 pages taken. Domain
+ * solve: 0 tile start, 1 tile loaded, 2 own records done, 3 tile stored, 4 cycles waiting for
+ * pages, 5 cycles in block barriers, 6 pages taken, 7 records taken. */
 int32_t yb_factor_set_phase_clock(yb_factor *f, void *d_clock);
 int32_t yb_factor_get_tile(const yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *threads,
                            int32_t *blocks_per_sm);

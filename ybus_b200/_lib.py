@@ -76,6 +76,9 @@ SIGNATURES: dict[str, tuple] = {
     "yb_factor_check_error": (i32, [vp]),
     "yb_factor_set_phase_clock": (i32, [vp, vp]),
     "yb_factor_set_tail_level": (i32, [vp, i32, i32]),
+    "yb_factor_set_domain": (i32, [vp, i32, i32, i32, i32, i32]),
+    "yb_factor_domain_info": (i32, [vp, i32, P_i32, P_i32, P_i32, P_i64, P_i64, P_i64, P_dbl]),
+    "yb_domain_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp]),
     "yb_solve_many": (i32, [vp, vp, i64, vp]),
     "yb_solve_many_device": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
 }

@@ -9,6 +9,7 @@
 #include "capi_common.hpp"
 #include "device.cuh"
 #include "factor_state.cuh"
+#include "domain_solve.cuh"
 #include "smem_solve.cuh"
 #include "stream_solve.cuh"
 #include "solve.cuh"
@@ -280,7 +281,7 @@ extern "C" int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int3
   return guard([&] {
     require(f != nullptr, "null factor");
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
-    require(kind >= kTileAuto && kind <= kTileStream, "unknown tile kind");
+    require(kind >= kTileAuto && kind <= kTileDomain, "unknown tile kind");
     (precision == YB_FP64 ? f->tile64 : f->tile32).kind = kind;
     return YB_OK;
   });
@@ -543,10 +544,96 @@ template <class T> void launch_stream(yb_factor *f, StreamArgs a, const TileConf
   }
 }
 
+// The domain layout of a shape, built and uploaded on first use; null if the factor admits none
+// (an upper-triangle entry of a top row reaching below the cut, as an LU factor may have).
+template <class T> DeviceDomain *domain_for(yb_factor *f, const TileConfig &cfg, cudaStream_t stream) {
+  const auto key = std::make_tuple((int)sizeof(T), cfg.domain_warps, cfg.domain_page, cfg.domain_cut);
+  auto it = f->domains.find(key);
+  if (it != f->domains.end()) return it->second.get();
+  std::unique_ptr<DeviceDomain> d;
+  try {
+    const DomainLayout lay = domain_layout(f->plan, (int)sizeof(T), cfg.domain_warps, cfg.domain_page, cfg.domain_cut);
+    d = std::make_unique<DeviceDomain>();
+    d->K = lay.K, d->tail = lay.tail, d->stages = lay.stages, d->warps = lay.warps, d->page_bytes = lay.page_bytes;
+    d->records = lay.records, d->bytes = (int64_t)lay.blob.size(), d->entries = lay.entries;
+    d->dense_entries = lay.dense_entries, d->cost = lay.cost;
+    d->blob.upload(lay.blob, stream);
+    d->warp_page.upload(lay.warp_page, stream);
+    d->tail_slot.upload(lay.tail_slot.empty() ? std::vector<int32_t>{0} : lay.tail_slot, stream);
+    cuda_check(cudaStreamSynchronize(stream), "domain layout upload");
+  } catch (const host::Error &e) {
+    if (e.status != host::kInvalidArgument && e.status != host::kTooLarge) throw;
+    d.reset();
+  }
+  auto *out = d.get();
+  f->domains.emplace(key, std::move(d));
+  return out;
+}
+
+template <class T> size_t domain_smem(const yb_factor *f, const TileConfig &cfg, const DeviceDomain *d, int W) {
+  return domain_smem_bytes((int32_t)f->n, W, (int32_t)sizeof(T), d->tail, cfg.domain_warps, cfg.domain_ring,
+                           cfg.domain_page);
+}
+
+template <class T, int W, class IO>
+void launch_domain_w(yb_factor *f, const TileConfig &cfg, int64_t count, const IO &io, cudaStream_t stream) {
+  DeviceDomain *d = domain_for<T>(f, cfg, stream);
+  if (!d) throw host::Error(host::kInvalidArgument, "the factor admits no domain layout");
+  const size_t smem = domain_smem<T>(f, cfg, d, W);
+  if (smem > (size_t)f->gpu->smem_optin) throw host::Error(host::kInvalidArgument, "the tile does not fit in shared memory");
+  DomainArgs a{};
+  a.n = (int32_t)f->n;
+  a.count = count;
+  a.tiles = (count + W - 1) / W;
+  a.blob = d->blob.get();
+  a.warp_page = d->warp_page.get();
+  a.page_bytes = cfg.domain_page;
+  a.ring = cfg.domain_ring;
+  a.stages = d->stages;
+  a.tail = d->tail;
+  a.tail_slot = d->tail_slot.get();
+  a.error = f->error.get();
+  a.phase_clock = f->phase_clock;
+  cuda_check(cudaFuncSetAttribute(domain_tile_kernel<T, W, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  const int64_t grid = std::min<int64_t>(a.tiles, (int64_t)f->gpu->sm_count);
+  domain_tile_kernel<T, W, IO><<<(unsigned)grid, cfg.domain_warps * 32, smem, stream>>>(a, io);
+  cuda_check(cudaGetLastError(), "domain_tile_kernel launch");
+}
+
+template <class T, class IO>
+void launch_domain(yb_factor *f, const TileConfig &cfg, int64_t count, const IO &io, cudaStream_t stream) {
+  switch (cfg.width) {
+    case 1: return launch_domain_w<T, 1>(f, cfg, count, io, stream);
+    case 2: return launch_domain_w<T, 2>(f, cfg, count, io, stream);
+    case 4: return launch_domain_w<T, 4>(f, cfg, count, io, stream);
+    case 8: return launch_domain_w<T, 8>(f, cfg, count, io, stream);
+    case 16: return launch_domain_w<T, 16>(f, cfg, count, io, stream);
+    default: throw host::Error(host::kInvalidArgument, "unsupported tile width for the domain solve");
+  }
+}
+
 // The shape the auto kind runs: the streamed solve at the widest tile whose working vector and
 // page rings fit in shared memory (one block per SM), else the global-scratch kernel.
-template <class T> TileConfig resolve(const yb_factor *f, TileConfig cfg) {
+template <class T> TileConfig resolve(yb_factor *f, TileConfig cfg) {
   if (cfg.kind == kTileGlobal) return cfg;
+  if (cfg.kind == kTileDomain || cfg.kind == kTileAuto) {
+    DeviceDomain *d = domain_for<T>(f, cfg, f->gpu->stream);
+    if (cfg.kind == kTileDomain) {
+      if (!d) throw host::Error(host::kInvalidArgument, "the factor admits no domain layout");
+      if (domain_smem<T>(f, cfg, d, cfg.width) > (size_t)f->gpu->smem_optin)
+        throw host::Error(host::kInvalidArgument, "the tile does not fit in shared memory");
+      return cfg;
+    }
+    if (d)
+      for (int w = 16; w >= 1; w /= 2)
+        if (domain_smem<T>(f, cfg, d, w) <= (size_t)f->gpu->smem_optin) {
+          TileConfig c = cfg;
+          c.width = w;
+          c.kind = kTileDomain;
+          return c;
+        }
+  }
   if (cfg.kind == kTileStream) {
     if (!stream_fits<T>(f, cfg, cfg.width)) throw host::Error(host::kInvalidArgument, "the tile does not fit in shared memory");
     return cfg;
@@ -595,7 +682,10 @@ void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t
   auto run = [&](auto zero, const TileConfig &configured, auto &fwd, auto &bwd, auto &scratch, auto &cache) {
     using T = decltype(zero);
     const TileConfig cfg = resolve<T>(f, configured);
-    if (cfg.kind == kTileStream) {
+    if (cfg.kind == kTileDomain) {
+      DenseIO io{b, ldb, x, ldx, f->in_slot.get(), f->out_slot.get()};
+      launch_domain<T>(f, cfg, count, io, stream);
+    } else if (cfg.kind == kTileStream) {
       StreamArgs a{};
       a.n = (int32_t)f->n;
       a.count = count;
@@ -761,3 +851,42 @@ extern "C" int32_t yb_factor_stream_info(yb_factor *f, int32_t precision, int32_
   });
 }
 
+
+extern "C" int32_t yb_factor_set_domain(yb_factor *f, int32_t precision, int32_t warps, int32_t ring, int32_t page_bytes,
+                                        int32_t cut) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(warps >= 1 && warps <= 16, "warps must be 1 to 16");
+    require(ring >= 2 && ring <= 8, "the ring holds 2 to 8 pages");
+    require(page_bytes >= 512 && page_bytes <= 16384 && page_bytes % 16 == 0,
+            "page bytes must be a multiple of 16 from 512 to 16384");
+    require(cut >= -1, "the cut is -1 (chosen) or a forward level");
+    TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
+    t.domain_warps = warps, t.domain_ring = ring, t.domain_page = page_bytes, t.domain_cut = cut;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *cut,
+                                         int32_t *top_rows, int64_t *records, int64_t *bytes, int64_t *smem_bytes,
+                                         double *model_cycles) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    const TileConfig &configured = precision == YB_FP64 ? f->tile64 : f->tile32;
+    TileConfig cfg = precision == YB_FP64 ? resolve<double>(f, configured) : resolve<float>(f, configured);
+    if (cfg.kind != kTileDomain) throw host::Error(host::kInvalidArgument, "the solve this precision runs is not the domain solve");
+    DeviceDomain *d = precision == YB_FP64 ? domain_for<double>(f, cfg, f->gpu->stream) : domain_for<float>(f, cfg, f->gpu->stream);
+    if (tile_width) *tile_width = cfg.width;
+    if (cut) *cut = d->K;
+    if (top_rows) *top_rows = d->tail;
+    if (records) *records = d->records;
+    if (bytes) *bytes = d->bytes;
+    if (smem_bytes)
+      *smem_bytes = (int64_t)(precision == YB_FP64 ? domain_smem<double>(f, cfg, d, cfg.width) : domain_smem<float>(f, cfg, d, cfg.width));
+    if (model_cycles) *model_cycles = d->cost;
+    return YB_OK;
+  });
+}

@@ -1,0 +1,365 @@
+// The domain solve: one thread block per SM holds a tile of W right-hand sides' whole working
+// vector in shared memory and takes both sweeps through it, each warp reading its own stream of
+// records (DomainLayout in plan.hpp) from pages that TMA bulk copies bring into a per-warp ring.
+//
+// Per tile:
+//   load      b's W columns into slots (coalesced along each column), no scaling
+//   stage 0   each warp solves its domains forward, level after level
+//   stage 1   r_T = b_T - L_TB y_B into the tail buffer (top rows dealt over the warps)
+//   stage 2   y_T = L_TT^-1 r_T (dense rows) into the top rows' slots
+//   stage 3   y_T copied into the tail buffer
+//   stage 4   x_T = U_TT^-1 y_T (dense rows) into the top rows' slots
+//   stage 5   each warp solves its domains backward
+//   store     the slots into x's W columns
+// A block barrier separates stages; within a stage a warp orders its own records with
+// __syncwarp. Without a top block, stages 1-5 collapse into stage 0: every warp's domains are
+// closed under both sweeps, so no warp waits for another.
+//
+// The load and store policies (IO) give the tile its right-hand sides and take its solutions: dense
+// columns of b and x here; other policies build right-hand sides on the device or fuse epilogues.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device.cuh"
+#include "plan.hpp"
+#include "stream_solve.cuh"
+
+namespace yb {
+
+struct DomainArgs {
+  int32_t n;
+  int64_t count, tiles;
+  const uint8_t *__restrict__ blob;
+  const int32_t *__restrict__ warp_page;  // [warps + 1]
+  int32_t page_bytes, ring, stages;
+  int32_t tail;                           // rows of the top block (0: none)
+  const int32_t *__restrict__ tail_slot;  // [tail]
+  int32_t *error;                         // set to 1 if a wait ran out
+  // diagnostics: if set, block 0 writes clock64() marks for its first 4 tiles as [tile][warp][8]:
+  // 0 tile start, 1 load done, 2 last record done, 3 store done, 4 cycles waiting for pages,
+  // 5 cycles in stage barriers, 6 pages taken, 7 records taken
+  long long *phase_clock;
+};
+
+// The shared-memory footprint of a domain solve block.
+__host__ __device__ inline size_t domain_smem_bytes(int32_t n, int32_t W, int32_t value_bytes, int32_t tail,
+                                                    int32_t warps, int32_t ring, int32_t page_bytes) {
+  const size_t y = (((size_t)(n + 2) * W * value_bytes) + 127) & ~(size_t)127;
+  const size_t tb = (((size_t)(tail + 1) * W * value_bytes) + 15) & ~(size_t)15;
+  const size_t ts = (((size_t)(tail + 1) * 4) + 127) & ~(size_t)127;
+  return y + tb + ts + (size_t)warps * ring * page_bytes + (size_t)warps * ring * 8;
+}
+
+// Dense columns of b in, dense columns of x out (column-major, natural row order; the
+// permutations are applied on the shared-memory side). While a tile is solved, the columns of the
+// block's next tile are prefetched into L2 by bulk prefetches, so its load finds them there.
+struct DenseIO {
+  const double *__restrict__ b;
+  int64_t ldb;
+  double *__restrict__ x;
+  int64_t ldx;
+  const int32_t *__restrict__ in_slot;
+  const int32_t *__restrict__ out_slot;
+
+  template <class T, int W>
+  __device__ __forceinline__ void load(int64_t col0, int64_t count, int n, T *Ys) const {
+    constexpr int U = W >= 4 ? 2 : 8 / W;  // loads in flight per thread and column
+#pragma unroll 1
+    for (int r0 = threadIdx.x; r0 < n; r0 += blockDim.x * U) {
+      double v[U][W];
+      int s[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = r0 + u * blockDim.x;
+        s[u] = r < n ? __ldg(in_slot + r) : n + 1;
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc)
+          v[u][cc] = (r < n && col0 + cc < count) ? __ldcs(b + (col0 + cc) * ldb + r) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        T t[W];
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc) t[cc] = (T)v[u][cc];
+        store_w<T, W>(Ys + (size_t)s[u] * W, t);
+      }
+    }
+  }
+
+  // Prefetches the columns col0 .. col0 + W - 1 into L2 (one bulk prefetch per column and 64 KB).
+  template <int W> __device__ __forceinline__ void prefetch(int64_t col0, int64_t count, int n) const {
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    const int64_t bytes = (int64_t)n * 8;
+    const int chunks = (int)((bytes + 65535) / 65536);
+    for (int i = lane; i < W * chunks; i += 32) {
+      const int cc = i / chunks, ch = i % chunks;
+      if (col0 + cc >= count) continue;
+      const char *base = reinterpret_cast<const char *>(b + (col0 + cc) * ldb) + (int64_t)ch * 65536;
+      const int64_t left = bytes - (int64_t)ch * 65536;
+      // a bulk prefetch wants a 16-byte aligned start and a multiple of 16 bytes
+      const uintptr_t a0 = reinterpret_cast<uintptr_t>(base);
+      const uintptr_t lo = (a0 + 15) & ~(uintptr_t)15;
+      const int64_t len = ((int64_t)(a0 + (left < 65536 ? left : 65536)) - (int64_t)lo) & ~(int64_t)15;
+      if (len > 0)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((uint32_t)len) : "memory");
+    }
+  }
+
+  template <class T, int W>
+  __device__ __forceinline__ void store(int64_t col0, int64_t count, int n, const T *Ys) const {
+#pragma unroll 4
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+      T t[W];
+      load_w<T, W>(Ys + (size_t)__ldg(out_slot + r) * W, t);
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc)
+        if (col0 + cc < count) __stcs(x + (col0 + cc) * ldx + r, (double)t[cc]);
+    }
+  }
+};
+
+template <class T, int W, class IO>
+__global__ void __launch_bounds__(512, 1) domain_tile_kernel(DomainArgs a, IO io) {
+  static_assert(32 % W == 0, "W divides a warp");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int n = a.n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  const int S = a.ring, PB = a.page_bytes;
+  const int m = a.tail;
+  const size_t y_bytes = (((size_t)(n + 2) * W * sizeof(T)) + 127) & ~(size_t)127;
+  const size_t tb_bytes = (((size_t)(m + 1) * W * sizeof(T)) + 15) & ~(size_t)15;
+  const size_t ts_bytes = (((size_t)(m + 1) * 4) + 127) & ~(size_t)127;
+  T *Ys = reinterpret_cast<T *>(smem_raw);
+  T *Tb = reinterpret_cast<T *>(smem_raw + y_bytes);
+  int32_t *tslot = reinterpret_cast<int32_t *>(smem_raw + y_bytes + tb_bytes);
+  uint8_t *ring = smem_raw + y_bytes + tb_bytes + ts_bytes + (size_t)warp * S * PB;
+  uint64_t *full =
+      reinterpret_cast<uint64_t *>(smem_raw + y_bytes + tb_bytes + ts_bytes + (size_t)warps * S * PB) + warp * S;
+
+  // slot n is always zero (the target of padded split entries); slot n + 1 takes the load's spare writes
+  if (threadIdx.x < 2 * W) Ys[n * W + threadIdx.x] = T(0);
+  for (int t = threadIdx.x; t <= m; t += blockDim.x) tslot[t] = t < m ? __ldg(a.tail_slot + t) : n;
+  if (lane == 0)
+    for (int s = 0; s < S; ++s) mbar_init(full + s, 1);
+  mbar_fence_init();
+  __syncthreads();
+
+  const int p0 = __ldg(a.warp_page + warp), np = __ldg(a.warp_page + warp + 1) - p0;
+  const int64_t my_tiles = blockIdx.x < a.tiles ? (a.tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int64_t total_pages = (int64_t)np * my_tiles;
+  // Page k of this warp's run over all its tiles is stream page k % np; it goes to ring slot k % S
+  int slot_next = 0, page_next = 0;
+  int64_t issued = 0;
+  auto issue_one = [&]() {
+    if (issued < total_pages) {
+      fence_proxy_async();
+      bulk_page(ring + (size_t)slot_next * PB, a.blob + (size_t)(p0 + page_next) * PB, (uint32_t)PB, full + slot_next);
+    }
+    ++issued;
+    if (++slot_next == S) slot_next = 0;
+    if (++page_next == np) page_next = 0;
+  };
+  if (lane == 0)
+    for (int s = 0; s < S; ++s) issue_one();
+  __syncwarp();
+
+  int slot_cur = 0;
+  uint32_t parity = 0;
+  for (int64_t tile = blockIdx.x; tile < a.tiles; tile += gridDim.x) {
+    const int64_t col0 = tile * W;
+    const int64_t it = (tile - blockIdx.x) / gridDim.x;
+    long long *pc =
+        (a.phase_clock && blockIdx.x == 0 && it < 4 && lane == 0) ? a.phase_clock + (it * 16 + warp) * 8 : nullptr;
+    if (pc) pc[0] = clock64();
+    io.template load<T, W>(col0, a.count, n, Ys);
+    if (tile + gridDim.x < a.tiles) io.template prefetch<W>((tile + gridDim.x) * W, a.count, n);
+    __syncthreads();
+    if (pc) pc[1] = clock64();
+    long long wait_cycles = 0, barrier_cycles = 0, pages_seen = 0, records_seen = 0;
+
+    int done = 0;
+    T acc[W];  // a split row's or a dense row's running sums, kept across its chunks
+#pragma unroll
+    for (int cc = 0; cc < W; ++cc) acc[cc] = T(0);
+    for (int j = 0; j < np; ++j) {
+      const long long w0 = pc ? clock64() : 0;
+      const bool ready = mbar_wait_bounded(full + slot_cur, parity, a.error);
+      if (pc) wait_cycles += clock64() - w0, ++pages_seen;
+      const uint8_t *page = ring + (size_t)slot_cur * PB;
+      int pos = ready ? 0 : PB;  // a page that never arrived is skipped
+      while (pos + 16 <= PB) {
+        const int4 hdr = *reinterpret_cast<const int4 *>(page + pos);
+        const int kind = hdr.x, flags = hdr.w;
+        if (kind < 0) break;
+        const int stage = min(hdr.y, a.stages);
+        if (done < stage) {
+          const long long b0 = pc ? clock64() : 0;
+          while (done < stage) {
+            __syncthreads();
+            ++done;
+          }
+          if (pc) barrier_cycles += clock64() - b0;
+        }
+        if (pc) ++records_seen;
+        if (kind == kRecordRows) {
+          // k = 2^kl lanes per row: each lane sums its share of the row's entries (two sums for
+          // ILP), the k lanes reduce, and the row's first lane finishes the row
+          const int4 h2 = *reinterpret_cast<const int4 *>(page + pos + 16);
+          const int4 h3 = *reinterpret_cast<const int4 *>(page + pos + 32);
+          const int rows = hdr.z, kl = h2.x, k = 1 << kl;
+          const uint8_t *rec = page + pos;
+          const int r = lane >> kl, sub = lane & (k - 1);
+          const uint16_t *cols = reinterpret_cast<const uint16_t *>(rec + h3.z);
+          const T *vals = reinterpret_cast<const T *>(rec + h3.w);
+          int slot = 0, dest = 0, len = 0, start = 0;
+          if (r < rows) {
+            const int2 in = reinterpret_cast<const int2 *>(rec + h3.x)[r];
+            slot = in.x & 0xffff, len = (int)((unsigned)in.x >> 16);
+            start = in.y & 0xffff, dest = (int)((unsigned)in.y >> 16);
+          }
+          T s0[W], s1[W];
+#pragma unroll
+          for (int cc = 0; cc < W; ++cc) s0[cc] = T(0), s1[cc] = T(0);
+          int q = sub;
+          for (; q + k < len; q += 2 * k) {
+            const int c0 = cols[start + q], c1 = cols[start + q + k];
+            const T v0 = vals[start + q], v1 = vals[start + q + k];
+            T y0[W], y1[W];
+            load_w<T, W>(Ys + c0 * W, y0);
+            load_w<T, W>(Ys + c1 * W, y1);
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) s0[cc] += v0 * y0[cc], s1[cc] += v1 * y1[cc];
+          }
+          if (q < len) {
+            const int c0 = cols[start + q];
+            const T v0 = vals[start + q];
+            T y0[W];
+            load_w<T, W>(Ys + c0 * W, y0);
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) s0[cc] += v0 * y0[cc];
+          }
+#pragma unroll
+          for (int cc = 0; cc < W; ++cc) s0[cc] += s1[cc];
+          for (int off = k >> 1; off > 0; off >>= 1)
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) s0[cc] += __shfl_xor_sync(0xffffffffu, s0[cc], off);
+          if (r < rows && sub == 0) {
+            T y[W];
+            load_w<T, W>(Ys + slot * W, y);
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) y[cc] -= s0[cc];
+            if (flags & kRecordToTail) {
+              store_w<T, W>(Tb + dest * W, y);
+            } else {
+              const T d = reinterpret_cast<const T *>(rec + h3.y)[r];
+#pragma unroll
+              for (int cc = 0; cc < W; ++cc) y[cc] *= d;
+              store_w<T, W>(Ys + dest * W, y);
+            }
+          }
+          pos += h2.z;
+        } else if (kind == kRecordDense) {
+          // a chunk of a dense inverse row: lanes split the columns, each lane keeps W sums
+          const int len = hdr.z;
+          const int t = *reinterpret_cast<const int32_t *>(page + pos + 16);
+          const int j0 = *reinterpret_cast<const int32_t *>(page + pos + 20);
+          const T *val = reinterpret_cast<const T *>(page + pos + 32);
+          if (flags & kRecordFirst)
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) acc[cc] = T(0);
+          for (int e = lane; e < len; e += 32) {
+            const T v = val[e];
+            T y[W];
+            load_w<T, W>(Tb + (size_t)(j0 + e) * W, y);
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) acc[cc] += v * y[cc];
+          }
+          if (flags & kRecordLast) {
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+              T v = acc[cc];
+#pragma unroll
+              for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+              if (lane == cc) Ys[(size_t)tslot[t] * W + cc] = v;
+            }
+          }
+          pos += 32 + (int)(((int64_t)sizeof(T) * len + 15) & ~int64_t(15));
+        } else if (kind == kRecordCopy) {
+          // this warp's share of the top rows' slots into the tail buffer
+          for (int idx = warp * 32 + lane; idx < m * W; idx += warps * 32)
+            Tb[idx] = Ys[(size_t)tslot[idx / W] * W + idx % W];
+          pos += 16;
+        } else if (kind == kRecordSplit) {
+          // one long row over the lanes: each lane's share of the entries, then a reduction
+          const int len = hdr.z;
+          const int row = *reinterpret_cast<const int32_t *>(page + pos + 16);
+          const int dest = *reinterpret_cast<const int32_t *>(page + pos + 20);
+          const T dinv = *reinterpret_cast<const T *>(page + pos + 32);
+          const int32_t *col = reinterpret_cast<const int32_t *>(page + pos + 48);
+          const int col_bytes = (4 * len + 15) & ~15;
+          const T *val = reinterpret_cast<const T *>(page + pos + 48 + col_bytes);
+          if (flags & kRecordFirst)
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) acc[cc] = T(0);
+          for (int e = lane; e < len; e += 32) {
+            const T v = val[e];
+            T y[W];
+            load_w<T, W>(Ys + (size_t)col[e] * W, y);
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) acc[cc] += v * y[cc];
+          }
+          if (flags & kRecordLast) {
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+              T v = acc[cc];
+#pragma unroll
+              for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+              if (lane == cc) {
+                if (flags & kRecordToTail)
+                  Tb[(size_t)dest * W + cc] = Ys[(size_t)row * W + cc] - v;
+                else
+                  Ys[(size_t)row * W + cc] = (Ys[(size_t)row * W + cc] - v) * dinv;
+              }
+            }
+          }
+          pos += 48 + col_bytes + (int)(((int64_t)sizeof(T) * len + 15) & ~int64_t(15));
+        } else {
+          atomicExch(a.error, 2);  // an unknown record: stop reading this page
+          break;
+        }
+        __syncwarp();
+      }
+      __syncwarp();
+      if (lane == 0) issue_one();
+      if (++slot_cur == S) slot_cur = 0, parity ^= 1u;
+    }
+    if (pc) pc[2] = clock64(), pc[4] = wait_cycles, pc[6] = pages_seen, pc[7] = records_seen;
+    {
+      const long long b0 = pc ? clock64() : 0;
+      while (done < a.stages) {
+        __syncthreads();
+        ++done;
+      }
+      if (pc) pc[5] = barrier_cycles + (clock64() - b0);
+    }
+    io.template store<T, W>(col0, a.count, n, Ys);
+    __syncthreads();
+    if (pc) pc[3] = clock64();
+  }
+  // Every copy issued was waited for above unless a wait ran out; then wait (bounded) for the
+  // copies still in flight before the block's shared memory is released
+  if (lane == 0 && total_pages > 0) {
+    const int64_t first = total_pages > S ? total_pages - S : 0;
+    for (int64_t kk = first; kk < total_pages; ++kk) {
+      long tries = 0;
+      while (!mbar_try_wait(full + (kk % S), (uint32_t)((kk / S) & 1)) && ++tries < kWaitLimit) {
+      }
+    }
+  }
+}
+
+}  // namespace yb

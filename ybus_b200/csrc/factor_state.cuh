@@ -39,7 +39,7 @@ struct Timings {
 
 // Which tile solve runs: the shared-memory one (the tile's working vector in shared memory) when
 // it fits, or the one whose working vectors live in a global scratch buffer.
-enum TileKind : int { kTileAuto = 0, kTileShared = 1, kTileGlobal = 2, kTileStream = 3 };
+enum TileKind : int { kTileAuto = 0, kTileShared = 1, kTileGlobal = 2, kTileStream = 3, kTileDomain = 4 };
 
 // The launch shape of the tile solve for one precision.
 struct TileConfig {
@@ -51,6 +51,18 @@ struct TileConfig {
   // row count under which a level goes to warp 0 (0: twice the rows of a slice)
   int stream_warps = 8, ring = 4, page_bytes = 2048, narrow_rows = 0;
   int tail_level = -1;  // forward level from which rows form the dense tail (0: none, -1: chosen)
+  // the domain solve's shape: warps per block, pages in flight per warp, page bytes, and the cut
+  // (first forward level of the top block; -1: chosen by the layout's cost model)
+  int domain_warps = 16, domain_ring = 2, domain_page = 2048, domain_cut = -1;
+};
+
+// A domain layout on the device (DomainLayout in plan.hpp).
+struct DeviceDomain {
+  int32_t K = 0, tail = 0, stages = 0, warps = 0, page_bytes = 0;
+  int64_t records = 0, bytes = 0, entries = 0, dense_entries = 0;
+  double cost = 0;
+  DeviceArray<uint8_t> blob;
+  DeviceArray<int32_t> warp_page, tail_slot;
 };
 
 // A streamed layout on the device (StreamLayout in plan.hpp).
@@ -90,6 +102,8 @@ struct yb_factor {
   std::map<int, std::unique_ptr<yb::DeviceSlices<float>[]>> slices32;
   // streamed layouts by shape (precision, width, warps, page bytes, narrow rows)
   std::map<std::tuple<int, int, int, int, int, int>, std::unique_ptr<yb::DeviceStream>> streams;
+  // domain layouts by shape (value bytes, warps, page bytes, cut); a null entry: the factor admits none
+  std::map<std::tuple<int, int, int, int>, std::unique_ptr<yb::DeviceDomain>> domains;
   yb::DeviceArray<int32_t> error;  // the device error word (a bounded wait that ran out)
   long long *phase_clock = nullptr;  // diagnostics buffer of the caller's, or null
   yb::DeviceArray<double> scratch64;

@@ -85,7 +85,14 @@ struct StreamLayout {
   std::vector<double> load_scale;   // [n] by row of b: the forward diagonal's reciprocal, or 1
 };
 
-enum RecordKind : int32_t { kRecordEnd = -1, kRecordSlice = 0, kRecordSplit = 1, kRecordDense = 2, kRecordCopy = 3 };
+enum RecordKind : int32_t {
+  kRecordEnd = -1,
+  kRecordSlice = 0,
+  kRecordSplit = 1,
+  kRecordDense = 2,
+  kRecordCopy = 3,
+  kRecordRows = 4
+};
 // kRecordToTail: a slice whose rows are tail indices; its results (unscaled) go to the tail buffer
 enum RecordFlags : int32_t { kRecordFirst = 1, kRecordLast = 2, kRecordToTail = 4 };
 
@@ -94,6 +101,42 @@ template <class T> struct Plan;
 template <class T>
 StreamLayout stream_layout(const Plan<T> &plan, int32_t W, int32_t value_bytes, int32_t warps, int32_t page_bytes,
                            int32_t narrow_rows, int32_t tail_level = 0);
+
+// The factor of both sweeps cut for the domain solve (domain_solve.cuh). The rows at forward level
+// K and above form the top T; the rows below fall into domains, the connected groups of rows
+// joined by dependencies of either sweep that avoid T (for a Cholesky factor, the subtrees of the
+// elimination tree hanging under T). Each domain goes whole to one warp, balanced by work, and a
+// warp takes its domains level by level with only warp synchronisation: no block barrier between
+// the levels below K. T is solved as one dense block through the explicit inverses of L_TT and
+// U_TT (computed here in FP64): forward r_T = b_T - L_TB y_B over all warps, then y_T =
+// L_TT^-1 r_T; backward x_T = U_TT^-1 y_T, then the domains in their backward order. Valid when no
+// upper-triangle entry of a T row reaches below T (always so for a Cholesky factor).
+//
+// Records, in each warp's pages (16-byte aligned parts):
+//   kRecordRows:  int4 {kind, stage, rows, flags}, int4 {kl, entries, record bytes, 0},
+//                 int4 {byte offsets of info, dinv, cols, vals in the record}, then int2 info per
+//                 row {slot | len << 16, start | dest << 16}, T dinv per row, uint16 col per entry,
+//                 T val per entry. 2^kl lanes take each row: r = Y[slot] - the sum of its len
+//                 entries from `start`; then Y[dest] = r * dinv, or, with kRecordToTail, the tail
+//                 buffer's entry dest = r.
+//   kRecordSplit, kRecordDense, kRecordCopy: as for the streamed solve; a split record's second
+//                 header word is its destination, with kRecordToTail an entry of the tail buffer.
+struct DomainLayout {
+  int32_t warps = 0, page_bytes = 0, value_bytes = 0, stages = 0;
+  int32_t K = 0;                    // first forward level of T (levels of the tree cut)
+  int32_t tail = 0;                 // |T|
+  std::vector<int32_t> tail_slot;   // [tail] slot of each T row
+  std::vector<uint8_t> blob;        // pages of all warps
+  std::vector<int32_t> warp_page;   // [warps + 1]
+  int64_t records = 0, entries = 0, dense_entries = 0;
+  double cost = 0;                  // the cost model's estimate for the chosen K (cycles per tile)
+};
+
+// Builds the domain layout of `plan` for values of `value_bytes` (8 or 4). K < 0 picks the cut by
+// a cost model; K = 0 puts every row into T (a dense solve). Throws host::Error if the factor does
+// not admit the cut (kInvalidArgument) or the order does not fit 16-bit slots (kTooLarge).
+template <class T>
+DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t warps, int32_t page_bytes, int32_t K);
 
 template <class T> struct Plan {
   int32_t n = 0;

@@ -172,7 +172,7 @@ class GpuFactor:
         _check(lib().yb_factor_set_tile(self._h, precision, width, threads, blocks_per_sm))
 
     def set_tile_kind(self, precision: int, kind: int) -> None:
-        """0 automatic, 1 shared-memory tile solve, 2 global-scratch tile solve."""
+        """0 automatic, 1 shared-memory, 2 global-scratch, 3 streamed, 4 domain tile solve."""
         _check(lib().yb_factor_set_tile_kind(self._h, precision, kind))
 
     def set_stream(self, precision: int, warps: int = 8, ring: int = 4, page_bytes: int = 2048,
@@ -190,6 +190,23 @@ class GpuFactor:
     def set_tail_level(self, precision: int, level: int) -> None:
         """-1: chosen from the factor, 0: no dense tail, else the first forward level of the tail."""
         _check(lib().yb_factor_set_tail_level(self._h, precision, level))
+
+    def set_domain(self, precision: int, warps: int = 16, ring: int = 2, page_bytes: int = 2048, cut: int = -1) -> None:
+        """The domain solve's shape: warps per block, pages in flight per warp, page bytes, cut
+        (-1: chosen by the layout's cost model)."""
+        _check(lib().yb_factor_set_domain(self._h, precision, warps, ring, page_bytes, cut))
+
+    def domain_info(self, precision: int) -> dict:
+        w, cut, top = C.c_int32(), C.c_int32(), C.c_int32()
+        rec, by, sm, cyc = C.c_int64(), C.c_int64(), C.c_int64(), C.c_double()
+        _check(lib().yb_factor_domain_info(self._h, precision, C.byref(w), C.byref(cut), C.byref(top), C.byref(rec),
+                                           C.byref(by), C.byref(sm), C.byref(cyc)))
+        return {"tile": w.value, "cut": cut.value, "top": top.value, "records": rec.value, "bytes": by.value,
+                "smem": sm.value, "model_cycles": cyc.value}
+
+    def set_phase_clock(self, d_clock: int | None) -> None:
+        """Diagnostics: a device buffer of 512 int64 for phase clocks (None to stop)."""
+        _check(lib().yb_factor_set_phase_clock(self._h, d_clock))
 
     def check_error(self) -> None:
         _check(lib().yb_factor_check_error(self._h))

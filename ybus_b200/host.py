@@ -176,3 +176,22 @@ def lu(a: Matrix, ordering: int = AMD, pivot_threshold: float = 0.1) -> HostLu:
     finally:
         lib().yb_host_factor_free(h)
     return HostLu(n=n, l=l, u=u, row_perm=rp, col_perm=cp, is_complex=cplx)
+
+
+def domain_layout(chol: HostCholesky, value_bytes: int = 8, warps: int = 16, page_bytes: int = 2048,
+                  cut: int = -1) -> dict:
+    """The domain solve's records for a Cholesky factor, built on the host (no GPU): the per-warp
+    pages the kernel streams, with the cut and the top block's rows (diagnostics and tests)."""
+    info = np.zeros(8, np.int64)
+    l = chol.l
+    val = np.ascontiguousarray(l.val, dtype=np.float64)
+    args = (chol.n, ptr(l.ptr), ptr(l.idx), ptr(val), ptr(chol.perm), value_bytes, warps, page_bytes, cut)
+    check(lib().yb_domain_layout_cholesky(*args, ptr(info), None, None, None))
+    cut_, top, stages, w, pages, records, entries, pb = (int(v) for v in info)
+    blob = np.zeros(pages * pb, np.uint8)
+    warp_page = np.zeros(w + 1, np.int32)
+    top_slot = np.zeros(max(top, 1), np.int32)
+    check(lib().yb_domain_layout_cholesky(*args, ptr(info), ptr(blob), ptr(warp_page), ptr(top_slot)))
+    return {"cut": cut_, "top": top, "stages": stages, "warps": w, "pages": pages, "records": records,
+            "entries": entries, "page_bytes": pb, "blob": blob, "warp_page": warp_page, "top_slot": top_slot[:top],
+            "value_bytes": value_bytes}
