@@ -195,6 +195,21 @@ int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count, double *ou
 int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
                              int64_t count, int32_t precision, void *stream);
 
+/* No counterpart in ybus. The device-array solve for callers that must not have the library
+ * allocate device memory: programs whose own pool allocator has reserved the GPU's memory (so a
+ * cudaMalloc from here could fail or fragment their pool) and latency-bound loops that cannot take
+ * an allocation's implicit synchronisation. It runs the level-scheduled tile solve with its working
+ * vectors in a 16 MiB array compiled into the library, which every GPU that loads the library
+ * holds until exit, and calls no cudaMalloc or cudaFree. Arguments as yb_solve_many_device; the
+ * factor's upload (yb_factor_from_*) still allocates, once. The tile width is the one
+ * yb_factor_set_tile gives the precision; YB_ERROR_TOO_LARGE if one block's working vectors
+ * (order x tile width x value size) exceed the array. The first call on a device looks up the
+ * array's address and should come before any stream capture. Every call shares the array and
+ * leaves its contents behind (no part needs to start at zero); calls that overlap on the GPU race
+ * on it and must be serialised by the caller. */
+int32_t yb_solve_many_device_noalloc(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
+                                     int64_t count, int32_t precision, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -81,6 +81,7 @@ SIGNATURES: dict[str, tuple] = {
     "yb_domain_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp]),
     "yb_solve_many": (i32, [vp, vp, i64, vp]),
     "yb_solve_many_device": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
+    "yb_solve_many_device_noalloc": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
 }
 
 _lib: C.CDLL | None = None
