@@ -181,7 +181,8 @@ int32_t yb_factor_check_error(yb_factor *f);
  * [tile][warp < 16][8]. Streamed solve: 0 tile loaded, 1 own records done, 2 all stages done,
  * 3 tile stored, 4 cycles waiting for pages, 5 cycles in block barriers, 6 pages taken. Domain
  * solve: 0 tile start, 1 tile loaded, 2 own records done, 3 tile stored, 4 cycles waiting for
- * pages, 5 cycles in block barriers, 6 pages taken, 7 records taken. */
+ * pages, 5 cycles in block barriers, 6 pages taken, 7 records taken; a refined solve writes the
+ * first 4 passes of block 0's first tile in place of 4 tiles. */
 int32_t yb_factor_set_phase_clock(yb_factor *f, void *d_clock);
 int32_t yb_factor_get_tile(const yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *threads,
                            int32_t *blocks_per_sm);
@@ -194,6 +195,20 @@ int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count, double *ou
  * cudaStream_t, NULL for the GPU's own), asynchronous, in YB_FP64 or YB_FP32 substitution. */
 int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
                              int64_t count, int32_t precision, void *stream);
+
+/* Attaches A, the matrix the factor factors (CSR, n x n, natural order, FP64), for refinement:
+ * ybus_sparse's `solve_refined` takes it the same way (accuracy.rs:281-308). A copy with its
+ * columns mapped to the factor's solution order is kept on the device. */
+int32_t yb_factor_attach_matrix(yb_factor *f, const int64_t *a_ptr, const int64_t *a_idx, const double *a_val);
+/* No ybus counterpart on the GPU; the CPU's is `solve_refined_normwise` (accuracy.rs:83-122):
+ * the substitutions in FP32, the residual and the update x += d in FP64 against the attached A (the
+ * residual kept as r -= A d in FP64, the residual of x to rounding), up to max_steps corrections
+ * per tile, until every column's ||r||inf / ||b||inf <= tolerance or the residual stops halving. Device arrays as yb_solve_many_device; d_ratio (double,
+ * count) and d_steps (int32, count) receive each column's final relative residual and corrections
+ * (either may be NULL). Needs the domain solve (YB_ERROR_INVALID_ARGUMENT otherwise). */
+int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
+                                     int64_t count, int32_t max_steps, double tolerance, double *d_ratio,
+                                     int32_t *d_steps, void *stream);
 
 /* No counterpart in ybus. The device-array solve for callers that must not have the library
  * allocate device memory: programs whose own pool allocator has reserved the GPU's memory (so a

@@ -1,0 +1,79 @@
+"""FP32 substitution with FP64 iterative refinement (yb_solve_many_refined_device) against the
+oracle: the relative residual ||b - A x||inf / ||b||inf of every column (accuracy.rs:58-79) reaches
+the tolerance, the device's own ratios agree with the oracle's, the corrections stop early when the
+tolerance is met, and the solutions agree with the FP64 oracle to what the residual allows. Runs
+on the reference's fixture matrix and the synthetic 2,000- and 10,000-bus grids."""
+import numpy as np
+import pytest
+
+import oracle.oracle as orc
+from fixtures import random_spd, right_hand_sides, worst_relative_difference
+from ybus_b200 import CudaError, GpuFactor, grids, host
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def bprime(n_bus, extra, seed):
+    g = grids.make_grid(n_bus, extra, seed)
+    r, c, v = grids.bbus_triplets(g)
+    keep = np.arange(1, n_bus)
+    return host.Matrix.from_triplets(n_bus, n_bus, r, c, v).select(keep, keep)
+
+
+def refined(gpu, a, rhs, max_steps=4, tol=TOL):
+    import torch
+    chol = host.cholesky(a)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.attach_matrix(a)
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    ratio = torch.empty(rhs.shape[0], dtype=torch.float64, device="cuda")
+    steps = torch.empty(rhs.shape[0], dtype=torch.int32, device="cuda")
+    factor.solve_many_refined_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], max_steps, tol, ratio.data_ptr(),
+                                     steps.data_ptr())
+    gpu.synchronize()
+    factor.check_error()
+    return chol, x.cpu().numpy(), ratio.cpu().numpy(), steps.cpu().numpy()
+
+
+@pytest.mark.parametrize("case", ["fixture", "grid2k", "grid10k"])
+def test_refinement_reaches_the_tolerance(gpu, case):
+    if case == "fixture":
+        a = random_spd(300, 3, 7)
+        rhs = right_hand_sides(300, 37, 11)
+    elif case == "grid2k":
+        a = bprime(2000, 700, grids.SEED_BASE + 1)
+        rhs = np.random.default_rng(1).standard_normal((257, 1999))
+    else:
+        a = bprime(10000, 3500, grids.SEED_BASE + 2)
+        rhs = np.random.default_rng(2).standard_normal((600, 9999))
+    chol, x, ratio, steps = refined(gpu, a, rhs)
+    p, i, v = a.to_csr().arrays()
+    oracle_ratio = np.array([orc.relative_residual(p, i, v, x[k], rhs[k]) for k in range(rhs.shape[0])])
+    assert oracle_ratio.max() <= TOL, oracle_ratio.max()
+    # the device's ratios are the residuals of the x it returned, to the rounding of a residual
+    # computed in a different order (FMA contraction, row order): up to ~1e-11 near convergence on the 10k grid
+    assert ratio.max() <= TOL
+    assert np.allclose(ratio, oracle_ratio, rtol=0.05, atol=1e-11)
+    assert steps.min() >= 1 and steps.max() <= 4
+    cpu = orc.solve_many(chol, rhs, threads=8)
+    assert worst_relative_difference(x, cpu) < 1e-8
+
+
+def test_zero_steps_is_the_fp32_solve_and_reports_its_residual(gpu):
+    a = random_spd(300, 3, 7)
+    rhs = right_hand_sides(300, 9, 3)
+    _, x, ratio, steps = refined(gpu, a, rhs, max_steps=0)
+    assert (steps == 0).all()
+    assert 1e-12 < ratio.max() < 1e-4
+
+
+def test_refinement_needs_an_attached_matrix(gpu):
+    import torch
+    chol = host.cholesky(random_spd(50, 5, 2))
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    b = torch.ones((2, 50), dtype=torch.float64, device="cuda")
+    with pytest.raises(CudaError):
+        factor.solve_many_refined_device(b.data_ptr(), b.data_ptr(), 2)

@@ -82,6 +82,8 @@ SIGNATURES: dict[str, tuple] = {
     "yb_solve_many": (i32, [vp, vp, i64, vp]),
     "yb_solve_many_device": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
     "yb_solve_many_device_noalloc": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
+    "yb_factor_attach_matrix": (i32, [vp, vp, vp, vp]),
+    "yb_solve_many_refined_device": (i32, [vp, vp, i64, vp, i64, i64, i32, dbl, vp, vp, vp]),
 }
 
 _lib: C.CDLL | None = None

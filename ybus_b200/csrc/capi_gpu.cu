@@ -890,3 +890,79 @@ extern "C" int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_
     return YB_OK;
   });
 }
+
+extern "C" int32_t yb_factor_attach_matrix(yb_factor *f, const int64_t *a_ptr, const int64_t *a_idx,
+                                           const double *a_val) {
+  return guard([&] {
+    require(f != nullptr && a_ptr != nullptr, "null argument");
+    const int64_t n = f->n;
+    require(a_ptr[0] == 0, "pointers must start at 0");
+    for (int64_t i = 0; i < n; ++i) require(a_ptr[i + 1] >= a_ptr[i], "pointers must not decrease");
+    const int64_t nnz = a_ptr[n];
+    require(nnz == 0 || (a_idx && a_val), "null index or value array");
+    require(nnz < INT32_MAX, "the matrix has too many entries for 32-bit indices", host::kTooLarge);
+    for (int64_t k = 0; k < nnz; ++k) require(a_idx[k] >= 0 && a_idx[k] < n, "a column index is out of range");
+    // rows in natural order, 32 to a slice (sliced ELL: entry q of row 32g + l at ptr[g] + 32q + l),
+    // columns mapped to solution slots (x's row c comes from slot out_slot[c]); padding entries
+    // read the always-zero slot n with value 0
+    const int64_t slices = (n + 31) / 32;
+    std::vector<int32_t> p(slices + 1, 0), idx;
+    std::vector<double> val;
+    for (int64_t g = 0; g < slices; ++g) {
+      int64_t width = 0;
+      for (int64_t r = 32 * g; r < std::min<int64_t>(n, 32 * g + 32); ++r) width = std::max<int64_t>(width, a_ptr[r + 1] - a_ptr[r]);
+      const size_t o = idx.size();
+      idx.resize(o + 32 * width, (int32_t)n);
+      val.resize(o + 32 * width, 0.0);
+      for (int64_t r = 32 * g; r < std::min<int64_t>(n, 32 * g + 32); ++r)
+        for (int64_t k = a_ptr[r]; k < a_ptr[r + 1]; ++k) {
+          const size_t at = o + 32 * (size_t)(k - a_ptr[r]) + (size_t)(r - 32 * g);
+          idx[at] = f->plan.out_slot[a_idx[k]];
+          val[at] = a_val[k];
+        }
+      require(idx.size() < (size_t)INT32_MAX, "the matrix is too large for 32-bit offsets", host::kTooLarge);
+      p[g + 1] = (int32_t)idx.size();
+    }
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    cudaStream_t s = f->gpu->stream;
+    f->a_ptr.upload(p, s);
+    f->a_idx.upload(idx.empty() ? std::vector<int32_t>{0} : idx, s);
+    f->a_val.upload(val.empty() ? std::vector<double>{0.0} : val, s);
+    cuda_check(cudaStreamSynchronize(s), "matrix upload");
+    f->a_rows = n;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out,
+                                                int64_t ldx, int64_t count, int32_t max_steps, double tolerance,
+                                                double *d_ratio, int32_t *d_steps, void *stream) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(count >= 0, "negative count");
+    require(max_steps >= 0 && max_steps <= 64, "max_steps must be 0 to 64");
+    require(tolerance >= 0.0, "the tolerance must not be negative");
+    require(count == 0 || (d_rhs && d_out), "null device array");
+    require(ldb >= f->n && ldx >= f->n, "a leading dimension is below the factor's order");
+    require(f->a_rows == f->n, "no matrix attached: call yb_factor_attach_matrix first");
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    if (count == 0 || f->n == 0) return YB_OK;
+    require(!f->single, "a single-row factor needs no refinement: use yb_solve_many_device");
+    cudaStream_t s = stream ? (cudaStream_t)stream : f->gpu->stream;
+    TileConfig cfg = resolve<float>(f, f->tile32);
+    if (cfg.kind != kTileDomain)
+      throw host::Error(host::kInvalidArgument, "the refined solve needs the domain solve, which this factor does not admit");
+    const int64_t tiles = (count + cfg.width - 1) / cfg.width;
+    const int64_t grid = std::min<int64_t>(tiles, (int64_t)f->gpu->sm_count);
+    f->refine_scratch.reserve((size_t)(grid * f->n * cfg.width));
+    RefineIO io{};
+    io.scratch = f->refine_scratch.get();
+    io.b = d_rhs, io.ldb = ldb, io.x = d_out, io.ldx = ldx;
+    io.in_slot = f->in_slot.get(), io.out_slot = f->out_slot.get();
+    io.a_ptr = f->a_ptr.get(), io.a_idx = f->a_idx.get(), io.a_val = f->a_val.get();
+    io.max_steps = max_steps, io.tolerance = tolerance;
+    io.ratio_out = d_ratio, io.steps_out = d_steps;
+    launch_domain<float>(f, cfg, count, io, s);
+    return YB_OK;
+  });
+}

@@ -44,19 +44,24 @@ struct DomainArgs {
   long long *phase_clock;
 };
 
+// Shared memory an IO policy may declare statically (its reductions), kept free beside the
+// dynamic shared memory.
+constexpr size_t kIoStaticSmem = 1024;
+
 // The shared-memory footprint of a domain solve block.
 __host__ __device__ inline size_t domain_smem_bytes(int32_t n, int32_t W, int32_t value_bytes, int32_t tail,
                                                     int32_t warps, int32_t ring, int32_t page_bytes) {
   const size_t y = (((size_t)(n + 2) * W * value_bytes) + 127) & ~(size_t)127;
   const size_t tb = (((size_t)(tail + 1) * W * value_bytes) + 15) & ~(size_t)15;
   const size_t ts = (((size_t)(tail + 1) * 4) + 127) & ~(size_t)127;
-  return y + tb + ts + (size_t)warps * ring * page_bytes + (size_t)warps * ring * 8;
+  return y + tb + ts + (size_t)warps * ring * page_bytes + (size_t)warps * ring * 8 + kIoStaticSmem;
 }
 
 // Dense columns of b in, dense columns of x out (column-major, natural row order; the
 // permutations are applied on the shared-memory side). While a tile is solved, the columns of the
 // block's next tile are prefetched into L2 by bulk prefetches, so its load finds them there.
 struct DenseIO {
+  static constexpr bool kRefine = false;
   const double *__restrict__ b;
   int64_t ldb;
   double *__restrict__ x;
@@ -66,6 +71,13 @@ struct DenseIO {
 
   template <class T, int W>
   __device__ __forceinline__ void load(int64_t col0, int64_t count, int n, T *Ys) const {
+    load_columns<T, W>(b, ldb, in_slot, col0, count, n, Ys);
+  }
+
+  template <class T, int W>
+  __device__ __forceinline__ static void load_columns(const double *__restrict__ b, int64_t ldb,
+                                                      const int32_t *__restrict__ in_slot, int64_t col0,
+                                                      int64_t count, int n, T *Ys) {
     constexpr int U = W >= 4 ? 2 : 8 / W;  // loads in flight per thread and column
 #pragma unroll 1
     for (int r0 = threadIdx.x; r0 < n; r0 += blockDim.x * U) {
@@ -89,8 +101,14 @@ struct DenseIO {
     }
   }
 
-  // Prefetches the columns col0 .. col0 + W - 1 into L2 (one bulk prefetch per column and 64 KB).
   template <int W> __device__ __forceinline__ void prefetch(int64_t col0, int64_t count, int n) const {
+    prefetch_columns<W>(b, ldb, col0, count, n);
+  }
+
+  // Prefetches the columns col0 .. col0 + W - 1 into L2 (one bulk prefetch per column and 64 KB).
+  template <int W>
+  __device__ __forceinline__ static void prefetch_columns(const double *b, int64_t ldb, int64_t col0, int64_t count,
+                                                          int n) {
     if (threadIdx.x >= 32) return;
     const int lane = threadIdx.x;
     const int64_t bytes = (int64_t)n * 8;
@@ -111,6 +129,13 @@ struct DenseIO {
 
   template <class T, int W>
   __device__ __forceinline__ void store(int64_t col0, int64_t count, int n, const T *Ys) const {
+    store_columns<T, W>(x, ldx, out_slot, col0, count, n, Ys);
+  }
+
+  template <class T, int W>
+  __device__ __forceinline__ static void store_columns(double *__restrict__ x, int64_t ldx,
+                                                       const int32_t *__restrict__ out_slot, int64_t col0,
+                                                       int64_t count, int n, const T *Ys) {
 #pragma unroll 4
     for (int r = threadIdx.x; r < n; r += blockDim.x) {
       T t[W];
@@ -119,6 +144,200 @@ struct DenseIO {
       for (int cc = 0; cc < W; ++cc)
         if (col0 + cc < count) __stcs(x + (col0 + cc) * ldx + r, (double)t[cc]);
     }
+  }
+};
+
+// Iterative refinement (ybus_sparse's `refine_normwise`, accuracy.rs:83-122): the substitutions in
+// the precision of the tile (FP32); the residual and the update x += d in FP64 against the FP64
+// matrix A. Pass 0 loads b into the slots and into the block's FP64 residual scratch R (natural row
+// order, the W values of a row together). After each solve, `update` adds the solve's result d to
+// x (x = d the first time) and updates R -= A d, both row by row in natural order, with A's
+// columns mapped to solution slots so d is gathered from shared memory; then R goes into the slots
+// for the next solve. R is updated rather than recomputed from x, so it is the residual of x up to
+// rounding of the order of eps ||A|| ||x||. The tile is done when every column's relative residual
+// ||r||inf / ||b||inf is at most the tolerance, after `max_steps` corrections, or when no column
+// above the tolerance at least halved its residual in the last step (stagnation). Unlike the CPU's
+// routine, which keeps each column's best iterate, the last iterate is kept; the final ratio and
+// the corrections taken are reported per column.
+struct RefineIO {
+  static constexpr bool kRefine = true;
+  const double *__restrict__ b;
+  int64_t ldb;
+  double *x;  // written and re-read within the launch: no read-only or streaming loads
+  int64_t ldx;
+  const int32_t *__restrict__ in_slot;
+  const int32_t *__restrict__ out_slot;
+  // A's rows in natural order, 32 rows to a slice (sliced ELL): slice g's entry q of row 32g + l
+  // at a_ptr[g] + 32 q + l, with a_ptr[g + 1] - a_ptr[g] = 32 times the slice's longest row;
+  // columns mapped to solution slots, padding pointing at the always-zero slot n with value 0
+  const int32_t *__restrict__ a_ptr;  // [slices + 1]
+  const int32_t *__restrict__ a_idx;
+  const double *__restrict__ a_val;
+  double *scratch;  // gridDim.x blocks of n * W doubles
+  int32_t max_steps;
+  double tolerance;
+  double *__restrict__ ratio_out;  // [count] or null
+  int32_t *__restrict__ steps_out;  // [count] or null
+
+  template <int W> __device__ __forceinline__ double *residual(int n) const {
+    return scratch + (size_t)blockIdx.x * n * W;
+  }
+
+  // b into the slots and into R, and ||b||inf of each column into bnorm (for all threads)
+  template <class T, int W>
+  __device__ __forceinline__ void load_b(int64_t col0, int64_t count, int n, T *Ys, double (&bnorm)[W]) const {
+    constexpr int U = W >= 8 ? 1 : 4;  // rows in flight per thread
+    __shared__ double red[32][W];
+    double *R = residual<W>(n);
+    double local[W];
+#pragma unroll
+    for (int cc = 0; cc < W; ++cc) local[cc] = 0.0;
+#pragma unroll 1
+    for (int r0 = threadIdx.x; r0 < n; r0 += blockDim.x * U) {
+      double v[U][W];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = r0 + u * blockDim.x;
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc) v[u][cc] = (r < n && col0 + cc < count) ? b[(col0 + cc) * ldb + r] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = r0 + u * blockDim.x;
+        if (r >= n) break;
+        T t[W];
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc) {
+          local[cc] = fmax(local[cc], fabs(v[u][cc]));
+          t[cc] = (T)v[u][cc];
+          R[(size_t)r * W + cc] = v[u][cc];
+        }
+        store_w<T, W>(Ys + (size_t)__ldg(in_slot + r) * W, t);
+      }
+    }
+    block_max<W>(local, red, bnorm);
+  }
+
+  // x (first) or x += d from the slots; R -= A d; ||R||inf per column into rnorm; R into the slots
+  template <class T, int W>
+  __device__ __forceinline__ void update(bool first, int64_t col0, int64_t count, int n, T *Ys,
+                                         double (&rnorm)[W]) const {
+    constexpr int U = W >= 8 ? 1 : 4;  // rows in flight per thread
+    __shared__ double red[32][W];
+    double *R = residual<W>(n);
+    double local[W];
+#pragma unroll
+    for (int cc = 0; cc < W; ++cc) local[cc] = 0.0;
+#pragma unroll 1
+    for (int r0 = threadIdx.x; r0 < n; r0 += blockDim.x * U) {
+      double acc[U][W], xo[U][W];
+      int p0[U], p1[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = r0 + u * blockDim.x;
+        const bool in = r < n;
+        p0[u] = in ? __ldg(a_ptr + (r >> 5)) + (r & 31) : 0;
+        p1[u] = in ? __ldg(a_ptr + (r >> 5) + 1) : 0;
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc) {
+          acc[u][cc] = in ? R[(size_t)r * W + cc] : 0.0;
+          xo[u][cc] = (in && !first && col0 + cc < count) ? x[(col0 + cc) * ldx + r] : 0.0;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = r0 + u * blockDim.x;
+        if (r >= n) break;
+        T d[W];
+        load_w<T, W>(Ys + (size_t)__ldg(out_slot + r) * W, d);
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc)
+          if (col0 + cc < count) x[(col0 + cc) * ldx + r] = xo[u][cc] + (double)d[cc];
+        int p = p0[u];
+#pragma unroll 1
+        for (; p + 96 < p1[u]; p += 128) {  // four entries of the row at a time, their loads together
+          int j[4];
+          double v[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) j[e] = __ldg(a_idx + p + 32 * e), v[e] = __ldg(a_val + p + 32 * e);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            T y[W];
+            load_w<T, W>(Ys + (size_t)j[e] * W, y);
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) acc[u][cc] -= v[e] * (double)y[cc];
+          }
+        }
+        for (; p < p1[u]; p += 32) {
+          const double v = __ldg(a_val + p);
+          T y[W];
+          load_w<T, W>(Ys + (size_t)__ldg(a_idx + p) * W, y);
+#pragma unroll
+          for (int cc = 0; cc < W; ++cc) acc[u][cc] -= v * (double)y[cc];
+        }
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc) {
+          if (col0 + cc >= count) acc[u][cc] = 0.0;
+          R[(size_t)r * W + cc] = acc[u][cc];
+          local[cc] = fmax(local[cc], fabs(acc[u][cc]));
+        }
+      }
+    }
+    block_max<W>(local, red, rnorm);  // every gather of d is done past its barrier
+#pragma unroll 1
+    for (int r0 = threadIdx.x; r0 < n; r0 += blockDim.x * U) {
+      double v[U][W];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = r0 + u * blockDim.x;
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc) v[u][cc] = r < n ? R[(size_t)r * W + cc] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = r0 + u * blockDim.x;
+        if (r >= n) break;
+        T t[W];
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc) t[cc] = (T)v[u][cc];
+        store_w<T, W>(Ys + (size_t)__ldg(in_slot + r) * W, t);
+      }
+    }
+    __syncthreads();
+  }
+
+  // The largest of every thread's values, per column, returned to all threads (NaN propagates).
+  template <int W>
+  __device__ __forceinline__ static void block_max(const double (&local)[W], double (&red)[32][W], double (&out)[W]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+#pragma unroll
+    for (int cc = 0; cc < W; ++cc) {
+      double v = local[cc];
+      bool nan = v != v;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double u = __shfl_xor_sync(0xffffffffu, v, off);
+        nan = nan || (u != u);
+        v = fmax(v, u);
+      }
+      if (lane == 0) red[warp][cc] = nan ? __longlong_as_double(0x7ff8000000000000LL) : v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int cc = 0; cc < W; ++cc) {
+      double v = 0.0;
+      bool nan = false;
+      for (int w = 0; w < warps; ++w) {
+        nan = nan || (red[w][cc] != red[w][cc]);
+        v = fmax(v, red[w][cc]);
+      }
+      out[cc] = nan ? __longlong_as_double(0x7ff8000000000000LL) : v;
+    }
+    __syncthreads();
+  }
+
+  template <int W> __device__ __forceinline__ void prefetch(int64_t col0, int64_t count, int n) const {
+    DenseIO::prefetch_columns<W>(b, ldb, col0, count, n);
   }
 };
 
@@ -150,20 +369,20 @@ __global__ void __launch_bounds__(512, 1) domain_tile_kernel(DomainArgs a, IO io
 
   const int p0 = __ldg(a.warp_page + warp), np = __ldg(a.warp_page + warp + 1) - p0;
   const int64_t my_tiles = blockIdx.x < a.tiles ? (a.tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  const int64_t total_pages = (int64_t)np * my_tiles;
-  // Page k of this warp's run over all its tiles is stream page k % np; it goes to ring slot k % S
+  // The warp's stream is taken once per solve pass, np pages each, cyclically: page k of the run
+  // is stream page k % np and lands in ring slot k % S. A refined solve takes a data-dependent
+  // number of passes, so copies run S pages ahead of use and the last S are drained at the end.
+  const bool streaming = np > 0 && my_tiles > 0;
   int slot_next = 0, page_next = 0;
-  int64_t issued = 0;
+  int64_t issued = 0, consumed = 0;
   auto issue_one = [&]() {
-    if (issued < total_pages) {
-      fence_proxy_async();
-      bulk_page(ring + (size_t)slot_next * PB, a.blob + (size_t)(p0 + page_next) * PB, (uint32_t)PB, full + slot_next);
-    }
+    fence_proxy_async();
+    bulk_page(ring + (size_t)slot_next * PB, a.blob + (size_t)(p0 + page_next) * PB, (uint32_t)PB, full + slot_next);
     ++issued;
     if (++slot_next == S) slot_next = 0;
     if (++page_next == np) page_next = 0;
   };
-  if (lane == 0)
+  if (lane == 0 && streaming)
     for (int s = 0; s < S; ++s) issue_one();
   __syncwarp();
 
@@ -172,11 +391,22 @@ __global__ void __launch_bounds__(512, 1) domain_tile_kernel(DomainArgs a, IO io
   for (int64_t tile = blockIdx.x; tile < a.tiles; tile += gridDim.x) {
     const int64_t col0 = tile * W;
     const int64_t it = (tile - blockIdx.x) / gridDim.x;
+    double bnorm[W], prev[W];
+#pragma unroll
+    for (int cc = 0; cc < W; ++cc) bnorm[cc] = 0.0, prev[cc] = __longlong_as_double(0x7ff0000000000000LL);
+    for (int pass = 0;; ++pass) {
+    // diagnostics rows: the first 4 tiles, or for a refined solve the first 4 passes of tile 0
+    const int64_t mark = IO::kRefine ? (it == 0 ? pass : 4) : it;
     long long *pc =
-        (a.phase_clock && blockIdx.x == 0 && it < 4 && lane == 0) ? a.phase_clock + (it * 16 + warp) * 8 : nullptr;
+        (a.phase_clock && blockIdx.x == 0 && mark < 4 && lane == 0) ? a.phase_clock + (mark * 16 + warp) * 8 : nullptr;
     if (pc) pc[0] = clock64();
-    io.template load<T, W>(col0, a.count, n, Ys);
-    if (tile + gridDim.x < a.tiles) io.template prefetch<W>((tile + gridDim.x) * W, a.count, n);
+    if (pass == 0) {
+      if constexpr (IO::kRefine)
+        io.template load_b<T, W>(col0, a.count, n, Ys, bnorm);
+      else
+        io.template load<T, W>(col0, a.count, n, Ys);
+    }
+    if (pass == 0 && tile + gridDim.x < a.tiles) io.template prefetch<W>((tile + gridDim.x) * W, a.count, n);
     __syncthreads();
     if (pc) pc[1] = clock64();
     long long wait_cycles = 0, barrier_cycles = 0, pages_seen = 0, records_seen = 0;
@@ -334,6 +564,7 @@ __global__ void __launch_bounds__(512, 1) domain_tile_kernel(DomainArgs a, IO io
         __syncwarp();
       }
       __syncwarp();
+      ++consumed;
       if (lane == 0) issue_one();
       if (++slot_cur == S) slot_cur = 0, parity ^= 1u;
     }
@@ -346,15 +577,46 @@ __global__ void __launch_bounds__(512, 1) domain_tile_kernel(DomainArgs a, IO io
       }
       if (pc) pc[5] = barrier_cycles + (clock64() - b0);
     }
-    io.template store<T, W>(col0, a.count, n, Ys);
-    __syncthreads();
-    if (pc) pc[3] = clock64();
+    if constexpr (IO::kRefine) {
+      double rnorm[W];
+      io.template update<T, W>(pass == 0, col0, a.count, n, Ys, rnorm);
+      if (pc) pc[3] = clock64();
+      // the relative residual of each column after `pass` corrections (accuracy.rs:58-79), and
+      // whether another correction is worth it
+      bool open = false, progress = false, bad = false;
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) {
+        if (col0 + cc >= a.count) continue;
+        const double ratio = bnorm[cc] > 0.0 ? rnorm[cc] / bnorm[cc]
+                                             : (rnorm[cc] > 0.0 ? __longlong_as_double(0x7ff0000000000000LL) : 0.0);
+        bad = bad || (ratio != ratio);
+        if (ratio > io.tolerance) {
+          open = true;
+          progress = progress || (ratio <= 0.5 * prev[cc]);
+        }
+        prev[cc] = ratio;
+      }
+      if (!open || !progress || bad || pass >= io.max_steps) {
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc)
+          if (threadIdx.x == cc && col0 + cc < a.count) {
+            if (io.ratio_out) io.ratio_out[col0 + cc] = prev[cc];
+            if (io.steps_out) io.steps_out[col0 + cc] = pass;
+          }
+        break;
+      }
+    } else {
+      io.template store<T, W>(col0, a.count, n, Ys);
+      __syncthreads();
+      if (pc) pc[3] = clock64();
+      break;
+    }
+    }
   }
-  // Every copy issued was waited for above unless a wait ran out; then wait (bounded) for the
-  // copies still in flight before the block's shared memory is released
-  if (lane == 0 && total_pages > 0) {
-    const int64_t first = total_pages > S ? total_pages - S : 0;
-    for (int64_t kk = first; kk < total_pages; ++kk) {
+  // Every copy issued but not consumed (the S run ahead, or more after a wait that ran out) is
+  // waited for, bounded, before the block's shared memory is released
+  if (lane == 0 && streaming) {
+    for (int64_t kk = consumed; kk < issued; ++kk) {
       long tries = 0;
       while (!mbar_try_wait(full + (kk % S), (uint32_t)((kk / S) & 1)) && ++tries < kWaitLimit) {
       }

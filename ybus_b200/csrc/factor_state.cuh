@@ -109,6 +109,12 @@ struct yb_factor {
   yb::DeviceArray<double> scratch64;
   yb::DeviceArray<float> scratch32;
   yb::DeviceArray<double> dev_b, dev_x;
+  // the matrix A the factor factors, for refinement: rows in natural order, columns mapped to
+  // the solution slots, FP64
+  int64_t a_rows = -1;
+  yb::DeviceArray<int32_t> a_ptr, a_idx;
+  yb::DeviceArray<double> a_val;
+  yb::DeviceArray<double> refine_scratch;  // per block n * W residuals
   yb::PinnedBuffer staging;
   int64_t width = 1;
   yb::Timings timings;

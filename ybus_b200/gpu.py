@@ -231,6 +231,23 @@ class GpuFactor:
         """`solve_many` into a caller's (count, n) buffer (pinned buffers are copied directly)."""
         _check(lib().yb_solve_many(self._h, b.ctypes.data, b.shape[0], out.ctypes.data))
 
+    def attach_matrix(self, a) -> None:
+        """Attaches A (a host.Matrix, or (ptr, idx, val) CSR arrays in natural order) for refinement."""
+        if hasattr(a, "arrays"):
+            a = a.to_csr().arrays()
+        p, i, v = (np.ascontiguousarray(a[0], dtype=np.int64), np.ascontiguousarray(a[1], dtype=np.int64),
+                   np.ascontiguousarray(a[2], dtype=np.float64))
+        self._matrix = (p, i, v)
+        _check(lib().yb_factor_attach_matrix(self._h, ptr(p), ptr(i), ptr(v)))
+
+    def solve_many_refined_device(self, d_rhs: int, d_out: int, count: int, max_steps: int = 3,
+                                  tolerance: float = 1e-10, d_ratio: int | None = None, d_steps: int | None = None,
+                                  stream: int | None = None, ldb: int | None = None, ldx: int | None = None) -> None:
+        """FP32 substitution with FP64 refinement on device pointers (accuracy.rs:83-122)."""
+        n = self.dim()
+        _check(lib().yb_solve_many_refined_device(self._h, d_rhs, ldb or n, d_out, ldx or n, count, max_steps,
+                                                  float(tolerance), d_ratio, d_steps, stream))
+
     def solve_many_device(self, d_rhs: int, d_out: int, count: int, precision: int = FP64, stream: int | None = None,
                           ldb: int | None = None, ldx: int | None = None) -> None:
         """The solve on device pointers (column-major n x count), asynchronous on `stream`."""
