@@ -34,6 +34,7 @@ UNIT = "RHS/s"
 WORKLOAD = "10k-bus PTDF block: B' 9,999 x 9,999 AMD Cholesky, 13,499 branch RHS"
 N_BUS, EXTRA = 10000, 3500
 FALLBACK_HBM_GBS = 6650.0
+IR_TOLERANCE, IR_MAX_STEPS = 1e-10, 3
 
 
 def parse():
@@ -42,7 +43,7 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--mode", default="auto", choices=["auto", "fp64", "fp32"])
+    p.add_argument("--mode", default="auto", choices=["auto", "fp64", "fp32_ir"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--rhs", type=int, default=0, help="solve only the first RHS (a smaller case for profiling)")
@@ -128,13 +129,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(n: int, count: int, entries: int, precision: str) -> int:
-    """Bytes a solve of `count` right-hand sides must move: per RHS read b (8n), write the
-    intermediate y and read it back (2 s n), write x (8n), plus the factor once (values and
-    int32 indices of both sweeps, and their row pointers)."""
-    s = 8 if precision == "fp64" else 4
-    factor = entries * (s + 4) + 2 * 4 * (n + 1)
-    return count * (16 * n + 2 * s * n) + factor
+def algorithmic_bytes(n: int, count: int, info: dict, mode: str, steps: float = 0.0, a_nnz: int = 0) -> int:
+    """The per-launch byte model of the solve path (per RHS, plus the factor once):
+    FP64: read b (8n), write and read the intermediate y (16n), write x (8n): 32 n.
+    FP32 + m refinement steps: 24 n for the first solve, 48 n per step (residual reads x and b and
+    writes r, the substitution writes and reads y, the update reads d and reads and writes x),
+    plus the FP64 matrix once. The factor: values and int32 indices of both sweeps, row pointers."""
+    entries = info["fwd_entries"] + info["bwd_entries"]
+    if mode == "fp64":
+        return int(count * 32 * n + entries * 12 + 8 * (n + 1))
+    a_bytes = a_nnz * 12 + 4 * (n + 1)
+    return int(count * (24 * n + steps * 48 * n) + entries * 8 + 8 * (n + 1) + a_bytes)
 
 
 def cpu_baseline(chol, rhs, seconds_target: float = 10.0) -> dict:
@@ -209,73 +214,102 @@ def main():
     gpu = Gpu.new(local)
     factor = GpuFactor.from_cholesky(gpu, chol)
     info = factor.plan_info()
-    mode = "fp64" if a.mode in ("auto", "fp64") else "fp32"
-    precision = FP64 if mode == "fp64" else FP32
+    factor.attach_matrix(bp)
 
     d_b = torch.from_numpy(rhs).cuda()
     d_x = torch.empty_like(d_b)
+    d_ratio = torch.empty(count, dtype=torch.float64, device="cuda")
+    d_steps = torch.empty(count, dtype=torch.int32, device="cuda")
     # A stream of our own: the current (legacy default) stream's handle is 0, which the C ABI
     # reads as the library's own stream
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
 
-    def step():
-        factor.solve_many_device(d_b.data_ptr(), d_x.data_ptr(), count, precision, sh)
+    # each mode: one launch per step over the whole block
+    runs = {
+        "fp64": lambda: factor.solve_many_device(d_b.data_ptr(), d_x.data_ptr(), count, FP64, sh),
+        "fp32_ir": lambda: factor.solve_many_refined_device(d_b.data_ptr(), d_x.data_ptr(), count, IR_MAX_STEPS,
+                                                            IR_TOLERANCE, d_ratio.data_ptr(), d_steps.data_ptr(), sh),
+    }
+    modes = ["fp64", "fp32_ir"] if a.mode == "auto" else [a.mode]
 
-    for _ in range(max(a.warmup, 3)):
-        step()
-    torch.cuda.synchronize()
+    def timed(run):
+        for _ in range(max(a.warmup, 3)):
+            run()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for e0, e1 in evs:
+            e0.record(stream)
+            run()
+            e1.record(stream)
+        end.record(stream)
+        torch.cuda.synchronize()
+        elapsed_ms = start.elapsed_time(end)
+        launch_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs)
+        if world > 1:
+            dist.barrier()
+            t = torch.tensor([elapsed_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            elapsed_ms = float(t.item())
+        return elapsed_ms, launch_ms
 
-    clocks = ClockSampler(local).start()
-    time.sleep(0.3)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    for e0, e1 in evs:
-        e0.record(stream)
-        step()
-        e1.record(stream)
-    end.record(stream)
-    torch.cuda.synchronize()
-    elapsed_ms = start.elapsed_time(end)
-    launch_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs)
-    if world > 1:
-        dist.barrier()
-        t = torch.tensor([elapsed_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
-    clock_info = clocks.stop()
-
-    # Check the timed results: relative residual of every 13th column, and the oracle on a sample
-    from oracle import oracle as orc  # the checker, outside the timed region
-    xs = d_x.cpu().numpy()
+    from oracle import oracle as orc  # the checker, outside the timed regions
     p, i, v = bp.arrays()
-    resid = max(orc.relative_residual(p, i, v, xs[k], rhs[k]) for k in range(0, count, 13))
     sample = np.arange(0, count, max(1, count // 64))
     cpu = orc.solve_many(chol, rhs[sample], threads=os.cpu_count() or 1)
-    err = float(max(np.abs(xs[k] - c).max() / np.abs(c).max() for k, c in zip(sample, cpu)))
-
-    value = world * count * a.steps / (elapsed_ms / 1e3)
-    entries = info["fwd_entries"] + info["bwd_entries"]
-    alg = algorithmic_bytes(n, count, entries, mode)
     peak, peak_kind = measured_peak()
-    achieved = alg / (launch_ms / 1e3) / 1e9
+    clocks = ClockSampler(local).start()
+    time.sleep(0.3)
+    results = {}
+    for mode in modes:
+        elapsed_ms, launch_ms = timed(runs[mode])
+        # check the timed results: relative residual of every 13th column, the oracle on a sample
+        xs = d_x.cpu().numpy()
+        resid = max(orc.relative_residual(p, i, v, xs[k], rhs[k]) for k in range(0, count, 13))
+        err = float(max(np.abs(xs[k] - c).max() / np.abs(c).max() for k, c in zip(sample, cpu)))
+        r = {"rhs_s": world * count * a.steps / (elapsed_ms / 1e3), "ms_per_step": elapsed_ms / a.steps,
+             "launch_ms": launch_ms, "max_rel_residual": resid, "max_rel_err_vs_oracle": err}
+        if mode == "fp32_ir":
+            ratios, steps = d_ratio.cpu().numpy(), d_steps.cpu().numpy()
+            r.update({"device_max_ratio": float(ratios.max()), "mean_corrections": float(steps.mean()),
+                      "max_corrections": int(steps.max()), "tolerance": IR_TOLERANCE, "max_steps": IR_MAX_STEPS})
+            r["algorithmic_bytes_per_launch"] = algorithmic_bytes(n, count, info, "fp32_ir", float(steps.mean()), len(i))
+        else:
+            r["algorithmic_bytes_per_launch"] = algorithmic_bytes(n, count, info, "fp64")
+        r["tile"] = factor.domain_info(FP64 if mode == "fp64" else FP32)["tile"]
+        results[mode] = r
+    clock_info = clocks.stop()
 
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": elapsed_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if mode == "fp64" else "f32", "data": "synthetic",
+    # the headline: the fastest mode whose every checked column meets the 1e-10 relative residual
+    passing = [m for m in modes if results[m]["max_rel_residual"] <= 1e-10]
+    mode = max(passing, key=lambda m: results[m]["rhs_s"]) if passing else modes[0]
+    best = results[mode]
+    achieved = best["algorithmic_bytes_per_launch"] / (best["launch_ms"] / 1e3) / 1e9
+    compulsory = count * 16 * n / (best["launch_ms"] / 1e3) / 1e9
+    if "fp64" in results and "fp32_ir" in results:
+        results["fp32_ir_over_fp64"] = results["fp32_ir"]["rhs_s"] / results["fp64"]["rhs_s"]
+
+    line = {"metric": METRIC, "value": best["rhs_s"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": best["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if mode == "fp64" else "f32 substitution, f64 refinement",
+            "data": "synthetic",
             "config": {"workload": WORKLOAD, "rhs_per_step": count, "n": n, "mode": mode,
                        "nnz_factor_per_sweep": info["fwd_entries"] + n, "levels": [info["fwd_levels"], info["bwd_levels"]],
-                       "tile": factor.tile(precision), "flush": "inputs (1.08 GB) > L2", "parallelism": f"replicas x{world}"},
-            "accuracy": {"max_rel_residual": resid, "max_rel_err_vs_oracle": err},
+                       "tile": best["tile"], "flush": "inputs (1.08 GB) > L2", "parallelism": f"replicas x{world}"},
+            "accuracy": {"max_rel_residual": best["max_rel_residual"], "max_rel_err_vs_oracle": best["max_rel_err_vs_oracle"]},
+            "modes": results,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": alg, "launch_ms": launch_ms},
-            "clocks": clock_info, "gpu_launches": a.steps}
+                         "traffic": None, "peak_source": peak_kind, "kernel": "domain_tile_kernel",
+                         "algorithmic_bytes_per_launch": best["algorithmic_bytes_per_launch"],
+                         "launch_ms": best["launch_ms"], "compulsory_gbs": compulsory,
+                         "compulsory_frac": compulsory / peak},
+            "clocks": clock_info, "gpu_launches": a.steps * len(modes)}
 
     if rank == 0 and world == 1 and not a.no_e2e:
         b_pin = torch.from_numpy(rhs).pin_memory()
