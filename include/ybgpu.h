@@ -168,11 +168,14 @@ int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_t *tile_wid
                               int64_t *records, int64_t *bytes, int64_t *smem_bytes, double *model_cycles);
 /* No ybus counterpart, diagnostics on the host (no GPU needed): the domain layout a Cholesky factor
  * given as to yb_factor_from_cholesky gets for `value_bytes` (8 or 4). info receives {cut, top
- * rows, stages, warps, pages, records, entries, page bytes}; blob (pages * page_bytes bytes),
- * warp_page (warps + 1) and top_slot (top rows) may be NULL, so a first call can size them. */
+ * rows, stages, warps, pages, records, entries, page bytes}, top_condition the worse infinity-norm
+ * condition of the top block's two triangles; blob (pages * page_bytes bytes), warp_page (warps + 1),
+ * top_slot (top rows) and top_condition may be NULL, so a first call can size them. A cut whose top
+ * triangles have a condition above 1e4 is not used (their explicit inverses would lose accuracy). */
 int32_t yb_domain_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
                                   const int64_t *perm, int32_t value_bytes, int32_t warps, int32_t page_bytes,
-                                  int32_t cut, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *top_slot);
+                                  int32_t cut, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *top_slot,
+                                  double *top_condition);
 /* Waits for the device and reports YB_ERROR_DEVICE_TIMEOUT (clearing it) if a bounded wait in a
  * kernel of this factor ran out since the last check; the host-array calls check by themselves. */
 int32_t yb_factor_check_error(yb_factor *f);
@@ -195,6 +198,49 @@ int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count, double *ou
  * cudaStream_t, NULL for the GPU's own), asynchronous, in YB_FP64 or YB_FP32 substitution. */
 int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
                              int64_t count, int32_t precision, void *stream);
+
+/* ---- blocks solved on the device (ybus_cuda `GpuBlock`, `GpuOperator`, pairs.rs) ------------- */
+typedef struct yb_block yb_block;
+typedef struct yb_operator yb_operator;
+
+/* `GpuFactor::pair_solves` (pairs.rs:153-202): solves A y = e_plus - e_minus for each of `count`
+ * pairs (unknowns, -1 for none; at most yb_factor_block_width of them; the two unknowns of a pair
+ * differ), the right-hand sides built on the device, and keeps the solutions there. */
+int32_t yb_pair_solves(yb_factor *f, int64_t count, const int64_t *plus, const int64_t *minus, yb_block **out);
+/* `GpuFactor::pair_updates` (pairs.rs:204-253, kernels.cu:24-58): the pair solves, then each
+ * column's rank-one update of `base` (n values): x = base + alpha y, w = inverse_weight - c'y,
+ * z = c'x / w, result x + z y, each operation rounded on its own; w = 0 is singular and gives x. */
+int32_t yb_pair_updates(yb_factor *f, const double *base, int64_t count, const int64_t *plus, const int64_t *minus,
+                        const double *alpha, const double *inverse_weight, yb_block **out);
+/* `GpuBlock::columns`; -1 for a null block. */
+int64_t yb_block_columns(const yb_block *b);
+/* `GpuBlock::singular`: one flag per column (all 0 for pair solves). */
+int32_t yb_block_singular(const yb_block *b, int32_t *singular);
+/* `GpuBlock::solutions`: n x columns, column-major, indexed by unknown. */
+int32_t yb_block_solutions(yb_block *b, double *out);
+/* `GpuBlock::maxima` (pairs.rs:293-308, kernels.cu:78-128): each column's largest |value|, its
+ * unknown (the smallest on a tie, -1 if all are zero) and whether any value is not finite. Any
+ * output may be NULL. */
+int32_t yb_block_maxima(yb_block *b, int64_t *row, double *value, int32_t *not_finite);
+/* `GpuBlock::product` (pairs.rs:373-392): the operator's M theta + offset for every column, with
+ * column k's entry at zero_rows[k] set to 0 (-1: none; NULL: none at all), rows x columns
+ * column-major. */
+int32_t yb_block_product(yb_block *b, yb_operator *op, const int64_t *zero_rows, double *out);
+/* `GpuBlock::product_maxima` (pairs.rs:396-413): the products reduced on the device to each
+ * column's largest |value| * weight and its row (ties to the smaller row). */
+int32_t yb_block_product_maxima(yb_block *b, yb_operator *op, const int64_t *zero_rows, int64_t *row, double *value,
+                                int32_t *not_finite);
+void yb_block_free(yb_block *b);
+/* `GpuFactor::operator` (pairs.rs:112-149): a rows x n CSR matrix over the factor's unknowns,
+ * with offset 0 and weights 1. */
+int32_t yb_operator_new(yb_factor *f, int64_t rows, const int64_t *ptr, const int64_t *idx, const double *val,
+                        yb_operator **out);
+/* `GpuOperator::rows`; -1 for a null operator. */
+int64_t yb_operator_rows(const yb_operator *op);
+/* `GpuOperator::set_offset` / `set_weights` (pairs.rs:73-86): one value per row. */
+int32_t yb_operator_set_offset(yb_operator *op, const double *offset);
+int32_t yb_operator_set_weights(yb_operator *op, const double *weights);
+void yb_operator_free(yb_operator *op);
 
 /* Attaches A, the matrix the factor factors (CSR, n x n, natural order, FP64), for refinement:
  * ybus_sparse's `solve_refined` takes it the same way (accuracy.rs:281-308). A copy with its

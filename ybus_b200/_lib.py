@@ -78,11 +78,25 @@ SIGNATURES: dict[str, tuple] = {
     "yb_factor_set_tail_level": (i32, [vp, i32, i32]),
     "yb_factor_set_domain": (i32, [vp, i32, i32, i32, i32, i32]),
     "yb_factor_domain_info": (i32, [vp, i32, P_i32, P_i32, P_i32, P_i64, P_i64, P_i64, P_dbl]),
-    "yb_domain_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp]),
+    "yb_domain_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp, vp]),
     "yb_solve_many": (i32, [vp, vp, i64, vp]),
     "yb_solve_many_device": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
     "yb_solve_many_device_noalloc": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
     "yb_factor_attach_matrix": (i32, [vp, vp, vp, vp]),
+    "yb_pair_solves": (i32, [vp, i64, vp, vp, C.POINTER(vp)]),
+    "yb_pair_updates": (i32, [vp, vp, i64, vp, vp, vp, vp, C.POINTER(vp)]),
+    "yb_block_columns": (i64, [vp]),
+    "yb_block_singular": (i32, [vp, vp]),
+    "yb_block_solutions": (i32, [vp, vp]),
+    "yb_block_maxima": (i32, [vp, vp, vp, vp]),
+    "yb_block_product": (i32, [vp, vp, vp, vp]),
+    "yb_block_product_maxima": (i32, [vp, vp, vp, vp, vp, vp]),
+    "yb_block_free": (None, [vp]),
+    "yb_operator_new": (i32, [vp, i64, vp, vp, vp, C.POINTER(vp)]),
+    "yb_operator_rows": (i64, [vp]),
+    "yb_operator_set_offset": (i32, [vp, vp]),
+    "yb_operator_set_weights": (i32, [vp, vp]),
+    "yb_operator_free": (None, [vp]),
     "yb_solve_many_refined_device": (i32, [vp, vp, i64, vp, i64, i64, i32, dbl, vp, vp, vp]),
 }
 

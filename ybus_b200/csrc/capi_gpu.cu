@@ -713,6 +713,37 @@ void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t
     run(0.0f, f->tile32, f->fwd32, f->bwd32, f->scratch32, f->slices32);
 }
 
+// Solves the right-hand sides e_plus - e_minus of `count` pairs (natural rows, -1 for none) into
+// `out` (n x count, natural order), with each column's rank-one update of `base` when `base` is
+// given (then alpha, inverse_weight and singular too). The domain solve where the factor admits it,
+// else the global-scratch solve.
+void solve_pairs_device(yb_factor *f, int64_t count, const int32_t *plus, const int32_t *minus, const double *base,
+                        const double *alpha, const double *inverse_weight, int32_t *singular, double *out, int64_t ldo,
+                        cudaStream_t stream) {
+  if (count <= 0 || f->n == 0) return;
+  TileConfig cfg = resolve<double>(f, f->tile64);
+  if (cfg.kind == kTileDomain) {
+    if (base) {
+      PairIO<true> io{plus, minus, out, ldo, f->in_slot.get(), f->out_slot.get(), base, alpha, inverse_weight, singular};
+      launch_domain<double>(f, cfg, count, io, stream);
+    } else {
+      PairIO<false> io{plus, minus, out, ldo, f->in_slot.get(), f->out_slot.get(), nullptr, nullptr, nullptr, nullptr};
+      launch_domain<double>(f, cfg, count, io, stream);
+    }
+    return;
+  }
+  cfg = f->tile64;
+  cfg.kind = kTileGlobal;
+  auto a = base_args<double>(f, f->fwd64, f->bwd64);
+  a.x = out, a.ldx = ldo, a.count = count;
+  a.plus = plus, a.minus = minus;
+  a.base = base, a.alpha = alpha, a.inverse_weight = inverse_weight, a.singular = singular;
+  if (base)
+    launch_tiles<double, Load::Pairs, Store::PairUpdate>(f, a, cfg, stream, f->scratch64);
+  else
+    launch_tiles<double, Load::Pairs, Store::Dense>(f, a, cfg, stream, f->scratch64);
+}
+
 }  // namespace yb
 
 extern "C" int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,

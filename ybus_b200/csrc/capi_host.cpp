@@ -328,7 +328,8 @@ void yb_host_factor_free(yb_host_factor *f) { delete f; }
 
 int32_t yb_domain_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
                                   const int64_t *perm, int32_t value_bytes, int32_t warps, int32_t page_bytes,
-                                  int32_t cut, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *top_slot) {
+                                  int32_t cut, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *top_slot,
+                                  double *top_condition) {
   return guard([&] {
     require(n >= 0 && l_ptr && perm && info, "null argument");
     host::Compressed<double> lower;
@@ -353,6 +354,7 @@ int32_t yb_domain_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t
     if (blob) std::copy(lay.blob.begin(), lay.blob.end(), blob);
     if (warp_page) std::copy(lay.warp_page.begin(), lay.warp_page.end(), warp_page);
     if (top_slot) std::copy(lay.tail_slot.begin(), lay.tail_slot.end(), top_slot);
+    if (top_condition) *top_condition = lay.top_condition;
     return YB_OK;
   });
 }

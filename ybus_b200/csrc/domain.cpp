@@ -398,6 +398,22 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
           }
         }
       }
+      if (emit) {
+        // the infinity-norm condition of each triangle: the explicit inverses stand in for
+        // substitution only while it is small (their rounding grows with it)
+        auto cond = [m](const std::vector<double> &tri, const std::vector<double> &inv, bool lower) {
+          double tn = 0, in = 0;
+          for (int32_t i = 0; i < m; ++i) {
+            double ts = 0, is = 0;
+            for (int32_t j = 0; j < m; ++j) ts += std::fabs(tri[(size_t)i * m + j]);
+            for (int32_t j = lower ? 0 : i; j < (lower ? i + 1 : m); ++j)
+              is += std::fabs(lower ? inv[(size_t)i * (i + 1) / 2 + j] : inv[(size_t)i * m - (size_t)i * (i - 1) / 2 + (j - i)]);
+            tn = std::max(tn, ts), in = std::max(in, is);
+          }
+          return tn * in;
+        };
+        out->top_condition = std::max(cond(Lt, dense_inv_f, true), cond(Ut, dense_inv_b, false));
+      }
       // dense rows, dealt to balance their lengths: forward row t has t + 1 entries, backward m - t
       const int64_t dense_fixed = 32;
       const int64_t dense_max = (page_bytes - dense_fixed - 16) / value_bytes / 4 * 4;
@@ -483,37 +499,47 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
     return cycles;
   };
 
-  // The cut: as asked, or the cheapest valid one with a top of at most kMaxTop rows
+  // The cut: as asked, or the cheapest valid one with a top of at most kMaxTop rows whose dense
+  // triangles are well conditioned
   constexpr int32_t kMaxTop = 768;
-  int32_t K = K_in;
-  if (K > levels) K = levels;
-  if (K < 0) {
-    double best = std::numeric_limits<double>::infinity();
-    for (int32_t k = levels; k >= 1; --k) {
-      int32_t top = 0;
-      for (int32_t l = k; l < levels; ++l) top += F.level_ptr[l + 1] - F.level_ptr[l];
-      if (top > kMaxTop) break;
-      const Cut c = make_cut(k);
-      if (!valid(c.top)) continue;
-      const double cost = build(c, false, nullptr);
-      if (cost < best) best = cost, K = k;
-    }
-    if (K < 0) throw Error(host::kInvalidArgument, "the factor admits no domain cut");
+  constexpr double kMaxTopCondition = 1e4;
+  auto emit_cut = [&](int32_t K) {
+    const Cut c = make_cut(K);
+    if (!valid(c.top)) throw Error(host::kInvalidArgument, "an upper-triangle entry of a top row reaches below the cut");
+    if (c.tail > 4096) throw Error(host::kInvalidArgument, "the top block is too large");
+    DomainLayout out;
+    out.warps = warps;
+    out.page_bytes = page_bytes;
+    out.value_bytes = value_bytes;
+    out.K = K;
+    out.tail = c.tail;
+    out.tail_slot.assign(c.tail, 0);
+    for (int32_t i = 0; i < n; ++i)
+      if (c.top[i]) out.tail_slot[c.tail_index[i]] = i;
+    out.cost = build(c, true, &out);
+    return out;
+  };
+  if (K_in >= 0) {
+    DomainLayout out = emit_cut(std::min(K_in, levels));
+    if (!(out.top_condition <= kMaxTopCondition))
+      throw Error(host::kInvalidArgument, "the top block is too ill-conditioned for its explicit inverse");
+    return out;
   }
-  const Cut c = make_cut(K);
-  if (!valid(c.top)) throw Error(host::kInvalidArgument, "an upper-triangle entry of a top row reaches below the cut");
-  if (c.tail > 4096) throw Error(host::kInvalidArgument, "the top block is too large");
-  DomainLayout out;
-  out.warps = warps;
-  out.page_bytes = page_bytes;
-  out.value_bytes = value_bytes;
-  out.K = K;
-  out.tail = c.tail;
-  out.tail_slot.assign(c.tail, 0);
-  for (int32_t i = 0; i < n; ++i)
-    if (c.top[i]) out.tail_slot[c.tail_index[i]] = i;
-  out.cost = build(c, true, &out);
-  return out;
+  std::vector<std::pair<double, int32_t>> candidates;
+  for (int32_t k = levels; k >= 1; --k) {
+    int32_t top = 0;
+    for (int32_t l = k; l < levels; ++l) top += F.level_ptr[l + 1] - F.level_ptr[l];
+    if (top > kMaxTop) break;
+    const Cut c = make_cut(k);
+    if (!valid(c.top)) continue;
+    candidates.emplace_back(build(c, false, nullptr), k);
+  }
+  std::stable_sort(candidates.begin(), candidates.end());
+  for (auto [cost, k] : candidates) {
+    DomainLayout out = emit_cut(k);
+    if (out.top_condition <= kMaxTopCondition) return out;
+  }
+  throw Error(host::kInvalidArgument, "the factor admits no domain cut");
 }
 
 template DomainLayout domain_layout(const Plan<double> &, int32_t, int32_t, int32_t, int32_t);

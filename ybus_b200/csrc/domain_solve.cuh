@@ -147,6 +147,83 @@ struct DenseIO {
   }
 };
 
+// Right-hand sides e_plus - e_minus built on the device (ybus_cuda/src/kernels.cu:5-17: the
+// reference zeroes an n x width block and scatters the pairs; here the tile's slots are zeroed in
+// shared memory), solutions stored in natural order. With UPDATE, each column's rank-one
+// Sherman-Morrison update of `base` replaces the plain store (ybus_cuda/src/kernels.cu:24-58):
+// x = base + alpha y, w = inverse_weight - c'y, z = c'x / w, out = x + z y, every operation
+// rounded on its own as the reference's kernel (built with --fmad=false) rounds it; w = 0 flags the
+// column singular and stores x. `plus`/`minus` are natural rows (-1: none), as right-hand-side rows
+// for the load and as solution rows for the update.
+template <bool UPDATE> struct PairIO {
+  static constexpr bool kRefine = false;
+  const int32_t *__restrict__ plus;
+  const int32_t *__restrict__ minus;
+  double *__restrict__ out;
+  int64_t ldo;
+  const int32_t *__restrict__ in_slot;
+  const int32_t *__restrict__ out_slot;
+  const double *__restrict__ base;            // UPDATE: [n], natural order
+  const double *__restrict__ alpha;           // UPDATE: [count]
+  const double *__restrict__ inverse_weight;  // UPDATE: [count]
+  int32_t *__restrict__ singular;             // UPDATE: [count]
+
+  template <class T, int W>
+  __device__ __forceinline__ void load(int64_t col0, int64_t count, int n, T *Ys) const {
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+      T t[W];
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) t[cc] = T(0);
+      store_w<T, W>(Ys + (size_t)r * W, t);
+    }
+    __syncthreads();
+    if (threadIdx.x < W && col0 + threadIdx.x < count) {
+      const int64_t col = col0 + threadIdx.x;
+      const int p = __ldg(plus + col), m = __ldg(minus + col);
+      if (p >= 0) Ys[(size_t)__ldg(in_slot + p) * W + threadIdx.x] = T(1);
+      if (m >= 0) Ys[(size_t)__ldg(in_slot + m) * W + threadIdx.x] = T(-1);
+    }
+  }
+
+  template <int W> __device__ __forceinline__ void prefetch(int64_t, int64_t, int) const {}
+
+  template <class T, int W>
+  __device__ __forceinline__ void store(int64_t col0, int64_t count, int n, const T *Ys) const {
+    if constexpr (!UPDATE) {
+      DenseIO::store_columns<T, W>(out, ldo, out_slot, col0, count, n, Ys);
+    } else {
+#pragma unroll 1
+      for (int cc = 0; cc < W; ++cc) {
+        const int64_t col = col0 + cc;
+        if (col >= count) break;
+        const int p = __ldg(plus + col), m = __ldg(minus + col);
+        const double a = __ldg(alpha + col);
+        double cy = 0.0, cx = 0.0;
+        if (p >= 0) {
+          const double yp = (double)Ys[(size_t)__ldg(out_slot + p) * W + cc];
+          cy = __dadd_rn(cy, yp);
+          cx = __dadd_rn(cx, __dadd_rn(__ldg(base + p), __dmul_rn(a, yp)));
+        }
+        if (m >= 0) {
+          const double ym = (double)Ys[(size_t)__ldg(out_slot + m) * W + cc];
+          cy = __dsub_rn(cy, ym);
+          cx = __dsub_rn(cx, __dadd_rn(__ldg(base + m), __dmul_rn(a, ym)));
+        }
+        const double w = __dadd_rn(-cy, __ldg(inverse_weight + col));
+        const bool sing = (w == 0.0);
+        const double z = sing ? 0.0 : __ddiv_rn(cx, w);
+        if (threadIdx.x == 0) singular[col] = sing ? 1 : 0;
+        double *o = out + col * ldo;
+        for (int r = threadIdx.x; r < n; r += blockDim.x) {
+          const double y = (double)Ys[(size_t)__ldg(out_slot + r) * W + cc];
+          const double xr = __dadd_rn(__ldg(base + r), __dmul_rn(a, y));
+          o[r] = sing ? xr : __dadd_rn(xr, __dmul_rn(z, y));
+        }
+      }
+    }
+  }
+};
+
 // Iterative refinement (ybus_sparse's `refine_normwise`, accuracy.rs:83-122): the substitutions in
 // the precision of the tile (FP32); the residual and the update x += d in FP64 against the FP64
 // matrix A. Pass 0 loads b into the slots and into the block's FP64 residual scratch R (natural row

@@ -123,6 +123,9 @@ struct yb_factor {
 };
 
 namespace yb {
+void solve_pairs_device(yb_factor *f, int64_t count, const int32_t *plus, const int32_t *minus, const double *base,
+                        const double *alpha, const double *inverse_weight, int32_t *singular, double *out, int64_t ldo,
+                        cudaStream_t stream);
 void solve_single_row_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
                              cudaStream_t stream);
 }

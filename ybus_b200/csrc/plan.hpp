@@ -130,6 +130,7 @@ struct DomainLayout {
   std::vector<int32_t> warp_page;   // [warps + 1]
   int64_t records = 0, entries = 0, dense_entries = 0;
   double cost = 0;                  // the cost model's estimate for the chosen K (cycles per tile)
+  double top_condition = 0;         // infinity-norm condition of the worse of L_TT and U_TT (0: no T)
 };
 
 // Builds the domain layout of `plan` for values of `value_bytes` (8 or 4). K < 0 picks the cut by

@@ -248,8 +248,169 @@ class GpuFactor:
         _check(lib().yb_solve_many_refined_device(self._h, d_rhs, ldb or n, d_out, ldx or n, count, max_steps,
                                                   float(tolerance), d_ratio, d_steps, stream))
 
+    def operator(self, matrix) -> "GpuOperator":
+        """`GpuFactor::operator` (pairs.rs:112-149): a CSR matrix (host.Matrix or (rows, ptr, idx, val))
+        with one column per unknown."""
+        if hasattr(matrix, "arrays"):
+            m = matrix.to_csr()
+            rows = m.shape[0]
+            p, i, v = m.arrays()
+        else:
+            rows, p, i, v = matrix
+        p, i, v = np.ascontiguousarray(p, np.int64), np.ascontiguousarray(i, np.int64), np.ascontiguousarray(v, np.float64)
+        out = C.c_void_p()
+        _check(lib().yb_operator_new(self._h, rows, ptr(p), ptr(i), ptr(v), C.byref(out)))
+        return GpuOperator(self, out.value)
+
+
+    def pair_solves(self, pairs) -> "GpuBlock":
+        """`GpuFactor::pair_solves` (pairs.rs:194-202)."""
+        plus, minus = _pair_arrays(pairs)
+        out = C.c_void_p()
+        _check(lib().yb_pair_solves(self._h, plus.size, ptr(plus), ptr(minus), C.byref(out)))
+        return GpuBlock(self, out.value)
+
+
+    def pair_updates(self, base, updates) -> "GpuBlock":
+        """`GpuFactor::pair_updates` (pairs.rs:209-253)."""
+        base = np.ascontiguousarray(base, dtype=np.float64)
+        if base.size != self.dim():
+            raise ValueError("one base value per unknown")
+        plus, minus = _pair_arrays([u.pair for u in updates])
+        alpha = np.array([u.alpha for u in updates], np.float64)
+        inv = np.array([u.inverse_weight for u in updates], np.float64)
+        out = C.c_void_p()
+        _check(lib().yb_pair_updates(self._h, ptr(base), plus.size, ptr(plus), ptr(minus), ptr(alpha), ptr(inv),
+                                     C.byref(out)))
+        return GpuBlock(self, out.value)
+
     def solve_many_device(self, d_rhs: int, d_out: int, count: int, precision: int = FP64, stream: int | None = None,
                           ldb: int | None = None, ldx: int | None = None) -> None:
         """The solve on device pointers (column-major n x count), asynchronous on `stream`."""
         n = self.dim()
         _check(lib().yb_solve_many_device(self._h, d_rhs, ldb or n, d_out, ldx or n, count, precision, stream))
+
+
+# ---- blocks solved on the device (ybus_cuda/src/pairs.rs) ----------------------------------------
+
+@dataclass(frozen=True)
+class Pair:
+    """A right-hand side e_plus − e_minus over the unknowns (None for no entry) (pairs.rs:17)."""
+    plus: int | None
+    minus: int | None
+
+
+@dataclass(frozen=True)
+class PairUpdate:
+    """One column of `pair_updates` (pairs.rs:30): x = base + alpha y, w = inverse_weight − cᵀy,
+    z = cᵀx / w, result x + z y."""
+    pair: Pair
+    alpha: float
+    inverse_weight: float
+
+
+@dataclass(frozen=True)
+class ColumnMax:
+    """A column's largest |value| · weight (pairs.rs:42): its row (None if all are zero), the value,
+    and whether any value isn't finite."""
+    row: int | None
+    value: float
+    not_finite: bool
+
+
+def _pair_arrays(pairs):
+    plus = np.array([-1 if p.plus is None else p.plus for p in pairs], np.int64)
+    minus = np.array([-1 if p.minus is None else p.minus for p in pairs], np.int64)
+    return plus, minus
+
+
+def _maxima(rows, values, bad):
+    return [ColumnMax(None if r < 0 else int(r), float(v), bool(b)) for r, v, b in zip(rows, values, bad)]
+
+
+class GpuOperator:
+    """A sparse matrix over a factor's unknowns, applied to a block's columns (pairs.rs:55-86)."""
+
+    def __init__(self, factor: "GpuFactor", handle: int):
+        self.factor = factor
+        self._h = C.c_void_p(handle)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().yb_operator_free(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def rows(self) -> int:
+        return lib().yb_operator_rows(self._h)
+
+    def set_offset(self, offset) -> None:
+        offset = np.ascontiguousarray(offset, dtype=np.float64)
+        if offset.size != self.rows():
+            raise ValueError("one offset per row")
+        _check(lib().yb_operator_set_offset(self._h, ptr(offset)))
+
+    def set_weights(self, weights) -> None:
+        weights = np.ascontiguousarray(weights, dtype=np.float64)
+        if weights.size != self.rows():
+            raise ValueError("one weight per row")
+        _check(lib().yb_operator_set_weights(self._h, ptr(weights)))
+
+
+class GpuBlock:
+    """Solutions kept on the device, one column per pair (pairs.rs:90-110)."""
+
+    def __init__(self, factor: "GpuFactor", handle: int):
+        self.factor = factor
+        self._h = C.c_void_p(handle)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().yb_block_free(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def columns(self) -> int:
+        return lib().yb_block_columns(self._h)
+
+    def singular(self) -> list[bool]:
+        out = np.zeros(max(self.columns(), 1), np.int32)
+        _check(lib().yb_block_singular(self._h, ptr(out)))
+        return [bool(v) for v in out[: self.columns()]]
+
+    def solutions(self) -> np.ndarray:
+        out = np.zeros((self.columns(), self.factor.dim()))
+        _check(lib().yb_block_solutions(self._h, ptr(out)))
+        return out
+
+    def maxima(self) -> list[ColumnMax]:
+        k = self.columns()
+        rows, values, bad = np.zeros(max(k, 1), np.int64), np.zeros(max(k, 1)), np.zeros(max(k, 1), np.int32)
+        _check(lib().yb_block_maxima(self._h, ptr(rows), ptr(values), ptr(bad)))
+        return _maxima(rows[:k], values[:k], bad[:k])
+
+    @staticmethod
+    def _zero(zero, k):
+        return np.array([-1 if z is None else z for z in zero], np.int64) if zero is not None else np.full(k, -1, np.int64)
+
+    def product(self, op: GpuOperator, zero=None) -> np.ndarray:
+        k = self.columns()
+        z = self._zero(zero, k)
+        out = np.zeros((k, op.rows()))
+        _check(lib().yb_block_product(self._h, op._h, ptr(z), ptr(out)))
+        return out
+
+    def product_maxima(self, op: GpuOperator, zero=None) -> list[ColumnMax]:
+        k = self.columns()
+        z = self._zero(zero, k)
+        rows, values, bad = np.zeros(max(k, 1), np.int64), np.zeros(max(k, 1)), np.zeros(max(k, 1), np.int32)
+        _check(lib().yb_block_product_maxima(self._h, op._h, ptr(z), ptr(rows), ptr(values), ptr(bad)))
+        return _maxima(rows[:k], values[:k], bad[:k])
+
+

@@ -186,12 +186,13 @@ def domain_layout(chol: HostCholesky, value_bytes: int = 8, warps: int = 16, pag
     l = chol.l
     val = np.ascontiguousarray(l.val, dtype=np.float64)
     args = (chol.n, ptr(l.ptr), ptr(l.idx), ptr(val), ptr(chol.perm), value_bytes, warps, page_bytes, cut)
-    check(lib().yb_domain_layout_cholesky(*args, ptr(info), None, None, None))
+    check(lib().yb_domain_layout_cholesky(*args, ptr(info), None, None, None, None))
     cut_, top, stages, w, pages, records, entries, pb = (int(v) for v in info)
     blob = np.zeros(pages * pb, np.uint8)
     warp_page = np.zeros(w + 1, np.int32)
     top_slot = np.zeros(max(top, 1), np.int32)
-    check(lib().yb_domain_layout_cholesky(*args, ptr(info), ptr(blob), ptr(warp_page), ptr(top_slot)))
+    cond = C.c_double()
+    check(lib().yb_domain_layout_cholesky(*args, ptr(info), ptr(blob), ptr(warp_page), ptr(top_slot), C.byref(cond)))
     return {"cut": cut_, "top": top, "stages": stages, "warps": w, "pages": pages, "records": records,
             "entries": entries, "page_bytes": pb, "blob": blob, "warp_page": warp_page, "top_slot": top_slot[:top],
-            "value_bytes": value_bytes}
+            "value_bytes": value_bytes, "top_condition": cond.value}
