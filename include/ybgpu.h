@@ -242,6 +242,48 @@ int32_t yb_operator_set_offset(yb_operator *op, const double *offset);
 int32_t yb_operator_set_weights(yb_operator *op, const double *weights);
 void yb_operator_free(yb_operator *op);
 
+/* ---- the DC callers (ybus_powerflow/src/dc/gpu.rs: `DcGpuStudy`, `DcGpuSensitivity`) ---------- */
+typedef struct yb_dc_network yb_dc_network;
+
+/* A DC network from its branch list (bus indices, reactances x; no taps or shifters): Bbus and Bf
+ * stamped as ybus_powerflow's `Bdc::new` stamps them (dc.rs:79-113: b = 1/x, parallel branches
+ * summed), B' = Bbus without the slack's row and column factored by AMD Cholesky on the host
+ * (`DcModel::factor_over`, dc.rs:368-407) and uploaded with B' attached, Bf kept as an operator on
+ * the solutions, and the bridges found (islands.rs:132-176). The unknowns are the buses other than
+ * the slack, in bus order. */
+int32_t yb_dc_network_new(yb_gpu *gpu, int64_t n_bus, int64_t n_branch, const int64_t *from, const int64_t *to,
+                          const double *x, int64_t slack, yb_dc_network **out);
+void yb_dc_network_free(yb_dc_network *net);
+/* The network's uploaded factor (owned by the network). */
+yb_factor *yb_dc_network_factor(yb_dc_network *net);
+/* One flag per branch: whether it is a bridge (its outage islands the network). */
+int32_t yb_dc_bridges(const yb_dc_network *net, uint8_t *bridge);
+/* `DcGpuSensitivity::ptdf_columns` (gpu.rs:506-528; sensitivity.rs:233): for an injection at each
+ * of `count` buses, withdrawn at the slack, every branch's flow: n_branch x count, column-major. */
+int32_t yb_dc_ptdf_columns(yb_dc_network *net, int64_t count, const int64_t *buses, double *out);
+/* `DcGpuSensitivity::ptdf_transfers` (gpu.rs:532; sensitivity.rs:284): a transfer from each
+ * from_bus to its to_bus. */
+int32_t yb_dc_ptdf_transfers(yb_dc_network *net, int64_t count, const int64_t *from_bus, const int64_t *to_bus,
+                             double *out);
+/* `DcSensitivity::lodf_columns` on the GPU (sensitivity.rs:322-362): for the outage of each branch,
+ * every branch's change in flow as a fraction of its flow before, -1 for itself, a NaN column for a
+ * bridge; n_branch x count. */
+int32_t yb_dc_lodf_columns(yb_dc_network *net, int64_t count, const int64_t *branches, double *out);
+/* No ybus counterpart as such (the reference screens one base per outage, `DcGpuStudy::
+ * outage_loadings`, gpu.rs:334-430): N-1 screening of many injection scenarios per outage. Case c
+ * takes out branch outaged[c] (a rank-one update of B', dc/outage.rs:126-241) and has the scenario
+ * columns scenario_ptr[c] .. scenario_ptr[c+1] - 1 of `injections` (n_bus x total, column-major, by
+ * bus; the slack's entry is ignored). For every scenario column: the branch with the largest
+ * |flow| * weight (weights NULL: 1), the loading, whether any flow is not finite; per case whether
+ * the update is singular (1/b - c'y = 0: a bridge). All cases run as one pair solve and one
+ * scenario solve with the update, flows and maxima fused (YB_FP64), captured in a CUDA graph that
+ * later calls of the same sizes replay; or with FP32 substitution and FP64 refinement, then the
+ * same epilogue (YB_FP32; the slack must be bus 0). */
+int32_t yb_dc_outage_loadings_batch(yb_dc_network *net, int64_t cases, const int64_t *outaged,
+                                    const int64_t *scenario_ptr, const double *injections, const double *weights,
+                                    int32_t precision, int64_t *max_branch, double *max_loading, int32_t *not_finite,
+                                    int32_t *singular);
+
 /* Attaches A, the matrix the factor factors (CSR, n x n, natural order, FP64), for refinement:
  * ybus_sparse's `solve_refined` takes it the same way (accuracy.rs:281-308). A copy with its
  * columns mapped to the factor's solution order is kept on the device. */

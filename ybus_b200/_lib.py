@@ -97,6 +97,14 @@ SIGNATURES: dict[str, tuple] = {
     "yb_operator_set_offset": (i32, [vp, vp]),
     "yb_operator_set_weights": (i32, [vp, vp]),
     "yb_operator_free": (None, [vp]),
+    "yb_dc_network_new": (i32, [vp, i64, i64, vp, vp, vp, i64, C.POINTER(vp)]),
+    "yb_dc_network_free": (None, [vp]),
+    "yb_dc_network_factor": (vp, [vp]),
+    "yb_dc_bridges": (i32, [vp, vp]),
+    "yb_dc_ptdf_columns": (i32, [vp, i64, vp, vp]),
+    "yb_dc_ptdf_transfers": (i32, [vp, i64, vp, vp, vp]),
+    "yb_dc_lodf_columns": (i32, [vp, i64, vp, vp]),
+    "yb_dc_outage_loadings_batch": (i32, [vp, i64, vp, vp, vp, vp, i32, vp, vp, vp, vp]),
     "yb_solve_many_refined_device": (i32, [vp, vp, i64, vp, i64, i64, i32, dbl, vp, vp, vp]),
 }
 

@@ -1,0 +1,471 @@
+// C ABI of the DC callers of the solve path (ybus_powerflow/src/dc/gpu.rs: `DcGpuStudy`,
+// `DcGpuSensitivity`), for networks given as branch lists: B' and Bf built from the branch
+// stamps (ybus_powerflow/src/dc.rs:79-113: b = 1/x, parallel branches summed), B' factored by AMD
+// Cholesky on the host and uploaded, Bf kept as an operator on the solutions. On top of the
+// factor's pair solves and products: PTDF columns and transfers (dc/sensitivity.rs:233-300),
+// LODF columns with bridges masked (dc/sensitivity.rs:322-362, islands.rs:132-176), and the
+// batched N-1 screening of many injection scenarios per outage, in FP64 with the rank-one
+// outage update, the flows and their maxima fused into the solve, or in FP32 with FP64
+// refinement followed by the same epilogue.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "../../include/ybgpu.h"
+#include "capi_common.hpp"
+#include "device.cuh"
+#include "domain_solve.cuh"
+#include "factor_state.cuh"
+
+using namespace yb;
+using host::idx_t;
+
+namespace yb {
+// From capi_gpu.cu: the domain solve's launch for an IO policy, with the tile the factor resolves to.
+void launch_outage_domain(yb_factor *f, int64_t count, const OutageIO &io, cudaStream_t stream);
+}  // namespace yb
+
+struct yb_dc_network {
+  yb_gpu *gpu = nullptr;
+  int64_t n_bus = 0, n_branch = 0, slack = 0, n = 0;
+  std::vector<int64_t> from, to, unknown;  // unknown: per bus, -1 for the slack
+  std::vector<double> b;
+  std::vector<uint8_t> bridge;
+  yb_factor *factor = nullptr;
+  yb_operator *flows = nullptr;
+  // the screening's device data: per branch, per bus, and the workspace of the last batch size
+  DeviceArray<int32_t> br_slot_f, br_slot_t, br_u_f, br_u_t, bus_slot;
+  DeviceArray<double> br_b;
+  DeviceArray<double> d_weight, d_inj, d_y, d_theta, d_cy, d_invb, d_ratio;
+  DeviceArray<int32_t> d_case_of, d_plus_u, d_minus_u, d_plus_slot, d_minus_slot, d_branch, d_bad, d_sing, d_steps;
+  DeviceArray<int64_t> d_row;
+  DeviceArray<double> d_value;
+  // a captured graph of the FP64 screening for the sizes it was made for
+  cudaGraphExec_t graph = nullptr;
+  int64_t graph_cases = -1, graph_columns = -1;
+  ~yb_dc_network() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (flows) yb_operator_free(flows);
+    if (factor) yb_factor_free(factor);
+  }
+};
+
+namespace {
+
+// Bridges of a multigraph (ybus_powerflow/src/islands.rs:132-176): parallel branches are separate
+// edges, so neither of a parallel pair is a bridge; a self-loop never is. Iterative DFS.
+std::vector<uint8_t> find_bridges(int64_t n_bus, const std::vector<int64_t> &from, const std::vector<int64_t> &to) {
+  const int64_t m = (int64_t)from.size();
+  std::vector<std::vector<std::pair<int64_t, int64_t>>> adj(n_bus);
+  for (int64_t k = 0; k < m; ++k)
+    if (from[k] != to[k]) adj[from[k]].push_back({to[k], k}), adj[to[k]].push_back({from[k], k});
+  std::vector<int64_t> disc(n_bus, -1), low(n_bus, 0);
+  std::vector<uint8_t> bridge(m, 0);
+  int64_t timer = 0;
+  struct Frame {
+    int64_t node, via;
+    size_t next;
+  };
+  std::vector<Frame> stack;
+  for (int64_t root = 0; root < n_bus; ++root) {
+    if (disc[root] >= 0) continue;
+    disc[root] = low[root] = timer++;
+    stack.push_back({root, -1, 0});
+    while (!stack.empty()) {
+      Frame &fr = stack.back();
+      if (fr.next < adj[fr.node].size()) {
+        const auto [nxt, k] = adj[fr.node][fr.next++];
+        if (k == fr.via) continue;
+        if (disc[nxt] < 0) {
+          disc[nxt] = low[nxt] = timer++;
+          stack.push_back({nxt, k, 0});
+        } else {
+          low[fr.node] = std::min(low[fr.node], disc[nxt]);
+        }
+      } else {
+        const Frame done = fr;
+        stack.pop_back();
+        if (!stack.empty()) {
+          Frame &parent = stack.back();
+          low[parent.node] = std::min(low[parent.node], low[done.node]);
+          if (low[done.node] > disc[parent.node]) bridge[done.via] = 1;
+        }
+      }
+    }
+  }
+  return bridge;
+}
+
+yb_dc_network *check(yb_dc_network *net) {
+  require(net != nullptr, "null network");
+  return net;
+}
+
+// Solves pairs in chunks of the factor's block width and returns the flows (n_branch x count).
+std::vector<double> pair_flows(yb_dc_network *net, const std::vector<int64_t> &plus, const std::vector<int64_t> &minus) {
+  const int64_t count = (int64_t)plus.size();
+  std::vector<double> out((size_t)(net->n_branch * count));
+  const int64_t width = std::max<int64_t>(1, yb_factor_block_width(net->factor));
+  for (int64_t k0 = 0; k0 < count; k0 += width) {
+    const int64_t k1 = std::min(count, k0 + width);
+    yb_block *blk = nullptr;
+    int32_t st = yb_pair_solves(net->factor, k1 - k0, plus.data() + k0, minus.data() + k0, &blk);
+    if (st != YB_OK) throw host::Error(st, "pair solves failed");
+    st = yb_block_product(blk, net->flows, nullptr, out.data() + k0 * net->n_branch);
+    yb_block_free(blk);
+    if (st != YB_OK) throw host::Error(st, "flow products failed");
+  }
+  return out;
+}
+
+// The epilogue of the FP32-and-refinement screening: as OutageIO's, with theta from an array in
+// natural unknown order. One block of 256 threads per column.
+__global__ void outage_epilogue_kernel(const double *__restrict__ theta, int64_t ldt, const int32_t *__restrict__ case_of,
+                                       const int32_t *__restrict__ c_plus_u, const int32_t *__restrict__ c_minus_u,
+                                       const double *__restrict__ c_invb, const double *__restrict__ c_cy,
+                                       const int32_t *__restrict__ c_branch, const double *__restrict__ Y, int64_t ldy,
+                                       int32_t n_branch, const int32_t *__restrict__ br_u_f,
+                                       const int32_t *__restrict__ br_u_t, const double *__restrict__ br_b,
+                                       const double *__restrict__ weight, int64_t *__restrict__ out_row,
+                                       double *__restrict__ out_value, int32_t *__restrict__ out_bad,
+                                       int32_t *__restrict__ case_singular) {
+  __shared__ double red_v[8];
+  __shared__ int red_r[8], red_b[8];
+  const int64_t col = blockIdx.x;
+  const double *th = theta + col * ldt;
+  const int c = case_of[col];
+  const double *y = Y + (int64_t)c * ldy;
+  const int p = c_plus_u[c], m = c_minus_u[c];
+  const double cx = __dsub_rn(__dadd_rn(0.0, p >= 0 ? th[p] : 0.0), m >= 0 ? th[m] : 0.0);
+  const double w = __dadd_rn(-c_cy[c], c_invb[c]);
+  const bool sing = (w == 0.0);
+  const double z = sing ? 0.0 : __ddiv_rn(cx, w);
+  const int k = c_branch[c];
+  double v = 0.0;
+  int row = -1, bad = 0;
+  for (int l = threadIdx.x; l < n_branch; l += blockDim.x) {
+    const int uf = br_u_f[l], ut = br_u_t[l];
+    const double tf = uf < 0 ? 0.0 : __dadd_rn(th[uf], __dmul_rn(z, y[uf]));
+    const double tt = ut < 0 ? 0.0 : __dadd_rn(th[ut], __dmul_rn(z, y[ut]));
+    const double f = l == k ? 0.0 : __dadd_rn(__dmul_rn(br_b[l], tf), __dmul_rn(-br_b[l], tt));
+    if (!isfinite(f)) {
+      bad = 1;
+      continue;
+    }
+    const double load = fabs(f) * weight[l];
+    if (load > v) v = load, row = l;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double v2 = __shfl_xor_sync(0xffffffffu, v, off);
+    const int r2 = __shfl_xor_sync(0xffffffffu, row, off);
+    bad |= __shfl_xor_sync(0xffffffffu, bad, off);
+    better_max(v, row, v2, r2);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red_v[warp] = v, red_r[warp] = row, red_b[warp] = bad;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w2 = 1; w2 < (int)(blockDim.x >> 5); ++w2) {
+      better_max(v, row, red_v[w2], red_r[w2]);
+      bad |= red_b[w2];
+    }
+    out_row[col] = row;
+    out_value[col] = row >= 0 ? v : 0.0;
+    out_bad[col] = bad;
+    case_singular[c] = sing ? 1 : 0;
+  }
+}
+
+// c'y of each case, summed as the reference's update sums it: 0 + y_plus - y_minus
+__global__ void case_cy_kernel(const double *__restrict__ Y, int64_t ldy, const int32_t *__restrict__ plus_u,
+                               const int32_t *__restrict__ minus_u, int64_t cases, double *__restrict__ cy) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cases) return;
+  const double *y = Y + c * ldy;
+  double s = 0.0;
+  if (plus_u[c] >= 0) s = __dadd_rn(s, y[plus_u[c]]);
+  if (minus_u[c] >= 0) s = __dsub_rn(s, y[minus_u[c]]);
+  cy[c] = s;
+}
+
+}  // namespace
+
+extern "C" int32_t yb_dc_network_new(yb_gpu *gpu, int64_t n_bus, int64_t n_branch, const int64_t *from,
+                                     const int64_t *to, const double *x, int64_t slack, yb_dc_network **out) {
+  return guard([&] {
+    require(gpu && out, "null argument");
+    require(n_bus >= 2 && n_branch >= 1, "a network needs two buses and a branch");
+    require(from && to && x, "null branch arrays");
+    require(slack >= 0 && slack < n_bus, "the slack bus is out of range");
+    auto net = std::make_unique<yb_dc_network>();
+    net->gpu = gpu;
+    net->n_bus = n_bus, net->n_branch = n_branch, net->slack = slack, net->n = n_bus - 1;
+    net->from.assign(from, from + n_branch);
+    net->to.assign(to, to + n_branch);
+    net->b.resize(n_branch);
+    for (int64_t k = 0; k < n_branch; ++k) {
+      require(from[k] >= 0 && from[k] < n_bus && to[k] >= 0 && to[k] < n_bus, "a branch end is out of range");
+      require(x[k] != 0.0 && std::isfinite(x[k]), "a branch reactance is zero or not finite");
+      net->b[k] = 1.0 / x[k];
+    }
+    net->unknown.assign(n_bus, -1);
+    for (int64_t i = 0, u = 0; i < n_bus; ++i)
+      if (i != slack) net->unknown[i] = u++;
+    // Bbus stamps per branch (f,f,b), (f,t,-b), (t,f,-b), (t,t,b), duplicates summed in order;
+    // B' is Bbus without the slack's row and column
+    std::vector<host::Triplet<double>> t;
+    t.reserve(4 * n_branch);
+    for (int64_t k = 0; k < n_branch; ++k) {
+      const int64_t f = from[k], g = to[k];
+      const double bk = net->b[k];
+      t.push_back({f, f, bk});
+      t.push_back({f, g, -bk});
+      t.push_back({g, f, -bk});
+      t.push_back({g, g, bk});
+    }
+    const auto bbus = host::from_triplets<double>(n_bus, n_bus, t, true);
+    std::vector<idx_t> keep;
+    for (int64_t i = 0; i < n_bus; ++i)
+      if (i != slack) keep.push_back(i);
+    const auto bp = host::select(bbus, keep, keep);
+    const auto graph = host::adjacency_of(bp);
+    auto sym = host::analyze_cholesky(graph, host::approximate_minimum_degree(graph));
+    const auto chol = host::factor_cholesky(bp, sym);
+    const int64_t n = net->n;
+    std::vector<int64_t> perm(chol.perm.begin(), chol.perm.end());
+    int32_t st = yb_factor_from_cholesky(gpu, n, chol.l.ptr.data(), chol.l.idx.data(), chol.l.val.data(), perm.data(),
+                                         &net->factor);
+    if (st != YB_OK) throw host::Error(st, "uploading the factor failed");
+    st = yb_factor_attach_matrix(net->factor, bp.ptr.data(), bp.idx.data(), bp.val.data());
+    if (st != YB_OK) throw host::Error(st, "attaching B' failed");
+    // Bf over the unknowns: per branch (f, b), (t, -b), the slack's column dropped
+    std::vector<int64_t> ptr(1, 0), idx;
+    std::vector<double> val;
+    for (int64_t k = 0; k < n_branch; ++k) {
+      if (net->unknown[from[k]] >= 0) idx.push_back(net->unknown[from[k]]), val.push_back(net->b[k]);
+      if (net->unknown[to[k]] >= 0) idx.push_back(net->unknown[to[k]]), val.push_back(-net->b[k]);
+      ptr.push_back((int64_t)idx.size());
+    }
+    st = yb_operator_new(net->factor, n_branch, ptr.data(), idx.data(), val.data(), &net->flows);
+    if (st != YB_OK) throw host::Error(st, "uploading Bf failed");
+    net->bridge = find_bridges(n_bus, net->from, net->to);
+    // the screening's per-branch and per-bus device data
+    const yb_factor *f = net->factor;
+    std::vector<int32_t> sf(n_branch), stt(n_branch), uf(n_branch), ut(n_branch), bus_slot(n_bus);
+    for (int64_t k = 0; k < n_branch; ++k) {
+      uf[k] = (int32_t)net->unknown[from[k]];
+      ut[k] = (int32_t)net->unknown[to[k]];
+      sf[k] = uf[k] < 0 ? (int32_t)n : f->plan.out_slot[uf[k]];
+      stt[k] = ut[k] < 0 ? (int32_t)n : f->plan.out_slot[ut[k]];
+    }
+    for (int64_t i = 0; i < n_bus; ++i)
+      bus_slot[i] = net->unknown[i] < 0 ? (int32_t)(n + 1) : f->plan.in_slot[net->unknown[i]];
+    cudaStream_t s = gpu->stream;
+    cuda_check(cudaSetDevice(gpu->device), "cudaSetDevice");
+    net->br_slot_f.upload(sf, s), net->br_slot_t.upload(stt, s);
+    net->br_u_f.upload(uf, s), net->br_u_t.upload(ut, s);
+    net->bus_slot.upload(bus_slot, s);
+    net->br_b.upload(net->b, s);
+    cuda_check(cudaStreamSynchronize(s), "network upload");
+    *out = net.release();
+    return YB_OK;
+  });
+}
+
+extern "C" void yb_dc_network_free(yb_dc_network *net) {
+  if (!net) return;
+  cudaSetDevice(net->gpu->device);
+  delete net;
+}
+
+extern "C" yb_factor *yb_dc_network_factor(yb_dc_network *net) { return net ? net->factor : nullptr; }
+
+extern "C" int32_t yb_dc_bridges(const yb_dc_network *net, uint8_t *bridge) {
+  return guard([&] {
+    require(net && bridge, "null argument");
+    std::copy(net->bridge.begin(), net->bridge.end(), bridge);
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_dc_ptdf_columns(yb_dc_network *net, int64_t count, const int64_t *buses, double *out) {
+  return guard([&] {
+    check(net);
+    require(count >= 0 && (count == 0 || (buses && out)), "null argument");
+    std::vector<int64_t> plus(count), minus(count, -1);
+    for (int64_t k = 0; k < count; ++k) {
+      require(buses[k] >= 0 && buses[k] < net->n_bus, "a bus is out of range");
+      plus[k] = net->unknown[buses[k]];  // the slack's column is zero
+    }
+    const auto flows = pair_flows(net, plus, minus);
+    std::copy(flows.begin(), flows.end(), out);
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_dc_ptdf_transfers(yb_dc_network *net, int64_t count, const int64_t *from_bus,
+                                        const int64_t *to_bus, double *out) {
+  return guard([&] {
+    check(net);
+    require(count >= 0 && (count == 0 || (from_bus && to_bus && out)), "null argument");
+    std::vector<int64_t> plus(count), minus(count);
+    for (int64_t k = 0; k < count; ++k) {
+      require(from_bus[k] >= 0 && from_bus[k] < net->n_bus && to_bus[k] >= 0 && to_bus[k] < net->n_bus,
+              "a bus is out of range");
+      plus[k] = net->unknown[from_bus[k]];
+      minus[k] = net->unknown[to_bus[k]];
+      if (plus[k] >= 0 && plus[k] == minus[k]) plus[k] = minus[k] = -1;  // a transfer to itself moves nothing
+    }
+    const auto flows = pair_flows(net, plus, minus);
+    std::copy(flows.begin(), flows.end(), out);
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_dc_lodf_columns(yb_dc_network *net, int64_t count, const int64_t *branches, double *out) {
+  return guard([&] {
+    check(net);
+    require(count >= 0 && (count == 0 || (branches && out)), "null argument");
+    std::vector<int64_t> plus, minus, which;
+    for (int64_t k = 0; k < count; ++k) {
+      const int64_t br = branches[k];
+      require(br >= 0 && br < net->n_branch, "a branch is out of range");
+      if (net->bridge[br]) continue;
+      int64_t p = net->unknown[net->from[br]], m = net->unknown[net->to[br]];
+      if (p >= 0 && p == m) p = m = -1;
+      plus.push_back(p), minus.push_back(m), which.push_back(k);
+    }
+    const auto flows = pair_flows(net, plus, minus);
+    const int64_t nl = net->n_branch;
+    for (int64_t k = 0; k < count; ++k) std::fill(out + k * nl, out + (k + 1) * nl, std::nan(""));
+    for (size_t j = 0; j < which.size(); ++j) {
+      const int64_t k = which[j], row = branches[k];
+      double *col = out + k * nl;
+      std::copy(flows.begin() + (int64_t)j * nl, flows.begin() + ((int64_t)j + 1) * nl, col);
+      // LODF = H / (1 - H_kk), -1 on the outaged branch (dc/sensitivity.rs:349-362)
+      const double remaining = 1.0 - col[row];
+      for (int64_t l = 0; l < nl; ++l) col[l] /= remaining;
+      col[row] = -1.0;
+    }
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_dc_outage_loadings_batch(yb_dc_network *net, int64_t cases, const int64_t *outaged,
+                                               const int64_t *scenario_ptr, const double *injections,
+                                               const double *weights, int32_t precision, int64_t *max_branch,
+                                               double *max_loading, int32_t *not_finite, int32_t *singular) {
+  return guard([&] {
+    check(net);
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(cases >= 0 && (cases == 0 || (outaged && scenario_ptr)), "null argument");
+    if (cases == 0) return YB_OK;
+    require(scenario_ptr[0] == 0, "scenario pointers must start at 0");
+    for (int64_t c = 0; c < cases; ++c) require(scenario_ptr[c + 1] >= scenario_ptr[c], "scenario pointers must not decrease");
+    const int64_t S = scenario_ptr[cases];
+    require(S == 0 || (injections && max_branch && max_loading && not_finite), "null output");
+    yb_factor *f = net->factor;
+    const int64_t n = net->n, nl = net->n_branch;
+    // per case: the outaged branch's pair over the unknowns, its slots, 1/b
+    std::vector<int32_t> case_of(S), pu(cases), mu(cases), ps(cases), ms(cases), br(cases);
+    std::vector<double> invb(cases);
+    for (int64_t c = 0; c < cases; ++c) {
+      const int64_t k = outaged[c];
+      require(k >= 0 && k < nl, "an outaged branch is out of range");
+      int64_t p = net->unknown[net->from[k]], m = net->unknown[net->to[k]];
+      if (p >= 0 && p == m) p = m = -1;
+      pu[c] = (int32_t)p, mu[c] = (int32_t)m, br[c] = (int32_t)k;
+      ps[c] = p < 0 ? (int32_t)n : f->plan.out_slot[p];
+      ms[c] = m < 0 ? (int32_t)n : f->plan.out_slot[m];
+      invb[c] = (p < 0 && m < 0) ? 1.0 : 1.0 / net->b[k];
+      for (int64_t j = scenario_ptr[c]; j < scenario_ptr[c + 1]; ++j) case_of[j] = (int32_t)c;
+    }
+    std::vector<double> w(nl, 1.0);
+    if (weights) w.assign(weights, weights + nl);
+    cuda_check(cudaSetDevice(net->gpu->device), "cudaSetDevice");
+    cudaStream_t s = net->gpu->stream;
+    net->d_case_of.upload(case_of, s), net->d_plus_u.upload(pu, s), net->d_minus_u.upload(mu, s);
+    net->d_plus_slot.upload(ps, s), net->d_minus_slot.upload(ms, s), net->d_branch.upload(br, s);
+    net->d_invb.upload(invb, s), net->d_weight.upload(w, s);
+    net->d_inj.reserve((size_t)(net->n_bus * S));
+    net->d_y.reserve((size_t)(n * cases));
+    net->d_cy.reserve((size_t)cases);
+    net->d_row.reserve((size_t)S), net->d_value.reserve((size_t)S), net->d_bad.reserve((size_t)S);
+    net->d_sing.reserve((size_t)cases);
+    cuda_check(cudaMemcpyAsync(net->d_inj.get(), injections, sizeof(double) * net->n_bus * S, cudaMemcpyHostToDevice, s),
+               "upload injections");
+    OutageIO io{};
+    io.inj = net->d_inj.get(), io.ldi = net->n_bus, io.n_bus = (int32_t)net->n_bus, io.bus_slot = net->bus_slot.get();
+    io.case_of = net->d_case_of.get(), io.c_plus = net->d_plus_slot.get(), io.c_minus = net->d_minus_slot.get();
+    io.c_invb = net->d_invb.get(), io.c_cy = net->d_cy.get(), io.c_branch = net->d_branch.get();
+    io.Y = net->d_y.get(), io.ldy = n, io.n_branch = (int32_t)nl;
+    io.br_slot_f = net->br_slot_f.get(), io.br_slot_t = net->br_slot_t.get();
+    io.br_u_f = net->br_u_f.get(), io.br_u_t = net->br_u_t.get(), io.br_b = net->br_b.get(), io.weight = net->d_weight.get();
+    io.out_row = net->d_row.get(), io.out_value = net->d_value.get(), io.out_bad = net->d_bad.get();
+    io.case_singular = net->d_sing.get();
+    // y = B'^-1 c of every case, then c'y; then the scenarios
+    auto run = [&]() {
+      solve_pairs_device(f, cases, net->d_plus_u.get(), net->d_minus_u.get(), nullptr, nullptr, nullptr, nullptr,
+                         net->d_y.get(), n, s);
+      case_cy_kernel<<<(unsigned)((cases + 255) / 256), 256, 0, s>>>(net->d_y.get(), n, net->d_plus_u.get(),
+                                                                     net->d_minus_u.get(), cases, net->d_cy.get());
+      cuda_check(cudaGetLastError(), "case_cy_kernel launch");
+      if (S == 0) return;
+      if (precision == YB_FP64) {
+        launch_outage_domain(f, S, io, s);
+      } else {
+        net->d_theta.reserve((size_t)(n * S));
+        net->d_ratio.reserve((size_t)S), net->d_steps.reserve((size_t)S);
+        // scenario right-hand sides over the unknowns, then FP32 substitution with FP64 refinement
+        const int32_t st = yb_solve_many_refined_device(f, net->d_inj.get() + (net->slack == 0 ? 1 : 0), net->n_bus,
+                                                        net->d_theta.get(), n, S, 3, 1e-10, net->d_ratio.get(),
+                                                        net->d_steps.get(), s);
+        if (st != YB_OK) throw host::Error(st, "the refined scenario solve failed");
+        outage_epilogue_kernel<<<(unsigned)S, 256, 0, s>>>(
+            net->d_theta.get(), n, net->d_case_of.get(), net->d_plus_u.get(), net->d_minus_u.get(), net->d_invb.get(),
+            net->d_cy.get(), net->d_branch.get(), net->d_y.get(), n, (int32_t)nl, net->br_u_f.get(), net->br_u_t.get(),
+            net->br_b.get(), net->d_weight.get(), net->d_row.get(), net->d_value.get(), net->d_bad.get(),
+            net->d_sing.get());
+        cuda_check(cudaGetLastError(), "outage_epilogue_kernel launch");
+      }
+    };
+    if (precision == YB_FP32) require(net->slack == 0, "the FP32 screening takes the slack at bus 0");
+    if (precision == YB_FP64 && net->graph && net->graph_cases == cases && net->graph_columns == S) {
+      // the same sizes as the captured graph: its buffers hold this batch's inputs
+      cuda_check(cudaGraphLaunch(net->graph, s), "cudaGraphLaunch");
+    } else {
+      run();  // makes every layout and buffer the launches need, outside any capture
+      if (precision == YB_FP64) {
+        if (net->graph) cudaGraphExecDestroy(net->graph), net->graph = nullptr;
+        cudaGraph_t g = nullptr;
+        cuda_check(cudaStreamSynchronize(s), "before capture");
+        cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+        try {
+          run();
+        } catch (...) {
+          cudaStreamEndCapture(s, &g);
+          if (g) cudaGraphDestroy(g);
+          throw;
+        }
+        cuda_check(cudaStreamEndCapture(s, &g), "cudaStreamEndCapture");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        cuda_check(e, "cudaGraphInstantiate");
+        net->graph = exec, net->graph_cases = cases, net->graph_columns = S;
+      }
+    }
+    std::vector<int32_t> bad(S), sing(cases);
+    cuda_check(cudaMemcpyAsync(max_branch, net->d_row.get(), sizeof(int64_t) * S, cudaMemcpyDeviceToHost, s), "download");
+    cuda_check(cudaMemcpyAsync(max_loading, net->d_value.get(), sizeof(double) * S, cudaMemcpyDeviceToHost, s), "download");
+    cuda_check(cudaMemcpyAsync(not_finite, net->d_bad.get(), sizeof(int32_t) * S, cudaMemcpyDeviceToHost, s), "download");
+    cuda_check(cudaMemcpyAsync(sing.data(), net->d_sing.get(), sizeof(int32_t) * cases, cudaMemcpyDeviceToHost, s),
+               "download");
+    cuda_check(cudaStreamSynchronize(s), "outage screening");
+    if (singular) std::copy(sing.begin(), sing.end(), singular);
+    return YB_OK;
+  });
+}

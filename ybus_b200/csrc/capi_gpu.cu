@@ -744,6 +744,14 @@ void solve_pairs_device(yb_factor *f, int64_t count, const int32_t *plus, const 
     launch_tiles<double, Load::Pairs, Store::Dense>(f, a, cfg, stream, f->scratch64);
 }
 
+// The batched N-1 screening's scenario launch (capi_dc.cu): the domain solve with the outage epilogue.
+void launch_outage_domain(yb_factor *f, int64_t count, const OutageIO &io, cudaStream_t stream) {
+  const TileConfig cfg = resolve<double>(f, f->tile64);
+  if (cfg.kind != kTileDomain)
+    throw host::Error(host::kInvalidArgument, "the batched screening needs the domain solve, which this factor does not admit");
+  launch_domain<double>(f, cfg, count, io, stream);
+}
+
 }  // namespace yb
 
 extern "C" int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,

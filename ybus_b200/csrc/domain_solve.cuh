@@ -46,7 +46,7 @@ struct DomainArgs {
 
 // Shared memory an IO policy may declare statically (its reductions), kept free beside the
 // dynamic shared memory.
-constexpr size_t kIoStaticSmem = 1024;
+constexpr size_t kIoStaticSmem = 2048;
 
 // The shared-memory footprint of a domain solve block.
 __host__ __device__ inline size_t domain_smem_bytes(int32_t n, int32_t W, int32_t value_bytes, int32_t tail,
@@ -220,6 +220,109 @@ template <bool UPDATE> struct PairIO {
           o[r] = sing ? xr : __dadd_rn(xr, __dmul_rn(z, y));
         }
       }
+    }
+  }
+};
+
+// Keeps the larger (value, row): the larger value, the smaller row on a tie, row -1 never winning
+// (the rule of ybus_cuda/src/kernels.cu:78-128)
+__device__ __forceinline__ void better_max(double &v, int &r, double v2, int r2) {
+  if (r2 >= 0 && (v2 > v || (v2 == v && (r < 0 || r2 < r)))) v = v2, r = r2;
+}
+
+// The N-1 screening of many scenarios (ybus_powerflow/src/dc/gpu.rs:334-430, with one right-hand
+// side per scenario instead of one base): a column is a scenario's injections p over the buses
+// (the slack's ignored), solved to theta = B'^-1 p; the epilogue applies its case's rank-one
+// outage update theta' = theta + z y (y = B'^-1 c for c = e_from - e_to of the outaged branch,
+// z = c'theta / (1/b - c'y); singular when 1/b - c'y is 0, which leaves theta), computes every
+// branch's flow b (theta'_from - theta'_to) (the outaged branch carries nothing) and reduces it to
+// the column's largest |flow| * weight with its branch (the smaller on a tie) and whether any flow
+// is not finite. Only those maxima leave the GPU.
+struct OutageIO {
+  static constexpr bool kRefine = false;
+  const double *__restrict__ inj;  // n_bus x S, column-major
+  int64_t ldi;
+  int32_t n_bus;
+  const int32_t *__restrict__ bus_slot;  // [n_bus] slot of the bus's unknown; n + 1 for the slack
+  const int32_t *__restrict__ case_of;   // [S]
+  const int32_t *__restrict__ c_plus, *__restrict__ c_minus;  // per case: solution slots (n: none)
+  const double *__restrict__ c_invb, *__restrict__ c_cy;      // per case: 1/b and c'y
+  const int32_t *__restrict__ c_branch;                        // per case: the outaged branch
+  const double *__restrict__ Y;                                // n x C, natural unknown order
+  int64_t ldy;
+  int32_t n_branch;
+  const int32_t *__restrict__ br_slot_f, *__restrict__ br_slot_t;  // solution slots (n: slack)
+  const int32_t *__restrict__ br_u_f, *__restrict__ br_u_t;        // unknowns (-1: slack)
+  const double *__restrict__ br_b, *__restrict__ weight;
+  int64_t *__restrict__ out_row;
+  double *__restrict__ out_value;
+  int32_t *__restrict__ out_bad;
+  int32_t *__restrict__ case_singular;
+
+  template <class T, int W>
+  __device__ __forceinline__ void load(int64_t col0, int64_t count, int n, T *Ys) const {
+    for (int r = threadIdx.x; r < n_bus; r += blockDim.x) {
+      T t[W];
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) t[cc] = col0 + cc < count ? (T)__ldcs(inj + (col0 + cc) * ldi + r) : T(0);
+      store_w<T, W>(Ys + (size_t)__ldg(bus_slot + r) * W, t);
+    }
+  }
+
+  template <int W> __device__ __forceinline__ void prefetch(int64_t, int64_t, int) const {}
+
+  template <class T, int W>
+  __device__ __forceinline__ void store(int64_t col0, int64_t count, int n, const T *Ys) const {
+    __shared__ double red_v[16];
+    __shared__ int red_r[16], red_b[16];
+#pragma unroll 1
+    for (int cc = 0; cc < W; ++cc) {
+      const int64_t col = col0 + cc;
+      if (col >= count) break;
+      const int c = __ldg(case_of + col);
+      const double *y = Y + (int64_t)c * ldy;
+      const double cx = __dsub_rn(__dadd_rn(0.0, (double)Ys[(size_t)__ldg(c_plus + c) * W + cc]),
+                                  (double)Ys[(size_t)__ldg(c_minus + c) * W + cc]);
+      const double w = __dadd_rn(-__ldg(c_cy + c), __ldg(c_invb + c));
+      const bool sing = (w == 0.0);
+      const double z = sing ? 0.0 : __ddiv_rn(cx, w);
+      const int k = __ldg(c_branch + c);
+      double v = 0.0;
+      int row = -1, bad = 0;
+      for (int l = threadIdx.x; l < n_branch; l += blockDim.x) {
+        const int uf = __ldg(br_u_f + l), ut = __ldg(br_u_t + l);
+        const double tf = uf < 0 ? 0.0 : __dadd_rn((double)Ys[(size_t)__ldg(br_slot_f + l) * W + cc], __dmul_rn(z, __ldg(y + uf)));
+        const double tt = ut < 0 ? 0.0 : __dadd_rn((double)Ys[(size_t)__ldg(br_slot_t + l) * W + cc], __dmul_rn(z, __ldg(y + ut)));
+        const double b = __ldg(br_b + l);
+        const double f = l == k ? 0.0 : __dadd_rn(__dmul_rn(b, tf), __dmul_rn(-b, tt));
+        if (!isfinite(f)) {
+          bad = 1;
+          continue;
+        }
+        const double load = fabs(f) * __ldg(weight + l);
+        if (load > v) v = load, row = l;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, off);
+        const int r2 = __shfl_xor_sync(0xffffffffu, row, off);
+        bad |= __shfl_xor_sync(0xffffffffu, bad, off);
+        better_max(v, row, v2, r2);
+      }
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      if (lane == 0) red_v[warp] = v, red_r[warp] = row, red_b[warp] = bad;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int w2 = 1; w2 < (int)(blockDim.x >> 5); ++w2) {
+          better_max(v, row, red_v[w2], red_r[w2]);
+          bad |= red_b[w2];
+        }
+        out_row[col] = row;
+        out_value[col] = row >= 0 ? v : 0.0;
+        out_bad[col] = bad;
+        case_singular[c] = sing ? 1 : 0;
+      }
+      __syncthreads();
     }
   }
 };

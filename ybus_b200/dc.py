@@ -1,0 +1,90 @@
+"""The DC callers of the solve path (ybus_powerflow/src/dc/gpu.rs `DcGpuStudy`,
+`DcGpuSensitivity`), over libybgpu's C ABI: a network from its branch list, PTDF and LODF columns,
+bridges, and the batched N-1 screening of injection scenarios."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import lib, ptr
+from .gpu import FP64, Gpu, _check
+
+
+class DcNetwork:
+    """B′ and Bf of a network (bus indices `frm`, `to`, reactances `x`, a slack bus), B′ factored
+    on the host and uploaded, Bf kept on the device as an operator on the solutions."""
+
+    def __init__(self, gpu: Gpu, n_bus: int, frm, to, x, slack: int = 0):
+        self.gpu = gpu
+        self.n_bus = int(n_bus)
+        self.frm = np.ascontiguousarray(frm, np.int64)
+        self.to = np.ascontiguousarray(to, np.int64)
+        self.x = np.ascontiguousarray(x, np.float64)
+        self.slack = int(slack)
+        out = C.c_void_p()
+        _check(lib().yb_dc_network_new(gpu._h, self.n_bus, self.frm.size, ptr(self.frm), ptr(self.to), ptr(self.x),
+                                       self.slack, C.byref(out)))
+        self._h = out
+
+    @classmethod
+    def from_grid(cls, gpu: Gpu, grid, slack: int = 0) -> "DcNetwork":
+        return cls(gpu, grid.n_bus, grid.frm, grid.to, grid.x, slack)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().yb_dc_network_free(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def n_branch(self) -> int:
+        return int(self.frm.size)
+
+    def bridges(self) -> np.ndarray:
+        out = np.zeros(self.n_branch, np.uint8)
+        _check(lib().yb_dc_bridges(self._h, ptr(out)))
+        return out.astype(bool)
+
+    def ptdf_columns(self, buses) -> np.ndarray:
+        """(count, n_branch): each bus's PTDF column (injection there, withdrawal at the slack)."""
+        buses = np.ascontiguousarray(buses, np.int64)
+        out = np.zeros((buses.size, self.n_branch))
+        _check(lib().yb_dc_ptdf_columns(self._h, buses.size, ptr(buses), ptr(out)))
+        return out
+
+    def ptdf_transfers(self, from_bus, to_bus) -> np.ndarray:
+        f = np.ascontiguousarray(from_bus, np.int64)
+        t = np.ascontiguousarray(to_bus, np.int64)
+        out = np.zeros((f.size, self.n_branch))
+        _check(lib().yb_dc_ptdf_transfers(self._h, f.size, ptr(f), ptr(t), ptr(out)))
+        return out
+
+    def lodf_columns(self, branches) -> np.ndarray:
+        """(count, n_branch): each outaged branch's LODF column (NaN for a bridge)."""
+        br = np.ascontiguousarray(branches, np.int64)
+        out = np.zeros((br.size, self.n_branch))
+        _check(lib().yb_dc_lodf_columns(self._h, br.size, ptr(br), ptr(out)))
+        return out
+
+    def outage_loadings_batch(self, outaged, scenario_ptr, injections, weights=None, precision: int = FP64):
+        """N-1 screening: case c takes out branch outaged[c] under the scenarios
+        injections[scenario_ptr[c]:scenario_ptr[c+1]] (each a vector over the buses). Returns
+        (branch, loading, not_finite) per scenario and singular per case."""
+        outaged = np.ascontiguousarray(outaged, np.int64)
+        sp = np.ascontiguousarray(scenario_ptr, np.int64)
+        inj = np.ascontiguousarray(injections, np.float64)
+        total = int(sp[-1]) if sp.size else 0
+        if inj.shape != (total, self.n_bus):
+            raise ValueError("one injection vector over the buses per scenario")
+        w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+        row = np.zeros(max(total, 1), np.int64)
+        val = np.zeros(max(total, 1))
+        bad = np.zeros(max(total, 1), np.int32)
+        sing = np.zeros(max(outaged.size, 1), np.int32)
+        _check(lib().yb_dc_outage_loadings_batch(self._h, outaged.size, ptr(outaged), ptr(sp), ptr(inj), ptr(w),
+                                                 precision, ptr(row), ptr(val), ptr(bad), ptr(sing)))
+        return row[:total], val[:total], bad[:total].astype(bool), sing[: outaged.size].astype(bool)
