@@ -284,6 +284,19 @@ int32_t yb_dc_outage_loadings_batch(yb_dc_network *net, int64_t cases, const int
                                     int32_t precision, int64_t *max_branch, double *max_loading, int32_t *not_finite,
                                     int32_t *singular);
 
+/* No ybus counterpart: the adjoint of a flow loss over a DC network, a forward/backward pair (the
+ * analogue of an autograd function) for `count` injection scenarios (n_bus x count, column-major,
+ * the slack's entries ignored). Forward: theta = B'^-1 p, flows f = diag(b) A theta (n_branch x
+ * count, optional), loss = sum softplus(|f| - margin * limit)^2; theta and dL/df stay on the device.
+ * Backward: lambda = B'^-T (Bf' dL/df) with the same factor; dL/dp = lambda (0 at the slack; n_bus x
+ * count) and dL/db (n_branch), b = 1/x each branch's susceptance. Either output may be NULL. */
+typedef struct yb_dc_adjoint yb_dc_adjoint;
+int32_t yb_dc_adjoint_new(yb_dc_network *net, int64_t count, yb_dc_adjoint **out);
+int32_t yb_dc_adjoint_forward(yb_dc_adjoint *adj, const double *injections, const double *limits, double margin,
+                              double *loss, double *flows);
+int32_t yb_dc_adjoint_backward(yb_dc_adjoint *adj, double *grad_injections, double *grad_susceptance);
+void yb_dc_adjoint_free(yb_dc_adjoint *adj);
+
 /* Attaches A, the matrix the factor factors (CSR, n x n, natural order, FP64), for refinement:
  * ybus_sparse's `solve_refined` takes it the same way (accuracy.rs:281-308). A copy with its
  * columns mapped to the factor's solution order is kept on the device. */

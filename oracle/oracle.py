@@ -268,3 +268,41 @@ def outage_flows_smw(solve, n_unknown, position, frm, to, b, outaged, theta_base
         for zj, y in zip(z, ys):
             x = x + zj * y
     return x
+
+
+def flow_loss_and_gradient(chol, n_bus, frm, to, susceptance, position, injections, limits, margin=0.8):
+    """The flow loss Σ softplus(|f| − margin·limit)², f = diag(b) A θ, θ = B′⁻¹ p, and its gradients
+    on the CPU from the oracle's solves: λ = B′⁻ᵀ (Bfᵀ dL/df) by the transposed solve (the same
+    solve for a Cholesky factor, `Cholesky::substitute`, cholesky.rs:570-579), dL/dp = λ (0 at the
+    slack), dL/db_k = Σ_scenarios dL/df_k d_k − (λ_f − λ_t) d_k with d_k = θ_f − θ_t.
+    Returns (loss, dL/dp (count, n_bus), dL/db (n_branch))."""
+    p = np.atleast_2d(np.asarray(injections, np.float64))
+    frm, to = np.asarray(frm), np.asarray(to)
+    b = np.asarray(susceptance, np.float64)
+    unknown = position >= 0
+    theta = solve_many(chol, p[:, unknown])
+
+    def over_buses(v):
+        out = np.zeros((v.shape[0], n_bus))
+        out[:, unknown] = v[:, position[unknown]]
+        return out
+
+    tb = over_buses(theta)
+    d = tb[:, frm] - tb[:, to]
+    f = b * tb[:, frm] + (-b) * tb[:, to]
+    u = np.abs(f) - margin * np.asarray(limits)
+    s = np.maximum(u, 0.0) + np.log1p(np.exp(-np.abs(u)))
+    loss = float((s * s).sum())
+    sig = np.where(u >= 0, 1.0 / (1.0 + np.exp(-np.where(u >= 0, u, 0.0))),
+                   np.exp(np.where(u < 0, u, 0.0)) / (1.0 + np.exp(np.where(u < 0, u, 0.0))))
+    g = 2.0 * s * sig * np.sign(f)
+    q_bus = np.zeros((p.shape[0], n_bus))
+    np.add.at(q_bus.T, frm, (b * g).T)
+    np.add.at(q_bus.T, to, (-b * g).T)
+    q = np.zeros((p.shape[0], int(unknown.sum())))
+    q[:, position[unknown]] = q_bus[:, unknown]
+    lam = solve_many(chol, q)
+    lb = over_buses(lam)
+    e = lb[:, frm] - lb[:, to]
+    grad_b = (g * d - e * d).sum(axis=0)
+    return loss, lb, grad_b

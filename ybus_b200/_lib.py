@@ -105,6 +105,10 @@ SIGNATURES: dict[str, tuple] = {
     "yb_dc_ptdf_transfers": (i32, [vp, i64, vp, vp, vp]),
     "yb_dc_lodf_columns": (i32, [vp, i64, vp, vp]),
     "yb_dc_outage_loadings_batch": (i32, [vp, i64, vp, vp, vp, vp, i32, vp, vp, vp, vp]),
+    "yb_dc_adjoint_new": (i32, [vp, i64, C.POINTER(vp)]),
+    "yb_dc_adjoint_forward": (i32, [vp, vp, vp, dbl, vp, vp]),
+    "yb_dc_adjoint_backward": (i32, [vp, vp, vp]),
+    "yb_dc_adjoint_free": (None, [vp]),
     "yb_solve_many_refined_device": (i32, [vp, vp, i64, vp, i64, i64, i32, dbl, vp, vp, vp]),
 }
 

@@ -23,8 +23,8 @@ using namespace yb;
 using host::idx_t;
 
 namespace yb {
-// From capi_gpu.cu: the domain solve's launch for an IO policy, with the tile the factor resolves to.
-void launch_outage_domain(yb_factor *f, int64_t count, const OutageIO &io, cudaStream_t stream);
+// From capi_gpu.cu: the FP64 domain solve's launch for an IO policy.
+template <class IO> void launch_domain_fp64(yb_factor *f, int64_t count, const IO &io, cudaStream_t stream);
 }  // namespace yb
 
 struct yb_dc_network {
@@ -415,7 +415,7 @@ extern "C" int32_t yb_dc_outage_loadings_batch(yb_dc_network *net, int64_t cases
       cuda_check(cudaGetLastError(), "case_cy_kernel launch");
       if (S == 0) return;
       if (precision == YB_FP64) {
-        launch_outage_domain(f, S, io, s);
+        launch_domain_fp64(f, S, io, s);
       } else {
         net->d_theta.reserve((size_t)(n * S));
         net->d_ratio.reserve((size_t)S), net->d_steps.reserve((size_t)S);
@@ -466,6 +466,215 @@ extern "C" int32_t yb_dc_outage_loadings_batch(yb_dc_network *net, int64_t cases
                "download");
     cuda_check(cudaStreamSynchronize(s), "outage screening");
     if (singular) std::copy(sing.begin(), sing.end(), singular);
+    return YB_OK;
+  });
+}
+
+// ---- the adjoint of a flow loss (no ybus counterpart) ---------------------------------------------
+
+// A forward/backward pair over a DC network, the analogue of an autograd function: forward solves
+// theta = B'^-1 p for `count` injection scenarios, computes the flows f = diag(b) A theta and the
+// loss sum softplus(|f| - margin * limit)^2, and keeps theta and dL/df on the device; backward
+// solves lambda = B'^-T (Bf' dL/df) with the same factor (B' is symmetric) and gives dL/dp =
+// lambda (zero at the slack) and dL/db_k = sum over scenarios of dL/df_k (theta_f - theta_t) -
+// (lambda_f - lambda_t)(theta_f - theta_t): the sensitivity of the flows' own b plus the chain of
+// the outer-product accumulation -lambda theta' onto B''s pattern through dB'/db_k = a_k a_k'.
+struct yb_dc_adjoint {
+  yb_dc_network *net = nullptr;
+  int64_t count = 0;
+  bool forward_done = false;
+  DeviceArray<double> p, limits, theta, g, lambda, flows, loss_part, gb_part, grad_b;
+  DeviceArray<int32_t> inc_ptr, inc_branch;
+  DeviceArray<double> inc_value;
+};
+
+namespace {
+
+constexpr int kLossThreads = 256;
+constexpr int kGradChunk = 32;  // scenarios per partial sum of dL/db
+
+// softplus(u) = log(1 + e^u), written to stay finite for large |u|
+__device__ __forceinline__ double softplus(double u) { return fmax(u, 0.0) + log1p(exp(-fabs(u))); }
+__device__ __forceinline__ double sigmoid(double u) {
+  return u >= 0.0 ? 1.0 / (1.0 + exp(-u)) : exp(u) / (1.0 + exp(u));
+}
+
+// One thread per (branch, scenario): the flow, its loss term and dL/df; the block's loss terms
+// summed in a fixed tree into loss_part[block]
+__global__ void flow_loss_kernel(const double *__restrict__ theta, int64_t n, int32_t nl,
+                                 const int32_t *__restrict__ uf, const int32_t *__restrict__ ut,
+                                 const double *__restrict__ b, const double *__restrict__ limits, double margin,
+                                 int64_t total, double *__restrict__ flows, double *__restrict__ g,
+                                 double *__restrict__ loss_part) {
+  __shared__ double part[kLossThreads];
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double term = 0.0;
+  if (idx < total) {
+    const int64_t r = idx / nl;
+    const int l = (int)(idx % nl);
+    const double *th = theta + r * n;
+    const double tf = uf[l] < 0 ? 0.0 : th[uf[l]], tt = ut[l] < 0 ? 0.0 : th[ut[l]];
+    const double f = __dadd_rn(__dmul_rn(b[l], tf), __dmul_rn(-b[l], tt));
+    const double u = fabs(f) - margin * limits[l];
+    const double s = softplus(u);
+    term = s * s;
+    const double sign = f > 0.0 ? 1.0 : (f < 0.0 ? -1.0 : 0.0);
+    g[idx] = 2.0 * s * sigmoid(u) * sign;
+    if (flows) flows[idx] = f;
+  }
+  part[threadIdx.x] = term;
+  __syncthreads();
+  for (int stride = blockDim.x / 2; stride > 0; stride /= 2) {
+    if (threadIdx.x < stride) part[threadIdx.x] += part[threadIdx.x + stride];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) loss_part[blockIdx.x] = part[0];
+}
+
+// Partial sums of dL/db over a chunk of scenarios: gb_part[chunk][l]
+__global__ void grad_b_kernel(const double *__restrict__ theta, const double *__restrict__ lambda, int64_t n,
+                              const double *__restrict__ g, int32_t nl, const int32_t *__restrict__ uf,
+                              const int32_t *__restrict__ ut, int64_t count, double *__restrict__ gb_part) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nl) return;
+  const int64_t r0 = (int64_t)blockIdx.y * kGradChunk, r1 = min(count, r0 + kGradChunk);
+  double acc = 0.0;
+  for (int64_t r = r0; r < r1; ++r) {
+    const double *th = theta + r * n, *la = lambda + r * n;
+    const double d = (uf[l] < 0 ? 0.0 : th[uf[l]]) - (ut[l] < 0 ? 0.0 : th[ut[l]]);
+    const double e = (uf[l] < 0 ? 0.0 : la[uf[l]]) - (ut[l] < 0 ? 0.0 : la[ut[l]]);
+    acc += g[r * nl + l] * d - e * d;
+  }
+  gb_part[(int64_t)blockIdx.y * nl + l] = acc;
+}
+
+// dL/db_l: the chunks' partial sums in chunk order
+__global__ void grad_b_reduce_kernel(const double *__restrict__ gb_part, int32_t nl, int64_t chunks,
+                                     double *__restrict__ grad_b) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nl) return;
+  double s = 0.0;
+  for (int64_t c = 0; c < chunks; ++c) s += gb_part[c * nl + l];
+  grad_b[l] = s;
+}
+
+}  // namespace
+
+extern "C" int32_t yb_dc_adjoint_new(yb_dc_network *net, int64_t count, yb_dc_adjoint **out) {
+  return guard([&] {
+    check(net);
+    require(out != nullptr && count >= 1, "bad argument");
+    const int64_t n = net->n, nl = net->n_branch;
+    require(count * nl < ((int64_t)1 << 40), "too many scenarios", host::kTooLarge);
+    auto adj = std::make_unique<yb_dc_adjoint>();
+    adj->net = net;
+    adj->count = count;
+    // Bf' over the unknowns: each unknown's incident branches in branch order, +b at the from end
+    std::vector<std::vector<std::pair<int32_t, double>>> inc(n);
+    for (int64_t l = 0; l < nl; ++l) {
+      if (net->unknown[net->from[l]] >= 0) inc[net->unknown[net->from[l]]].push_back({(int32_t)l, net->b[l]});
+      if (net->unknown[net->to[l]] >= 0) inc[net->unknown[net->to[l]]].push_back({(int32_t)l, -net->b[l]});
+    }
+    std::vector<int32_t> ptr(1, 0), br;
+    std::vector<double> val;
+    for (auto &v : inc) {
+      for (auto [l, x] : v) br.push_back(l), val.push_back(x);
+      ptr.push_back((int32_t)br.size());
+    }
+    cuda_check(cudaSetDevice(net->gpu->device), "cudaSetDevice");
+    cudaStream_t s = net->gpu->stream;
+    adj->inc_ptr.upload(ptr, s);
+    adj->inc_branch.upload(br.empty() ? std::vector<int32_t>{0} : br, s);
+    adj->inc_value.upload(val.empty() ? std::vector<double>{0.0} : val, s);
+    adj->p.resize((size_t)(net->n_bus * count));
+    adj->limits.resize((size_t)nl);
+    adj->theta.resize((size_t)(n * count));
+    adj->lambda.resize((size_t)(n * count));
+    adj->g.resize((size_t)(nl * count));
+    adj->loss_part.resize((size_t)((nl * count + kLossThreads - 1) / kLossThreads));
+    adj->gb_part.resize((size_t)(((count + kGradChunk - 1) / kGradChunk) * nl));
+    adj->grad_b.resize((size_t)nl);
+    cuda_check(cudaStreamSynchronize(s), "adjoint set-up");
+    *out = adj.release();
+    return YB_OK;
+  });
+}
+
+extern "C" void yb_dc_adjoint_free(yb_dc_adjoint *adj) {
+  if (!adj) return;
+  cudaSetDevice(adj->net->gpu->device);
+  delete adj;
+}
+
+extern "C" int32_t yb_dc_adjoint_forward(yb_dc_adjoint *adj, const double *injections, const double *limits,
+                                         double margin, double *loss, double *flows) {
+  return guard([&] {
+    require(adj && injections && limits && loss, "null argument");
+    yb_dc_network *net = adj->net;
+    const int64_t n = net->n, nl = net->n_branch, count = adj->count;
+    cuda_check(cudaSetDevice(net->gpu->device), "cudaSetDevice");
+    cudaStream_t s = net->gpu->stream;
+    cuda_check(cudaMemcpyAsync(adj->p.get(), injections, sizeof(double) * net->n_bus * count, cudaMemcpyHostToDevice, s),
+               "upload injections");
+    cuda_check(cudaMemcpyAsync(adj->limits.get(), limits, sizeof(double) * nl, cudaMemcpyHostToDevice, s), "upload limits");
+    BusIO io{adj->p.get(), net->n_bus, (int32_t)net->n_bus, net->bus_slot.get(), adj->theta.get(), n,
+             net->factor->out_slot.get()};
+    launch_domain_fp64(net->factor, count, io, s);
+    if (flows) adj->flows.reserve((size_t)(nl * count));
+    const int64_t total = nl * count, blocks = (total + kLossThreads - 1) / kLossThreads;
+    flow_loss_kernel<<<(unsigned)blocks, kLossThreads, 0, s>>>(adj->theta.get(), n, (int32_t)nl, net->br_u_f.get(),
+                                                               net->br_u_t.get(), net->br_b.get(), adj->limits.get(),
+                                                               margin, total, flows ? adj->flows.get() : nullptr,
+                                                               adj->g.get(), adj->loss_part.get());
+    cuda_check(cudaGetLastError(), "flow_loss_kernel launch");
+    std::vector<double> part(blocks);
+    cuda_check(cudaMemcpyAsync(part.data(), adj->loss_part.get(), sizeof(double) * blocks, cudaMemcpyDeviceToHost, s),
+               "download loss");
+    if (flows)
+      cuda_check(cudaMemcpyAsync(flows, adj->flows.get(), sizeof(double) * total, cudaMemcpyDeviceToHost, s),
+                 "download flows");
+    cuda_check(cudaStreamSynchronize(s), "adjoint forward");
+    double sum = 0.0;
+    for (double v : part) sum += v;
+    *loss = sum;
+    adj->forward_done = true;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_dc_adjoint_backward(yb_dc_adjoint *adj, double *grad_injections, double *grad_susceptance) {
+  return guard([&] {
+    require(adj != nullptr, "null adjoint");
+    require(adj->forward_done, "backward needs a forward first");
+    yb_dc_network *net = adj->net;
+    const int64_t n = net->n, nl = net->n_branch, count = adj->count;
+    cuda_check(cudaSetDevice(net->gpu->device), "cudaSetDevice");
+    cudaStream_t s = net->gpu->stream;
+    AdjointIO io{adj->g.get(), nl, adj->inc_ptr.get(), adj->inc_branch.get(), adj->inc_value.get(),
+                 net->factor->in_slot.get(), adj->lambda.get(), n, net->factor->out_slot.get()};
+    launch_domain_fp64(net->factor, count, io, s);
+    const int64_t chunks = (count + kGradChunk - 1) / kGradChunk;
+    const dim3 grid((unsigned)((nl + 255) / 256), (unsigned)chunks);
+    grad_b_kernel<<<grid, 256, 0, s>>>(adj->theta.get(), adj->lambda.get(), n, adj->g.get(), (int32_t)nl,
+                                       net->br_u_f.get(), net->br_u_t.get(), count, adj->gb_part.get());
+    cuda_check(cudaGetLastError(), "grad_b_kernel launch");
+    grad_b_reduce_kernel<<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(adj->gb_part.get(), (int32_t)nl, chunks,
+                                                                      adj->grad_b.get());
+    cuda_check(cudaGetLastError(), "grad_b_reduce_kernel launch");
+    std::vector<double> lam;
+    if (grad_injections) {
+      lam.resize((size_t)(n * count));
+      cuda_check(cudaMemcpyAsync(lam.data(), adj->lambda.get(), sizeof(double) * n * count, cudaMemcpyDeviceToHost, s),
+                 "download lambda");
+    }
+    if (grad_susceptance)
+      cuda_check(cudaMemcpyAsync(grad_susceptance, adj->grad_b.get(), sizeof(double) * nl, cudaMemcpyDeviceToHost, s),
+                 "download dL/db");
+    cuda_check(cudaStreamSynchronize(s), "adjoint backward");
+    if (grad_injections)
+      for (int64_t r = 0; r < count; ++r)
+        for (int64_t i = 0; i < net->n_bus; ++i)
+          grad_injections[r * net->n_bus + i] = net->unknown[i] < 0 ? 0.0 : lam[r * n + net->unknown[i]];
     return YB_OK;
   });
 }

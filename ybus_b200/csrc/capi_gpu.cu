@@ -744,13 +744,17 @@ void solve_pairs_device(yb_factor *f, int64_t count, const int32_t *plus, const 
     launch_tiles<double, Load::Pairs, Store::Dense>(f, a, cfg, stream, f->scratch64);
 }
 
-// The batched N-1 screening's scenario launch (capi_dc.cu): the domain solve with the outage epilogue.
-void launch_outage_domain(yb_factor *f, int64_t count, const OutageIO &io, cudaStream_t stream) {
+// The domain solve in FP64 with an IO policy of the callers' (capi_dc.cu): the batched screening,
+// the adjoint's solves.
+template <class IO> void launch_domain_fp64(yb_factor *f, int64_t count, const IO &io, cudaStream_t stream) {
   const TileConfig cfg = resolve<double>(f, f->tile64);
   if (cfg.kind != kTileDomain)
-    throw host::Error(host::kInvalidArgument, "the batched screening needs the domain solve, which this factor does not admit");
+    throw host::Error(host::kInvalidArgument, "this solve needs the domain solve, which the factor does not admit");
   launch_domain<double>(f, cfg, count, io, stream);
 }
+template void launch_domain_fp64<OutageIO>(yb_factor *, int64_t, const OutageIO &, cudaStream_t);
+template void launch_domain_fp64<BusIO>(yb_factor *, int64_t, const BusIO &, cudaStream_t);
+template void launch_domain_fp64<AdjointIO>(yb_factor *, int64_t, const AdjointIO &, cudaStream_t);
 
 }  // namespace yb
 

@@ -327,6 +327,72 @@ struct OutageIO {
   }
 };
 
+// Right-hand sides given over the buses (column-major, n_bus rows; bus_slot maps each bus to its
+// unknown's slot, the slack to the spare slot n + 1, so its entry is ignored), solutions stored over
+// the unknowns in natural order.
+struct BusIO {
+  static constexpr bool kRefine = false;
+  const double *__restrict__ b;
+  int64_t ldb;
+  int32_t n_bus;
+  const int32_t *__restrict__ bus_slot;
+  double *__restrict__ x;
+  int64_t ldx;
+  const int32_t *__restrict__ out_slot;
+
+  template <class T, int W>
+  __device__ __forceinline__ void load(int64_t col0, int64_t count, int n, T *Ys) const {
+    DenseIO::load_columns<T, W>(b, ldb, bus_slot, col0, count, n_bus, Ys);
+  }
+  template <int W> __device__ __forceinline__ void prefetch(int64_t col0, int64_t count, int n) const {}
+  template <class T, int W>
+  __device__ __forceinline__ void store(int64_t col0, int64_t count, int n, const T *Ys) const {
+    DenseIO::store_columns<T, W>(x, ldx, out_slot, col0, count, n, Ys);
+  }
+};
+
+// The adjoint solve's right-hand sides built in the load: q = Bf' g for each column of g (branch
+// by scenario), Bf' given as each unknown's incident branches with their signed susceptances
+// (inc_ptr over unknowns), summed in that order; solutions stored over the unknowns.
+struct AdjointIO {
+  static constexpr bool kRefine = false;
+  const double *__restrict__ g;  // n_branch x count
+  int64_t ldg;
+  const int32_t *__restrict__ inc_ptr;  // [n + 1]
+  const int32_t *__restrict__ inc_branch;
+  const double *__restrict__ inc_value;
+  const int32_t *__restrict__ in_slot;
+  double *__restrict__ x;
+  int64_t ldx;
+  const int32_t *__restrict__ out_slot;
+
+  template <class T, int W>
+  __device__ __forceinline__ void load(int64_t col0, int64_t count, int n, T *Ys) const {
+    for (int u = threadIdx.x; u < n; u += blockDim.x) {
+      double q[W];
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) q[cc] = 0.0;
+      const int p1 = __ldg(inc_ptr + u + 1);
+      for (int p = __ldg(inc_ptr + u); p < p1; ++p) {
+        const int l = __ldg(inc_branch + p);
+        const double v = __ldg(inc_value + p);
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc)
+          if (col0 + cc < count) q[cc] = __dadd_rn(q[cc], __dmul_rn(v, __ldg(g + (col0 + cc) * ldg + l)));
+      }
+      T t[W];
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) t[cc] = (T)q[cc];
+      store_w<T, W>(Ys + (size_t)__ldg(in_slot + u) * W, t);
+    }
+  }
+  template <int W> __device__ __forceinline__ void prefetch(int64_t, int64_t, int) const {}
+  template <class T, int W>
+  __device__ __forceinline__ void store(int64_t col0, int64_t count, int n, const T *Ys) const {
+    DenseIO::store_columns<T, W>(x, ldx, out_slot, col0, count, n, Ys);
+  }
+};
+
 // Iterative refinement (ybus_sparse's `refine_normwise`, accuracy.rs:83-122): the substitutions in
 // the precision of the tile (FP32); the residual and the update x += d in FP64 against the FP64
 // matrix A. Pass 0 loads b into the slots and into the block's FP64 residual scratch R (natural row

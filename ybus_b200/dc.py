@@ -88,3 +88,42 @@ class DcNetwork:
         _check(lib().yb_dc_outage_loadings_batch(self._h, outaged.size, ptr(outaged), ptr(sp), ptr(inj), ptr(w),
                                                  precision, ptr(row), ptr(val), ptr(bad), ptr(sing)))
         return row[:total], val[:total], bad[:total].astype(bool), sing[: outaged.size].astype(bool)
+
+
+class FlowLoss:
+    """The adjoint of Σ softplus(|f| − margin·limit)² over a DC network's flows f = diag(b) A θ,
+    θ = B′⁻¹ p: `forward(p, limits)` gives the loss (and optionally the flows) and keeps θ and
+    dL/df on the device; `backward()` gives dL/dp (per scenario and bus, 0 at the slack) and dL/db
+    (per branch, b = 1/x) from one transposed solve with the same factor."""
+
+    def __init__(self, net: DcNetwork, count: int):
+        self.net = net
+        self.count = int(count)
+        out = C.c_void_p()
+        _check(lib().yb_dc_adjoint_new(net._h, self.count, C.byref(out)))
+        self._h = out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().yb_dc_adjoint_free(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def forward(self, injections, limits, margin: float = 0.8, flows: bool = False):
+        p = np.ascontiguousarray(injections, np.float64)
+        if p.shape != (self.count, self.net.n_bus):
+            raise ValueError("one injection vector over the buses per scenario")
+        lim = np.ascontiguousarray(limits, np.float64)
+        loss = C.c_double()
+        f = np.zeros((self.count, self.net.n_branch)) if flows else None
+        _check(lib().yb_dc_adjoint_forward(self._h, ptr(p), ptr(lim), float(margin), C.byref(loss), ptr(f)))
+        return (loss.value, f) if flows else loss.value
+
+    def backward(self):
+        gp = np.zeros((self.count, self.net.n_bus))
+        gb = np.zeros(self.net.n_branch)
+        _check(lib().yb_dc_adjoint_backward(self._h, ptr(gp), ptr(gb)))
+        return gp, gb
