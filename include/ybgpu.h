@@ -297,6 +297,28 @@ int32_t yb_dc_adjoint_forward(yb_dc_adjoint *adj, const double *injections, cons
 int32_t yb_dc_adjoint_backward(yb_dc_adjoint *adj, double *grad_injections, double *grad_susceptance);
 void yb_dc_adjoint_free(yb_dc_adjoint *adj);
 
+/* ---- complex LU factors and the multi-network batch (no ybus counterpart on the GPU) --------- */
+/* A complex128 LU factor P A Q = L U as ybus_sparse's generic LU makes it for a Ybus (lu.rs:268-417):
+ * L unit lower in CSC (diagonal first), U upper in CSC (diagonal last), values interleaved
+ * (re, im), row_perm = P, col_perm = Q. Kept on the device in complex128 and complex64. */
+int32_t yb_factor_from_lu_complex(yb_gpu *gpu, int64_t n, const int64_t *l_ptr, const int64_t *l_idx,
+                                  const double *l_val, const int64_t *u_ptr, const int64_t *u_idx, const double *u_val,
+                                  const int64_t *row_perm, const int64_t *col_perm, yb_factor **out);
+/* Attaches the complex matrix A (CSR, n x n, natural order, interleaved values) to a complex factor,
+ * for refinement and residuals. */
+int32_t yb_factor_attach_matrix_complex(yb_factor *f, const int64_t *a_ptr, const int64_t *a_idx, const double *a_val);
+/* Solves many complex factors' right-hand sides in one launch (a persistent work list of (network,
+ * tile) items, largest networks first): network i solves counts[i] complex128 right-hand sides at
+ * d_rhs[i] (column-major n_i x counts[i], interleaved) into d_out[i]. YB_FP64: complex128
+ * substitution. YB_FP32: complex64 substitution, then complex128 residuals b - A x against the
+ * attached matrices and complex64 corrections while any column is above `tolerance` and the worst
+ * one at least halves, at most max_steps; `steps` (host, per network, may be NULL) receives the
+ * corrections taken. d_ratio (NULL, or per network a device array of counts[i] doubles, entries may
+ * be NULL) receives each column's final ||b - A x||inf / ||b||inf. All factors on one GPU. */
+int32_t yb_solve_batch_complex(int64_t networks, yb_factor *const *factors, const double *const *d_rhs,
+                               double *const *d_out, const int64_t *counts, int32_t precision, int32_t max_steps,
+                               double tolerance, double *const *d_ratio, int32_t *steps, void *stream);
+
 /* Attaches A, the matrix the factor factors (CSR, n x n, natural order, FP64), for refinement:
  * ybus_sparse's `solve_refined` takes it the same way (accuracy.rs:281-308). A copy with its
  * columns mapped to the factor's solution order is kept on the device. */

@@ -7,7 +7,7 @@ ybus_cuda's API (include/ybgpu.h). Python mirrors that API on top of the C ABI.
 from . import grids, host
 from ._lib import YbError
 from .gpu import (FP32, FP64, ColumnMax, CudaError, Gpu, GpuBlock, GpuFactor, GpuOperator, Pair, PairUpdate,
-                  ShapeMismatch, Timings)
+                  ShapeMismatch, Timings, solve_batch_complex)
 
 __all__ = ["grids", "host", "Gpu", "GpuFactor", "GpuBlock", "GpuOperator", "Pair", "PairUpdate", "ColumnMax", "Timings",
-           "CudaError", "ShapeMismatch", "YbError", "FP64", "FP32"]
+           "CudaError", "ShapeMismatch", "YbError", "FP64", "FP32", "solve_batch_complex"]

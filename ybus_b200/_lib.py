@@ -83,6 +83,9 @@ SIGNATURES: dict[str, tuple] = {
     "yb_solve_many_device": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
     "yb_solve_many_device_noalloc": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
     "yb_factor_attach_matrix": (i32, [vp, vp, vp, vp]),
+    "yb_factor_from_lu_complex": (i32, [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]),
+    "yb_factor_attach_matrix_complex": (i32, [vp, vp, vp, vp]),
+    "yb_solve_batch_complex": (i32, [i64, vp, vp, vp, vp, i32, i32, dbl, vp, vp, vp]),
     "yb_pair_solves": (i32, [vp, i64, vp, vp, C.POINTER(vp)]),
     "yb_pair_updates": (i32, [vp, vp, i64, vp, vp, vp, vp, C.POINTER(vp)]),
     "yb_block_columns": (i64, [vp]),

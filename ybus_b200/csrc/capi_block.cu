@@ -117,6 +117,7 @@ std::vector<int32_t> rows32(const int64_t *rows, int64_t count, int64_t limit, b
 yb_block *make_block(yb_factor *f, int64_t count, const int64_t *plus, const int64_t *minus, const double *base,
                      const double *alpha, const double *inverse_weight) {
   require(f != nullptr, "null factor");
+  require(!f->is_complex, "pair solves take a real factor");
   require(count >= 0, "negative count");
   require(count <= f->width, "at most block_width() pairs");
   require(count == 0 || (plus && minus), "null pair arrays");

@@ -762,6 +762,7 @@ extern "C" int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64
                                         int64_t count, int32_t precision, void *stream) {
   return guard([&] {
     require(f != nullptr, "null factor");
+    require(!f->is_complex, "a complex factor solves with yb_solve_batch_complex");
     require(count >= 0, "negative count");
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
     require(count == 0 || (d_rhs && d_out), "null device array");
@@ -785,6 +786,7 @@ extern "C" int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64
 extern "C" int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count, double *out) {
   return guard([&] {
     require(f != nullptr, "null factor");
+    require(!f->is_complex, "a complex factor solves with yb_solve_batch_complex");
     require(count >= 0, "negative count");
     const int64_t n = f->n;
     if (n == 0 || count == 0) return YB_OK;
@@ -987,6 +989,7 @@ extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rh
     require(tolerance >= 0.0, "the tolerance must not be negative");
     require(count == 0 || (d_rhs && d_out), "null device array");
     require(ldb >= f->n && ldx >= f->n, "a leading dimension is below the factor's order");
+    require(!f->is_complex, "a complex factor solves with yb_solve_batch_complex");
     require(f->a_rows == f->n, "no matrix attached: call yb_factor_attach_matrix first");
     cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
     if (count == 0 || f->n == 0) return YB_OK;

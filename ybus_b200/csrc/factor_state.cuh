@@ -9,6 +9,7 @@
 #include <tuple>
 
 #include "../../include/ybgpu.h"
+#include "cplx.cuh"
 #include "device.cuh"
 #include "plan.hpp"
 
@@ -27,6 +28,7 @@ struct yb_gpu {
   int64_t smem_optin = 0;       // largest dynamic shared memory a block may opt into
   int64_t smem_per_sm = 0;
   std::string name;
+  std::shared_ptr<void> zwork;  // the complex batch's device workspace (capi_complex.cu), kept between calls
 };
 
 namespace yb {
@@ -115,6 +117,15 @@ struct yb_factor {
   yb::DeviceArray<int32_t> a_ptr, a_idx;
   yb::DeviceArray<double> a_val;
   yb::DeviceArray<double> refine_scratch;  // per block n * W residuals
+  // a complex LU factor (yb_factor_from_lu_complex): its plan, its sweeps in complex128 and
+  // complex64, and the complex matrix attached for refinement (CSR, natural order)
+  bool is_complex = false;
+  yb::Plan<yb::host::c128> cplan;
+  yb::DeviceSweep<yb::cplx<double>> fwdz, bwdz;
+  yb::DeviceSweep<yb::cplx<float>> fwdc, bwdc;
+  int64_t za_rows = -1;
+  yb::DeviceArray<int32_t> za_ptr, za_idx;
+  yb::DeviceArray<yb::cplx<double>> za_val;
   yb::PinnedBuffer staging;
   int64_t width = 1;
   yb::Timings timings;

@@ -91,6 +91,7 @@ extern "C" int32_t yb_solve_many_device_noalloc(yb_factor *f, const double *d_rh
   using namespace yb;
   return guard([&] {
     require(f != nullptr, "null factor");
+    require(!f->is_complex, "a complex factor solves with yb_solve_batch_complex");
     require(count >= 0, "negative count");
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
     require(count == 0 || (d_rhs && d_out), "null device array");

@@ -144,6 +144,28 @@ class GpuFactor:
                                        ptr(f.u.idx), ptr(f.u.val), ptr(f.row_perm), ptr(f.col_perm), C.byref(out)))
         return cls(gpu, out.value)
 
+    @classmethod
+    def from_lu_complex(cls, gpu: Gpu, f: HostLu) -> "GpuFactor":
+        """A complex128 LU factor (P A Q = L U of a Ybus), kept in complex128 and complex64."""
+        if not f.is_complex:
+            raise CudaError(_lib.YB_ERROR_INVALID_ARGUMENT, "a real factor uploads with from_lu")
+        lv = np.ascontiguousarray(f.l.val, np.complex128)
+        uv = np.ascontiguousarray(f.u.val, np.complex128)
+        out = C.c_void_p()
+        _check(lib().yb_factor_from_lu_complex(gpu._h, f.n, ptr(f.l.ptr), ptr(f.l.idx), ptr(lv), ptr(f.u.ptr),
+                                               ptr(f.u.idx), ptr(uv), ptr(f.row_perm), ptr(f.col_perm),
+                                               C.byref(out)))
+        factor = cls(gpu, out.value)
+        factor._keep = (lv, uv)
+        return factor
+
+    def attach_matrix_complex(self, a) -> None:
+        """Attaches the complex A (a host.Matrix) for refinement and residuals."""
+        p, i, v = a.to_csr().arrays()
+        v = np.ascontiguousarray(v, np.complex128)
+        self._cmatrix = (p, i, v)
+        _check(lib().yb_factor_attach_matrix_complex(self._h, ptr(p), ptr(i), ptr(v)))
+
     def dim(self) -> int:
         return lib().yb_factor_dim(self._h)
 
@@ -414,3 +436,20 @@ class GpuBlock:
         return _maxima(rows[:k], values[:k], bad[:k])
 
 
+
+
+def solve_batch_complex(factors, d_rhs, d_out, counts, precision: int = FP64, max_steps: int = 3,
+                        tolerance: float = 1e-10, d_ratio=None, stream: int | None = None) -> list[int]:
+    """Solves many complex factors' right-hand sides in one launch (device pointers per network,
+    complex128 column-major n x count). FP64: complex128 substitution; FP32: complex64 substitution
+    with complex128 refinement. Returns the corrections taken per network."""
+    k = len(factors)
+    hs = (C.c_void_p * k)(*[f._h.value for f in factors])
+    rhs = (C.c_void_p * k)(*d_rhs)
+    out = (C.c_void_p * k)(*d_out)
+    cnt = np.ascontiguousarray(counts, np.int64)
+    ratio = (C.c_void_p * k)(*d_ratio) if d_ratio is not None else None
+    steps = np.zeros(k, np.int32)
+    _check(lib().yb_solve_batch_complex(k, hs, rhs, out, ptr(cnt), precision, max_steps, float(tolerance), ratio,
+                                        ptr(steps), stream))
+    return steps.tolist()
