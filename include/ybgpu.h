@@ -119,6 +119,13 @@ int32_t yb_factor_from_lu(yb_gpu *gpu, int64_t n, const int64_t *l_ptr, const in
                           const double *l_val, const int64_t *u_ptr, const int64_t *u_idx,
                           const double *u_val, const int64_t *row_perm, const int64_t *col_perm,
                           yb_factor **out);
+/* `Lu::solve_transpose` (lu.rs:506-533) as a factor: the same arguments as yb_factor_from_lu, uploading
+ * the factor of A' = Q U' L' P, so every solve of the result solves A' x = b (U' forward, then L'
+ * backward). A Cholesky factor needs none: A' = A. */
+int32_t yb_factor_from_lu_transposed(yb_gpu *gpu, int64_t n, const int64_t *l_ptr, const int64_t *l_idx,
+                                     const double *l_val, const int64_t *u_ptr, const int64_t *u_idx,
+                                     const double *u_val, const int64_t *row_perm, const int64_t *col_perm,
+                                     yb_factor **out);
 void yb_factor_free(yb_factor *f);
 /* `GpuFactor::dim` and `block_width` (factor.rs:181-190); -1 for a null factor. */
 int64_t yb_factor_dim(const yb_factor *f);
@@ -166,6 +173,12 @@ int32_t yb_factor_set_domain(yb_factor *f, int32_t precision, int32_t warps, int
  * cost model's cycles per tile; YB_ERROR_INVALID_ARGUMENT if that choice is not the domain solve. */
 int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *cut, int32_t *top_rows,
                               int64_t *records, int64_t *bytes, int64_t *smem_bytes, double *model_cycles);
+/* No ybus counterpart: the autotuner. Times the domain solve of `count` right-hand sides for a
+ * precision over its shapes (warps 8/12/16, pages 1536/2048 bytes, 2 or 3 pages in flight, the
+ * widest tile that fits and half of it) and keeps the fastest for the factor; config receives
+ * {kind, tile width, warps, ring, page bytes} and best_ms its time (either may be NULL). With no
+ * domain solve to tune, the configuration is left as it was. */
+int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t count, int32_t *config, double *best_ms);
 /* No ybus counterpart, diagnostics on the host (no GPU needed): the domain layout a Cholesky factor
  * given as to yb_factor_from_cholesky gets for `value_bytes` (8 or 4). info receives {cut, top
  * rows, stages, warps, pages, records, entries, page bytes}, top_condition the worse infinity-norm

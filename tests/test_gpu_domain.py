@@ -91,3 +91,27 @@ def test_domain_solve_on_the_10k_grid(gpu):
         sample = np.arange(0, 1000, 37)
         d = worst_relative_difference(xs[sample], orc.solve_many(chol, rhs[sample], threads=8))
         assert d < bar, f"precision {prec}: {d:e}"
+
+
+def test_autotune_keeps_the_fastest_domain_shape_and_the_same_solutions(gpu):
+    chol = host.cholesky(random_spd(800, 2, 19))
+    rhs = right_hand_sides(800, 130, 23)
+    cpu = orc.solve_many(chol, rhs)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    for prec, bar in ((FP64, BAR), (FP32, 1e-4)):
+        best = factor.autotune(prec, 256)
+        assert best["kind"] == DOMAIN and best["warps"] in (8, 12, 16) and best["ring"] in (2, 3)
+        assert best["page_bytes"] in (1536, 2048) and best["tile"] >= 1 and 0 < best["ms"] < 1e3
+        assert factor.domain_info(prec)["tile"] == best["tile"]
+        if prec == FP64:
+            d = worst_relative_difference(factor.solve_many(rhs), cpu)
+            assert d < bar, f"{d:e}"
+    factor.check_error()
+
+
+def test_autotune_on_a_single_row_still_solves(gpu):
+    chol = host.cholesky(random_spd(1, 100, 1))
+    rhs = right_hand_sides(1, 40, 2)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.autotune(FP64, 16)
+    assert worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs)) < BAR

@@ -115,6 +115,31 @@ def test_lu_solves_match_the_cpu_with_pivoting(gpu):
     assert d < BAR, f"{d:e}"
 
 
+@pytest.mark.parametrize("kind", [0, SHARED, GLOBAL, STREAM])
+def test_transposed_lu_solves_match_the_cpu(gpu, kind):
+    # Lu::solve_transpose (lu.rs:506-533) as the factor of A': forward with U', back with L'
+    a = random_square(250, 4, 3)
+    lu = host.lu(a)
+    rhs = right_hand_sides(250, 45, 5)
+    cpu = orc.solve_many_lu(lu, rhs, transpose=True)
+    factor = GpuFactor.from_lu_transposed(gpu, lu)
+    factor.set_tile_kind(FP64, kind)
+    x = factor.solve_many(rhs)
+    d = worst_relative_difference(x, cpu)
+    assert d < BAR, f"kind {kind}: {d:e}"
+    dense = a.to_dense()
+    assert np.abs(x @ dense - rhs).max() < 1e-9 * np.abs(rhs).max() * np.abs(dense).max() * 250
+    # the untransposed factor of the same LU solves A x = b
+    assert worst_relative_difference(upload(gpu, lu).solve_many(rhs), orc.solve_many(lu, rhs)) < BAR
+
+
+def test_transposed_lu_of_a_single_row(gpu):
+    lu = host.lu(host.Matrix.from_triplets(1, 1, np.array([0]), np.array([0]), np.array([-2.5]), by_rows=False))
+    rhs = right_hand_sides(1, 9, 3)
+    x = GpuFactor.from_lu_transposed(gpu, lu).solve_many(rhs)
+    assert worst_relative_difference(x, orc.solve_many_lu(lu, rhs, transpose=True)) < BAR
+
+
 def test_two_by_two_blocks_and_a_single_row(gpu):
     lu = host.lu(two_by_two_blocks(40))
     rhs = right_hand_sides(80, 3, 1)

@@ -61,6 +61,7 @@ SIGNATURES: dict[str, tuple] = {
     "yb_gpu_synchronize": (i32, [vp, vp]),
     "yb_factor_from_cholesky": (i32, [vp, i64, vp, vp, vp, vp, C.POINTER(vp)]),
     "yb_factor_from_lu": (i32, [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]),
+    "yb_factor_from_lu_transposed": (i32, [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]),
     "yb_factor_free": (None, [vp]),
     "yb_factor_dim": (i64, [vp]),
     "yb_factor_block_width": (i64, [vp]),
@@ -77,6 +78,7 @@ SIGNATURES: dict[str, tuple] = {
     "yb_factor_set_phase_clock": (i32, [vp, vp]),
     "yb_factor_set_tail_level": (i32, [vp, i32, i32]),
     "yb_factor_set_domain": (i32, [vp, i32, i32, i32, i32, i32]),
+    "yb_factor_autotune": (i32, [vp, i32, i64, vp, P_dbl]),
     "yb_factor_domain_info": (i32, [vp, i32, P_i32, P_i32, P_i32, P_i64, P_i64, P_i64, P_dbl]),
     "yb_domain_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp, vp]),
     "yb_solve_many": (i32, [vp, vp, i64, vp]),

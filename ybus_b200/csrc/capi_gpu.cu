@@ -205,6 +205,25 @@ extern "C" int32_t yb_factor_from_lu(yb_gpu *gpu, int64_t n, const int64_t *l_pt
   });
 }
 
+extern "C" int32_t yb_factor_from_lu_transposed(yb_gpu *gpu, int64_t n, const int64_t *l_ptr, const int64_t *l_idx,
+                                                const double *l_val, const int64_t *u_ptr, const int64_t *u_idx,
+                                                const double *u_val, const int64_t *row_perm, const int64_t *col_perm,
+                                                yb_factor **out) {
+  return guard([&] {
+    require(gpu && out, "null argument");
+    require(n >= 0, "negative order");
+    require(n == 0 || (row_perm && col_perm), "null permutation");
+    // A' = Q U' L' P: forward with U' (U's columns read as rows: CSC of U is CSR of U'), backward
+    // with L' (unit diagonal stored first in L's columns, so first in L''s rows); b's slot i takes
+    // row Q[i], x's row P[i] comes from slot i (Lu::solve_transpose, lu.rs:506-533)
+    auto lower = csr_from_arrays(n, u_ptr, u_idx, u_val, true);
+    auto upper = csr_from_arrays(n, l_ptr, l_idx, l_val, true);
+    std::vector<int64_t> p(row_perm, row_perm + n), q(col_perm, col_perm + n);
+    *out = make_factor(gpu, n, std::move(lower), false, std::move(upper), q, p, YB_LU);
+    return YB_OK;
+  });
+}
+
 extern "C" void yb_factor_free(yb_factor *f) {
   if (!f) return;
   cudaSetDevice(f->gpu->device);
@@ -1009,6 +1028,75 @@ extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rh
     io.max_steps = max_steps, io.tolerance = tolerance;
     io.ratio_out = d_ratio, io.steps_out = d_steps;
     launch_domain<float>(f, cfg, count, io, s);
+    return YB_OK;
+  });
+}
+
+namespace yb {
+namespace {
+// Deterministic right-hand sides for timing: values in [-1, 1] from a multiplicative hash of the index
+__global__ void autotune_fill_kernel(double *b, int64_t total) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) b[i] = (double)((i * 2654435761LL) % 2001) / 1000.0 - 1.0;
+}
+}  // namespace
+}  // namespace yb
+
+extern "C" int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t count, int32_t *config, double *best_ms) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(!f->is_complex, "a complex factor has no domain solve to tune");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(count >= 1, "at least one right-hand side");
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    cudaStream_t s = f->gpu->stream;
+    const int64_t n = f->n;
+    DeviceArray<double> b((size_t)(n * count)), x((size_t)(n * count));
+    autotune_fill_kernel<<<(unsigned)((n * count + 255) / 256), 256, 0, s>>>(b.get(), n * count);
+    cuda_check(cudaGetLastError(), "autotune_fill_kernel launch");
+    TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
+    const TileConfig saved = t;
+    TileConfig best = saved;
+    double best_time = INFINITY;
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+    const int warps_list[] = {8, 12, 16}, page_list[] = {1536, 2048}, ring_list[] = {2, 3};
+    for (int warps : warps_list)
+      for (int page : page_list)
+        for (int ring : ring_list) {
+          TileConfig c = saved;
+          c.kind = kTileAuto;
+          c.domain_warps = warps, c.domain_page = page, c.domain_ring = ring;
+          TileConfig r;
+          try {
+            r = precision == YB_FP64 ? resolve<double>(f, c) : resolve<float>(f, c);
+          } catch (const host::Error &) {
+            continue;
+          }
+          if (r.kind != kTileDomain) continue;
+          for (int w = r.width; w >= 1 && w >= r.width / 2; w /= 2) {
+            TileConfig run = r;
+            run.width = w;
+            t = run;
+            solve_device(f, b.get(), n, x.get(), n, count, precision, s);  // warm-up
+            cuda_check(cudaEventRecord(e0, s), "cudaEventRecord");
+            for (int rep = 0; rep < 3; ++rep) solve_device(f, b.get(), n, x.get(), n, count, precision, s);
+            cuda_check(cudaEventRecord(e1, s), "cudaEventRecord");
+            cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float ms = 0;
+            cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            if (ms / 3 < best_time) best_time = ms / 3, best = run;
+          }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    t = std::isfinite(best_time) ? best : saved;
+    if (config) {
+      config[0] = t.kind, config[1] = t.width, config[2] = t.domain_warps, config[3] = t.domain_ring,
+      config[4] = t.domain_page;
+    }
+    if (best_ms) *best_ms = best_time;
     return YB_OK;
   });
 }

@@ -145,6 +145,17 @@ class GpuFactor:
         return cls(gpu, out.value)
 
     @classmethod
+    def from_lu_transposed(cls, gpu: Gpu, f: HostLu) -> "GpuFactor":
+        """The factor of Aᵀ from A's LU (`Lu::solve_transpose`, lu.rs:506-533): its solves solve Aᵀ x = b."""
+        if f.is_complex:
+            raise CudaError(_lib.YB_ERROR_INVALID_ARGUMENT, "a real LU factor only")
+        out = C.c_void_p()
+        _check(lib().yb_factor_from_lu_transposed(gpu._h, f.n, ptr(f.l.ptr), ptr(f.l.idx), ptr(f.l.val), ptr(f.u.ptr),
+                                                  ptr(f.u.idx), ptr(f.u.val), ptr(f.row_perm), ptr(f.col_perm),
+                                                  C.byref(out)))
+        return cls(gpu, out.value)
+
+    @classmethod
     def from_lu_complex(cls, gpu: Gpu, f: HostLu) -> "GpuFactor":
         """A complex128 LU factor (P A Q = L U of a Ybus), kept in complex128 and complex64."""
         if not f.is_complex:
@@ -225,6 +236,14 @@ class GpuFactor:
                                            C.byref(by), C.byref(sm), C.byref(cyc)))
         return {"tile": w.value, "cut": cut.value, "top": top.value, "records": rec.value, "bytes": by.value,
                 "smem": sm.value, "model_cycles": cyc.value}
+
+    def autotune(self, precision: int = FP64, count: int = 2048) -> dict:
+        """Times the domain solve's shapes on `count` right-hand sides and keeps the fastest."""
+        cfg = np.zeros(5, np.int32)
+        ms = C.c_double()
+        _check(lib().yb_factor_autotune(self._h, precision, count, ptr(cfg), C.byref(ms)))
+        return {"kind": int(cfg[0]), "tile": int(cfg[1]), "warps": int(cfg[2]), "ring": int(cfg[3]),
+                "page_bytes": int(cfg[4]), "ms": ms.value}
 
     def set_phase_clock(self, d_clock: int | None) -> None:
         """Diagnostics: a device buffer of 512 int64 for phase clocks (None to stop)."""
