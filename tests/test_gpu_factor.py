@@ -169,6 +169,28 @@ def test_repeated_solves_give_the_same_bits(gpu):
         assert np.array_equal(again.view(np.uint64), first.view(np.uint64))
 
 
+@pytest.mark.parametrize("pinned", [False, True])
+def test_host_array_solve_overlaps_many_chunks(gpu, pinned):
+    # 5,000 right-hand sides pass through the copy pipeline in 8 chunks, twice round its 4 slots
+    import torch
+    chol = host.cholesky(random_spd(300, 3, 7))
+    rhs = right_hand_sides(300, 5000, 29)
+    factor = upload(gpu, chol)
+    b, out = np.ascontiguousarray(rhs), np.zeros_like(rhs)
+    if pinned:
+        tb, tx = torch.from_numpy(b).pin_memory(), torch.zeros(out.shape, dtype=torch.float64).pin_memory()
+        b, out = tb.numpy(), tx.numpy()
+    factor.solve_many_into(b, out)
+    assert factor.timings().blocks == 8
+    sample = np.arange(0, 5000, 41)
+    assert worst_relative_difference(out[sample], orc.solve_many(chol, rhs[sample])) < BAR
+    again = np.zeros_like(out)
+    factor.set_block_width(3)  # blocks narrower than a chunk: one chunk per block
+    factor.solve_many_into(b, again)
+    assert np.array_equal(again[:7].view(np.uint64), out[:7].view(np.uint64)) or \
+        worst_relative_difference(again[sample], out[sample]) < BAR
+
+
 def test_empty_and_mismatched_right_hand_sides(gpu):
     chol = host.cholesky(random_spd(10, 20, 1))
     factor = upload(gpu, chol)

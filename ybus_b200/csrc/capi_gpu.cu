@@ -613,10 +613,24 @@ void launch_domain_w(yb_factor *f, const TileConfig &cfg, int64_t count, const I
   a.tail_slot = d->tail_slot.get();
   a.error = f->error.get();
   a.phase_clock = f->phase_clock;
-  cuda_check(cudaFuncSetAttribute(domain_tile_kernel<T, W, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+  // the footprint keeps kIoStaticSmem for the IO policy's static shared memory (its reductions,
+  // which grow with W); a policy that needs more at this width runs at half the width
+  cudaFuncAttributes attr{};
+  cuda_check(cudaFuncGetAttributes(&attr, domain_tile_kernel<T, W, IO>), "cudaFuncGetAttributes");
+  const size_t dynamic = smem - kIoStaticSmem;
+  if (dynamic + attr.sharedSizeBytes > (size_t)f->gpu->smem_optin) {
+    if constexpr (W > 1) {
+      TileConfig half = cfg;
+      half.width = W / 2;
+      return launch_domain_w<T, W / 2, IO>(f, half, count, io, stream);
+    } else {
+      throw host::Error(host::kInvalidArgument, "the tile does not fit in shared memory");
+    }
+  }
+  cuda_check(cudaFuncSetAttribute(domain_tile_kernel<T, W, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynamic),
              "cudaFuncSetAttribute");
   const int64_t grid = std::min<int64_t>(a.tiles, (int64_t)f->gpu->sm_count);
-  domain_tile_kernel<T, W, IO><<<(unsigned)grid, cfg.domain_warps * 32, smem, stream>>>(a, io);
+  domain_tile_kernel<T, W, IO><<<(unsigned)grid, cfg.domain_warps * 32, dynamic, stream>>>(a, io);
   cuda_check(cudaGetLastError(), "domain_tile_kernel launch");
 }
 
@@ -816,10 +830,15 @@ extern "C" int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count,
     }
     cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
     cudaStream_t s = f->gpu->stream;
-    const int64_t width = f->width;
-    const int64_t chunk = std::min(width, count);
-    f->dev_b.reserve((size_t)(n * chunk));
-    f->dev_x.reserve((size_t)(n * chunk));
+    // Chunks of at most the block width, small enough that uploads, solves and downloads of
+    // successive chunks overlap (at least 256 right-hand sides, so a solve still fills the GPU)
+    const int64_t chunk = std::min<int64_t>(f->width, std::min<int64_t>(kPipelineChunk, std::max<int64_t>(256, (count + 7) / 8)));
+    constexpr int S = CopyPipeline::kSlots;
+    auto &pipe = f->pipe;
+    pipe.ensure();
+    const size_t slot_values = (size_t)(n * std::min(chunk, count));
+    f->dev_b.reserve(slot_values * S);
+    f->dev_x.reserve(slot_values * S);
     auto is_pinned = [](const void *p) {
       cudaPointerAttributes attr{};
       if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
@@ -829,40 +848,67 @@ extern "C" int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count,
       return attr.type == cudaMemoryTypeHost;
     };
     const bool pinned_in = is_pinned(rhs), pinned_out = is_pinned(out);
-    double *stage = (!pinned_in || !pinned_out) ? (double *)f->staging.get((size_t)(n * chunk) * sizeof(double)) : nullptr;
-    using clock = std::chrono::steady_clock;
-    for (int64_t k0 = 0; k0 < count; k0 += width) {
-      const int64_t cols = std::min(width, count - k0);
-      const size_t bytes = (size_t)(n * cols) * sizeof(double);
-      const double *src = rhs + k0 * n;
-      if (!pinned_in) {
-        std::memcpy(stage, src, bytes);
-        src = stage;
-      }
-      const auto t0 = clock::now();
-      cuda_check(cudaMemcpyAsync(f->dev_b.get(), src, bytes, cudaMemcpyHostToDevice, s), "upload");
-      cuda_check(cudaStreamSynchronize(s), "upload");
-      const auto t1 = clock::now();
-      solve_device(f, f->dev_b.get(), n, f->dev_x.get(), n, cols, YB_FP64, s);
-      cuda_check(cudaStreamSynchronize(s), "solve");
-      {
-        int32_t word = 0;
-        cuda_check(cudaMemcpy(&word, f->error.get(), sizeof word, cudaMemcpyDeviceToHost), "read error word");
-        if (word != 0) {
-          cuda_check(cudaMemset(f->error.get(), 0, sizeof word), "clear error word");
-          throw host::Error(host::kDeviceTimeout, "a bounded device wait ran out in the streamed solve");
-        }
-      }
-      const auto t2 = clock::now();
-      double *dst = pinned_out ? out + k0 * n : stage;
-      cuda_check(cudaMemcpyAsync(dst, f->dev_x.get(), bytes, cudaMemcpyDeviceToHost, s), "download");
-      cuda_check(cudaStreamSynchronize(s), "download");
-      const auto t3 = clock::now();
-      if (!pinned_out) std::memcpy(out + k0 * n, stage, bytes);
-      f->timings.upload += std::chrono::duration<double>(t1 - t0).count();
-      f->timings.solve += std::chrono::duration<double>(t2 - t1).count();
-      f->timings.download += std::chrono::duration<double>(t3 - t2).count();
+    int64_t slot_k0[S], slot_cols[S];
+    bool busy[S] = {};
+    // Waits for the chunk in `slot` to come back, unstages it and adds its stages' times
+    auto finish = [&](int slot) {
+      if (!busy[slot]) return;
+      busy[slot] = false;
+      cudaEvent_t *e = pipe.ev[slot];
+      cuda_check(cudaEventSynchronize(e[CopyPipeline::kOutDone]), "download");
+      const size_t bytes = (size_t)(n * slot_cols[slot]) * sizeof(double);
+      if (!pinned_out) std::memcpy(out + slot_k0[slot] * n, pipe.stage_out[slot].get(bytes), bytes);
+      float up = 0, solve = 0, down = 0;
+      cuda_check(cudaEventElapsedTime(&up, e[CopyPipeline::kInStart], e[CopyPipeline::kInDone]), "cudaEventElapsedTime");
+      cuda_check(cudaEventElapsedTime(&solve, e[CopyPipeline::kSolveStart], e[CopyPipeline::kSolved]), "cudaEventElapsedTime");
+      cuda_check(cudaEventElapsedTime(&down, e[CopyPipeline::kOutStart], e[CopyPipeline::kOutDone]), "cudaEventElapsedTime");
+      f->timings.upload += up * 1e-3;
+      f->timings.solve += solve * 1e-3;
+      f->timings.download += down * 1e-3;
       f->timings.blocks += 1;
+    };
+    int64_t c = 0;
+    try {
+      for (int64_t k0 = 0; k0 < count; k0 += chunk, ++c) {
+        const int slot = (int)(c % S);
+        finish(slot);  // the slot's previous chunk is back: its buffers are free
+        const int64_t cols = std::min(chunk, count - k0);
+        const size_t bytes = (size_t)(n * cols) * sizeof(double);
+        double *db = f->dev_b.get() + slot * slot_values, *dx = f->dev_x.get() + slot * slot_values;
+        cudaEvent_t *e = pipe.ev[slot];
+        const double *src = rhs + k0 * n;
+        if (!pinned_in) {
+          auto *stage = (double *)pipe.stage_in[slot].get(bytes);
+          std::memcpy(stage, src, bytes);
+          src = stage;
+        }
+        double *dst = pinned_out ? out + k0 * n : (double *)pipe.stage_out[slot].get(bytes);
+        cuda_check(cudaEventRecord(e[CopyPipeline::kInStart], pipe.in), "cudaEventRecord");
+        cuda_check(cudaMemcpyAsync(db, src, bytes, cudaMemcpyHostToDevice, pipe.in), "upload");
+        cuda_check(cudaEventRecord(e[CopyPipeline::kInDone], pipe.in), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(s, e[CopyPipeline::kInDone], 0), "cudaStreamWaitEvent");
+        cuda_check(cudaEventRecord(e[CopyPipeline::kSolveStart], s), "cudaEventRecord");
+        solve_device(f, db, n, dx, n, cols, YB_FP64, s);
+        cuda_check(cudaEventRecord(e[CopyPipeline::kSolved], s), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(pipe.out, e[CopyPipeline::kSolved], 0), "cudaStreamWaitEvent");
+        cuda_check(cudaEventRecord(e[CopyPipeline::kOutStart], pipe.out), "cudaEventRecord");
+        cuda_check(cudaMemcpyAsync(dst, dx, bytes, cudaMemcpyDeviceToHost, pipe.out), "download");
+        cuda_check(cudaEventRecord(e[CopyPipeline::kOutDone], pipe.out), "cudaEventRecord");
+        slot_k0[slot] = k0, slot_cols[slot] = cols, busy[slot] = true;
+      }
+      for (int64_t i = 0; i < S; ++i) finish((int)((c + i) % S));
+    } catch (...) {
+      // leave no copy in flight into the caller's arrays or the staging
+      cudaStreamSynchronize(pipe.in);
+      cudaStreamSynchronize(s);
+      cudaStreamSynchronize(pipe.out);
+      throw;
+    }
+    int32_t word = 0;
+    cuda_check(cudaMemcpy(&word, f->error.get(), sizeof word, cudaMemcpyDeviceToHost), "read error word");
+    if (word != 0) {
+      cuda_check(cudaMemset(f->error.get(), 0, sizeof word), "clear error word");
+      throw host::Error(host::kDeviceTimeout, "a bounded device wait ran out in the solve");
     }
     return YB_OK;
   });

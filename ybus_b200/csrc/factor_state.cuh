@@ -17,6 +17,8 @@
 // block is one cuSPARSE SpSM call (ybus_cuda/src/factor.rs:12); here a block is one persistent
 // launch that needs at least one tile per SM to fill the GPU, so the cap is higher.
 constexpr int64_t kMaxDefaultWidth = 65536;
+// The largest chunk of right-hand sides the host-array solve moves through its copy pipeline
+constexpr int64_t kPipelineChunk = 1024;
 // The widest block a single-row factor uses (ybus_cuda/src/factor.rs:14-16): kept for API parity.
 constexpr int64_t kSingleRowWidth = 64;
 
@@ -37,6 +39,36 @@ namespace yb {
 struct Timings {
   double upload = 0, solve = 0, download = 0;
   int64_t blocks = 0;
+};
+
+// The host-array solve's overlap: chunks of right-hand sides pass through an upload stream, the
+// solve stream and a download stream, so the two copy engines and the SMs work on successive
+// chunks at once. Each of kSlots slots holds one chunk's device buffers (and, for pageable host
+// arrays, pinned staging) and the events that time its three stages.
+struct CopyPipeline {
+  static constexpr int kSlots = 4;
+  enum { kInStart, kInDone, kSolveStart, kSolved, kOutStart, kOutDone, kEvents };
+  int device = -1;
+  cudaStream_t in = nullptr, out = nullptr;
+  cudaEvent_t ev[kSlots][kEvents] = {};
+  PinnedBuffer stage_in[kSlots], stage_out[kSlots];
+  CopyPipeline() = default;
+  CopyPipeline(const CopyPipeline &) = delete;
+  CopyPipeline &operator=(const CopyPipeline &) = delete;
+  ~CopyPipeline() {
+    for (auto &slot : ev)
+      for (auto &e : slot)
+        if (e) cudaEventDestroy(e);
+    if (in) cudaStreamDestroy(in);
+    if (out) cudaStreamDestroy(out);
+  }
+  void ensure() {
+    if (in) return;
+    cuda_check(cudaStreamCreateWithFlags(&in, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaStreamCreateWithFlags(&out, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto &slot : ev)
+      for (auto &e : slot) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+  }
 };
 
 // Which tile solve runs: the shared-memory one (the tile's working vector in shared memory) when
@@ -127,6 +159,7 @@ struct yb_factor {
   yb::DeviceArray<int32_t> za_ptr, za_idx;
   yb::DeviceArray<yb::cplx<double>> za_val;
   yb::PinnedBuffer staging;
+  yb::CopyPipeline pipe;
   int64_t width = 1;
   yb::Timings timings;
   bool single = false;
