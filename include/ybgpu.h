@@ -144,12 +144,30 @@ int32_t yb_factor_plan_info(const yb_factor *f, int32_t *fwd_levels, int32_t *bw
  * of two; threads a multiple of 32 up to 512; resident blocks per SM 1..8). */
 int32_t yb_factor_set_tile(yb_factor *f, int32_t precision, int32_t tile_width, int32_t threads,
                            int32_t blocks_per_sm);
-/* No ybus counterpart: which tile solve runs for a precision: 0 automatic (the domain solve at the
- * widest tile that fits in shared memory; else the streamed solve likewise; else the
- * global-scratch solve), 1 the level-sliced shared-memory solve, 2 the global-scratch solve, 3 the
- * streamed solve, 4 the domain solve (1, 3 and 4 give YB_ERROR_INVALID_ARGUMENT at launch if the
- * tile does not fit in shared memory or, for 4, the factor admits no domain layout). */
+/* No ybus counterpart: which tile solve runs for a precision: 0 automatic (the lane solve for
+ * solves of at least the lane threshold's right-hand sides when the factor admits it; else the
+ * domain solve at the widest tile that fits in shared memory; else the streamed solve likewise;
+ * else the global-scratch solve), 1 the level-sliced shared-memory solve, 2 the global-scratch
+ * solve, 3 the streamed solve, 4 the domain solve, 5 the lane solve (1, 3, 4 and 5 give
+ * YB_ERROR_INVALID_ARGUMENT at launch if the tile does not fit in shared memory or the factor
+ * admits no domain or lane layout). The lane solve serves yb_solve_many_device and yb_solve_many;
+ * the pair, refined and batched solves take the automatic choice among the others. */
 int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int32_t kind);
+/* No ybus counterpart: the lane solve (one right-hand side per lane, a block of warps per 32; the
+ * factor's rows in an elimination-tree postorder cut into subtree domains the warps take in
+ * parallel under a top warp 0 takes, a few tens of live values per lane in shared memory; b, the
+ * forward results and x streaming through a work array in HBM). info receives 12 values: {slots,
+ * pages, page bytes, forward peak of live values, backward peak, entries of both sweeps, shared
+ * memory per block, warps per block, domains, top rows, partial values per block, 0};
+ * YB_ERROR_INVALID_ARGUMENT if the factor admits no lane layout (no postorder serves both sweeps,
+ * or too many live values). */
+int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t *info);
+/* No ybus counterpart: the lane solve's shape for a precision: warps per block (1..8, default 6)
+ * and page bytes (256..16384, a multiple of 16, default 2048). */
+int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32_t page_bytes);
+/* No ybus counterpart: the number of right-hand sides from which the automatic choice takes the
+ * lane solve (default 8192). */
+int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t min_count);
 /* No ybus counterpart: the streamed solve's shape for a precision: warps per block (1..16), pages
  * in flight per warp (2..16), page bytes (512..16384, a multiple of 16), and the row count under
  * which a level is taken by one warp alone (0: twice a slice's rows). */
@@ -179,6 +197,16 @@ int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_t *tile_wid
  * {kind, tile width, warps, ring, page bytes} and best_ms its time (either may be NULL). With no
  * domain solve to tune, the configuration is left as it was. */
 int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t count, int32_t *config, double *best_ms);
+/* No ybus counterpart, diagnostics on the host (no GPU needed): the lane solve's layout for a
+ * Cholesky factor given as to yb_factor_from_cholesky, values of `value_bytes` (8 or 4), `warps`
+ * warps per block. info receives 12 values: {slots, pages, page bytes, forward peak of live
+ * values, backward peak, forward entries, backward entries, warps, domains, top rows, partial
+ * values per block, 0}; blob (pages * page_bytes bytes), warp_page (warps + 1), in_pos and out_pos
+ * (n each: the work-array position of each row of b and of x) may be NULL. */
+int32_t yb_lane_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
+                                const int64_t *perm, int32_t value_bytes, int32_t page_bytes, int32_t max_slots,
+                                int32_t warps, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *in_pos,
+                                int32_t *out_pos);
 /* No ybus counterpart, diagnostics on the host (no GPU needed): the domain layout a Cholesky factor
  * given as to yb_factor_from_cholesky gets for `value_bytes` (8 or 4). info receives {cut, top
  * rows, stages, warps, pages, records, entries, page bytes}, top_condition the worse infinity-norm

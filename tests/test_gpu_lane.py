@@ -1,0 +1,132 @@
+"""The lane solve (one right-hand side per lane, the factor's rows in an elimination-tree postorder,
+b and x through a work array in solve order) against the oracle's CPU solves: counts around a
+warp's 32, dense columns split over several records, FP32, leading dimensions above n, repeats bit
+for bit, and the 10,000-bus grid. All calls go through the C ABI."""
+import numpy as np
+import pytest
+
+import oracle.oracle as orc
+from fixtures import random_spd, random_square, right_hand_sides, worst_relative_difference
+from ybus_b200 import FP32, FP64, CudaError, GpuFactor, grids, host
+
+pytestmark = pytest.mark.gpu
+
+BAR = 1e-12
+LANE = 5
+
+
+@pytest.mark.parametrize("warps", [1, 2, 4, 8])
+@pytest.mark.parametrize("count", [1, 31, 32, 33, 200])
+def test_lane_solve_matches_the_cpu(gpu, count, warps):
+    chol = host.cholesky(random_spd(200, 3, 7))
+    rhs = right_hand_sides(200, count, 11)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.set_tile_kind(FP64, LANE)
+    factor.set_lane(FP64, warps)
+    d = worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs))
+    assert d < BAR, f"count {count} warps {warps}: {d:e}"
+    factor.check_error()
+
+
+@pytest.mark.parametrize("warps", [1, 3])
+def test_dense_columns_over_several_records(gpu, warps):
+    # 512-byte pages hold 31 entries: the dense columns take several records each
+    chol = host.cholesky(random_spd(150, 30, 7))
+    rhs = right_hand_sides(150, 70, 3)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.set_tile_kind(FP64, LANE)
+    factor.set_lane(FP64, warps, 512)
+    info = factor.lane_info(FP64)
+    assert info["slots"] >= 1 and info["pages"] >= 1 and info["page_bytes"] == 512
+    d = worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs))
+    assert d < BAR, f"{d:e}"
+
+
+def test_device_arrays_with_leading_dimensions_and_fp32(gpu):
+    import torch
+    chol = host.cholesky(random_spd(300, 3, 7))
+    rhs = right_hand_sides(300, 45, 11)
+    cpu = orc.solve_many(chol, rhs)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    for prec, bar in ((FP64, BAR), (FP32, 1e-4)):
+        factor.set_tile_kind(prec, LANE)
+        b = torch.zeros((45, 310), dtype=torch.float64, device="cuda")
+        b[:, :300] = torch.from_numpy(rhs).cuda()
+        x = torch.full((45, 320), 7.0, dtype=torch.float64, device="cuda")
+        factor.solve_many_device(b.data_ptr(), x.data_ptr(), 45, prec, None, ldb=310, ldx=320)
+        gpu.synchronize()
+        xs = x.cpu().numpy()
+        assert worst_relative_difference(xs[:, :300], cpu) < bar
+        assert np.all(xs[:, 300:] == 7.0), "rows past n are not written"
+
+
+def test_repeated_lane_solves_give_the_same_bits(gpu):
+    chol = host.cholesky(random_spd(300, 3, 7))
+    rhs = right_hand_sides(300, 100, 17)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.set_tile_kind(FP64, LANE)
+    first = factor.solve_many(rhs)
+    for _ in range(3):
+        assert np.array_equal(factor.solve_many(rhs).view(np.uint64), first.view(np.uint64))
+
+
+def test_the_automatic_choice_takes_the_lane_solve_from_its_threshold(gpu):
+    chol = host.cholesky(random_spd(120, 3, 9))
+    rhs = right_hand_sides(120, 96, 5)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.set_lane_min_count(FP64, 64)
+    d = worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs))
+    assert d < BAR
+
+
+def test_an_lu_factor_solves_or_is_refused(gpu):
+    lu = host.lu(random_square(250, 4, 3))
+    rhs = right_hand_sides(250, 40, 5)
+    factor = GpuFactor.from_lu(gpu, lu)
+    factor.set_tile_kind(FP64, LANE)
+    try:
+        factor.lane_info(FP64)
+    except CudaError:
+        with pytest.raises(CudaError):
+            factor.solve_many(rhs)
+        return
+    assert worst_relative_difference(factor.solve_many(rhs), orc.solve_many(lu, rhs)) < BAR
+
+
+def test_lane_solve_on_the_10k_grid(gpu):
+    import torch
+    g = grids.make_grid(10000, 3500, grids.SEED_BASE + 2)
+    r, c, v = grids.bbus_triplets(g)
+    keep = np.arange(1, 10000)
+    bp = host.Matrix.from_triplets(10000, 10000, r, c, v).select(keep, keep)
+    chol = host.cholesky(bp)
+    rhs = np.random.default_rng(5).standard_normal((1000, chol.n))
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    assert factor.lane_info(FP64)["slots"] <= 48
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    for prec, bar, warps in ((FP64, BAR, 1), (FP64, BAR, 6), (FP64, BAR, 8), (FP32, 1e-3, 4)):
+        factor.set_tile_kind(prec, LANE)
+        factor.set_lane(prec, warps)
+        x.zero_()
+        factor.solve_many_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], prec, None)
+        gpu.synchronize()
+        factor.check_error()
+        xs = x.cpu().numpy()
+        sample = np.arange(0, 1000, 37)
+        d = worst_relative_difference(xs[sample], orc.solve_many(chol, rhs[sample], threads=8))
+        assert d < bar, f"precision {prec}: {d:e}"
+        if prec == FP64:
+            p, i, v = bp.arrays()
+            assert max(orc.relative_residual(p, i, v, xs[k], rhs[k]) for k in range(0, 1000, 97)) < 1e-11
+
+
+def test_a_factor_with_too_many_live_values_takes_another_solve(gpu):
+    # a random pattern keeps hundreds of values alive: the automatic choice passes the lane solve by
+    chol = host.cholesky(random_spd(500, 2, 13))
+    rhs = right_hand_sides(500, 64, 17)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.set_lane_min_count(FP64, 0)
+    with pytest.raises(CudaError):
+        factor.lane_info(FP64)
+    assert worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs)) < BAR

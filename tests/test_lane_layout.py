@@ -1,0 +1,67 @@
+"""The lane solve's layout, checked on the CPU: the record streams the layout builder makes,
+executed by a host interpreter of the kernel's semantics (warps between block barriers), solve the
+reference's fixture matrices and the synthetic grids to the oracle's solutions, with few live
+values (no GPU)."""
+import numpy as np
+import pytest
+
+import oracle.oracle as orc
+from fixtures import random_spd, right_hand_sides, worst_relative_difference
+from lane_interp import run
+from ybus_b200 import YbError, grids, host
+
+
+def grid_factor(n_bus, extra, seed):
+    g = grids.make_grid(n_bus, extra, seed)
+    r, c, v = grids.bbus_triplets(g)
+    keep = np.arange(1, n_bus)
+    return host.cholesky(host.Matrix.from_triplets(n_bus, n_bus, r, c, v).select(keep, keep))
+
+
+@pytest.mark.parametrize("warps", [1, 3, 8])
+@pytest.mark.parametrize("page", [256, 2048])
+@pytest.mark.parametrize("fill", [2, 6, 30])
+def test_lane_records_solve_the_fixture(page, fill, warps):
+    # fill 30: dense columns that take several records each on the smallest page
+    chol = host.cholesky(random_spd(150, fill, 7))
+    rhs = right_hand_sides(150, 5, 11)
+    lay = host.lane_layout(chol, 8, page, warps=warps)
+    d = worst_relative_difference(run(lay, chol.n, rhs), orc.solve_many(chol, rhs))
+    assert d < 1e-12, f"page {page} warps {warps}: {d:e}"
+    assert lay["fwd_entries"] == lay["bwd_entries"] == int(np.asarray(chol.l.ptr)[-1]) - chol.n
+
+
+def test_lane_records_in_fp32_are_close():
+    chol = host.cholesky(random_spd(200, 4, 3))
+    rhs = right_hand_sides(200, 3, 5)
+    lay = host.lane_layout(chol, 4, 1024, warps=4)
+    assert worst_relative_difference(run(lay, chol.n, rhs), orc.solve_many(chol, rhs)) < 1e-4
+
+
+@pytest.mark.parametrize("warps", [1, 4, 8])
+def test_the_10k_grid_keeps_few_live_values(warps):
+    chol = grid_factor(10000, 3500, grids.SEED_BASE + 2)
+    lay = host.lane_layout(chol, 8, 2048, warps=warps)
+    # the postorder with larger subtrees first keeps a few tens of values alive per lane
+    assert lay["slots"] <= 48, lay["slots"]
+    if warps > 1:
+        assert lay["domains"] >= warps and lay["top"] < chol.n // 10, (lay["domains"], lay["top"])
+    assert sorted(lay["in_pos"]) == list(range(chol.n))
+    rhs = np.random.default_rng(3).standard_normal((2, chol.n))
+    d = worst_relative_difference(run(lay, chol.n, rhs), orc.solve_many(chol, rhs))
+    assert d < 1e-12, d
+
+
+def test_too_many_live_values_is_refused():
+    chol = host.cholesky(random_spd(120, 30, 9))
+    with pytest.raises(YbError):
+        host.lane_layout(chol, 8, 2048, max_slots=4)
+
+
+def test_a_single_row_and_a_diagonal_matrix():
+    for n, fill in ((1, 100), (40, 0)):
+        for warps in (1, 4):
+            chol = host.cholesky(random_spd(n, fill, 5))
+            rhs = right_hand_sides(n, 3, 2)
+            lay = host.lane_layout(chol, 8, 512, warps=warps)
+            assert worst_relative_difference(run(lay, n, rhs), orc.solve_many(chol, rhs)) < 1e-12

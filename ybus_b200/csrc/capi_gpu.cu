@@ -10,6 +10,7 @@
 #include "device.cuh"
 #include "factor_state.cuh"
 #include "domain_solve.cuh"
+#include "lane_solve.cuh"
 #include "smem_solve.cuh"
 #include "stream_solve.cuh"
 #include "solve.cuh"
@@ -300,7 +301,7 @@ extern "C" int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int3
   return guard([&] {
     require(f != nullptr, "null factor");
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
-    require(kind >= kTileAuto && kind <= kTileDomain, "unknown tile kind");
+    require(kind >= kTileAuto && kind <= kTileLane, "unknown tile kind");
     (precision == YB_FP64 ? f->tile64 : f->tile32).kind = kind;
     return YB_OK;
   });
@@ -648,7 +649,78 @@ void launch_domain(yb_factor *f, const TileConfig &cfg, int64_t count, const IO 
 
 // The shape the auto kind runs: the streamed solve at the widest tile whose working vector and
 // page rings fit in shared memory (one block per SM), else the global-scratch kernel.
+// The lane solve's page ring, the most slots a layout may take (the automatic choice takes the lane
+// solve only up to kLaneAutoSlots, which leave room for several blocks per SM), and the largest
+// work array one launch fills (larger solves run in several launches)
+constexpr int32_t kLaneRing = 2, kLaneMaxSlots = 256, kLaneAutoSlots = 64;
+constexpr size_t kLaneWorkBytes = size_t(2) << 30;
+
+template <class T> DeviceLane *lane_for(yb_factor *f, int warps, int page_bytes, cudaStream_t stream) {
+  const auto key = std::make_tuple((int)sizeof(T), warps, page_bytes);
+  auto it = f->lanes.find(key);
+  if (it != f->lanes.end()) return it->second.get();
+  std::unique_ptr<DeviceLane> d;
+  try {
+    const LaneLayout lay = lane_layout(f->plan, (int)sizeof(T), page_bytes, kLaneMaxSlots, warps);
+    d = std::make_unique<DeviceLane>();
+    d->warps = lay.warps, d->slots = lay.slots, d->page_bytes = lay.page_bytes, d->domains = lay.domains;
+    d->top = lay.top, d->partials = lay.partials, d->fwd_live = lay.fwd_live, d->bwd_live = lay.bwd_live;
+    d->entries = lay.fwd_entries + lay.bwd_entries, d->pages = lay.warp_page.back();
+    d->blob.upload(lay.blob, stream);
+    d->warp_page.upload(lay.warp_page, stream);
+    d->in_pos.upload(lay.in_pos, stream);
+    d->out_pos.upload(lay.out_pos, stream);
+    cuda_check(cudaStreamSynchronize(stream), "lane layout upload");
+  } catch (const host::Error &e) {
+    if (e.status != host::kInvalidArgument && e.status != host::kTooLarge) throw;
+    d.reset();
+  }
+  auto *out = d.get();
+  f->lanes.emplace(key, std::move(d));
+  return out;
+}
+
+template <class T> size_t lane_smem(const DeviceLane *d) {
+  return (size_t)d->warps * lane_warp_bytes<T>(d->slots, kLaneRing, d->page_bytes);
+}
+
+// The lane solve of `count` right-hand sides: gather into the work array, solve in place, scatter.
+template <class T>
+void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
+                 cudaStream_t stream) {
+  const int64_t n = f->n;
+  const size_t group_bytes = (size_t)n * 32 * sizeof(T);
+  const int64_t groups_all = (count + 31) / 32;
+  const int64_t per_launch = std::max<int64_t>(1, std::min<int64_t>(groups_all, (int64_t)(kLaneWorkBytes / group_bytes)));
+  f->lane_work.reserve((size_t)per_launch * group_bytes);
+  f->lane_partial.reserve((size_t)per_launch * std::max(d->partials, 1) * 32 * sizeof(T));
+  T *work = reinterpret_cast<T *>(f->lane_work.get());
+  T *partial = reinterpret_cast<T *>(f->lane_partial.get());
+  const size_t smem = lane_smem<T>(d);
+  if (smem > (size_t)f->gpu->smem_optin) throw host::Error(host::kInvalidArgument, "the lane solve's block does not fit in shared memory");
+  cuda_check(cudaFuncSetAttribute(lane_solve_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  LaneArgs a{};
+  a.n = (int32_t)n;
+  a.slots = d->slots, a.page_bytes = d->page_bytes, a.ring = kLaneRing, a.partials = d->partials;
+  a.blob = d->blob.get();
+  a.warp_page = d->warp_page.get();
+  a.error = f->error.get();
+  for (int64_t g0 = 0; g0 < groups_all; g0 += per_launch) {
+    const int64_t groups = std::min(per_launch, groups_all - g0);
+    const int64_t cols = std::min(count - g0 * 32, groups * 32);
+    const dim3 io_grid((unsigned)((n + 63) / 64), (unsigned)std::min<int64_t>(groups, 65535));
+    lane_in_kernel<T><<<io_grid, 256, 0, stream>>>(b + g0 * 32 * ldb, ldb, cols, (int32_t)n, groups, d->in_pos.get(), work);
+    cuda_check(cudaGetLastError(), "lane_in_kernel launch");
+    lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
+    cuda_check(cudaGetLastError(), "lane_solve_kernel launch");
+    lane_out_kernel<T><<<io_grid, 256, 0, stream>>>(work, cols, (int32_t)n, groups, d->out_pos.get(), x + g0 * 32 * ldx, ldx);
+    cuda_check(cudaGetLastError(), "lane_out_kernel launch");
+  }
+}
+
 template <class T> TileConfig resolve(yb_factor *f, TileConfig cfg) {
+  if (cfg.kind == kTileLane) cfg.kind = kTileAuto;  // callers other than the plain solve
   if (cfg.kind == kTileGlobal) return cfg;
   if (cfg.kind == kTileDomain || cfg.kind == kTileAuto) {
     DeviceDomain *d = domain_for<T>(f, cfg, f->gpu->stream);
@@ -714,6 +786,14 @@ void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t
   if (count <= 0 || f->n == 0) return;
   auto run = [&](auto zero, const TileConfig &configured, auto &fwd, auto &bwd, auto &scratch, auto &cache) {
     using T = decltype(zero);
+    if (configured.kind == kTileLane || (configured.kind == kTileAuto && count >= configured.lane_min_count)) {
+      DeviceLane *d = lane_for<T>(f, configured.lane_warps, configured.lane_page, stream);
+      if (d && (configured.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
+        launch_lane<T>(f, d, b, ldb, x, ldx, count, stream);
+        return;
+      }
+      if (configured.kind == kTileLane) throw host::Error(host::kInvalidArgument, "the factor admits no lane layout");
+    }
     const TileConfig cfg = resolve<T>(f, configured);
     if (cfg.kind == kTileDomain) {
       DenseIO io{b, ldb, x, ldx, f->in_slot.get(), f->out_slot.get()};
@@ -997,6 +1077,46 @@ extern "C" int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_
     if (smem_bytes)
       *smem_bytes = (int64_t)(precision == YB_FP64 ? domain_smem<double>(f, cfg, d, cfg.width) : domain_smem<float>(f, cfg, d, cfg.width));
     if (model_cycles) *model_cycles = d->cost;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t *info) {
+  return guard([&] {
+    require(f != nullptr && info != nullptr, "null argument");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(!f->is_complex, "a complex factor has no lane solve");
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    const TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
+    DeviceLane *d = precision == YB_FP64 ? lane_for<double>(f, t.lane_warps, t.lane_page, f->gpu->stream)
+                                         : lane_for<float>(f, t.lane_warps, t.lane_page, f->gpu->stream);
+    if (!d) throw host::Error(host::kInvalidArgument, "the factor admits no lane layout");
+    const size_t smem = precision == YB_FP64 ? lane_smem<double>(d) : lane_smem<float>(d);
+    const int64_t v[12] = {d->slots, d->pages, d->page_bytes, d->fwd_live, d->bwd_live, d->entries, (int64_t)smem,
+                           d->warps, d->domains, d->top, d->partials, 0};
+    std::copy(v, v + 12, info);
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32_t page_bytes) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(warps >= 1 && warps <= kLaneMaxWarps, "1 to 8 warps per block");
+    require(page_bytes >= 256 && page_bytes <= 16384 && page_bytes % 16 == 0, "pages of 256 to 16384 bytes, a multiple of 16");
+    TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
+    t.lane_warps = warps, t.lane_page = page_bytes;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t min_count) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(min_count >= 0, "negative count");
+    (precision == YB_FP64 ? f->tile64 : f->tile32).lane_min_count = min_count;
     return YB_OK;
   });
 }

@@ -73,7 +73,7 @@ struct CopyPipeline {
 
 // Which tile solve runs: the shared-memory one (the tile's working vector in shared memory) when
 // it fits, or the one whose working vectors live in a global scratch buffer.
-enum TileKind : int { kTileAuto = 0, kTileShared = 1, kTileGlobal = 2, kTileStream = 3, kTileDomain = 4 };
+enum TileKind : int { kTileAuto = 0, kTileShared = 1, kTileGlobal = 2, kTileStream = 3, kTileDomain = 4, kTileLane = 5 };
 
 // The launch shape of the tile solve for one precision.
 struct TileConfig {
@@ -88,6 +88,18 @@ struct TileConfig {
   // the domain solve's shape: warps per block, pages in flight per warp, page bytes, and the cut
   // (first forward level of the top block; -1: chosen by the layout's cost model)
   int domain_warps = 16, domain_ring = 2, domain_page = 2048, domain_cut = -1;
+  // the automatic choice takes the lane solve from this many right-hand sides on (one warp per 32:
+  // fewer leave SMs idle, where the domain solve's tiles spread over all of them)
+  int64_t lane_min_count = 8192;
+  int lane_warps = 6, lane_page = 2048;  // the lane solve's warps per block (one group of 32 right-hand sides), page bytes
+};
+
+// A lane layout on the device (LaneLayout in plan.hpp).
+struct DeviceLane {
+  int32_t warps = 0, slots = 0, page_bytes = 0, domains = 0, top = 0, partials = 0, fwd_live = 0, bwd_live = 0;
+  int64_t entries = 0, pages = 0;
+  DeviceArray<uint8_t> blob;
+  DeviceArray<int32_t> warp_page, in_pos, out_pos;
 };
 
 // A domain layout on the device (DomainLayout in plan.hpp).
@@ -138,6 +150,9 @@ struct yb_factor {
   std::map<std::tuple<int, int, int, int, int, int>, std::unique_ptr<yb::DeviceStream>> streams;
   // domain layouts by shape (value bytes, warps, page bytes, cut); a null entry: the factor admits none
   std::map<std::tuple<int, int, int, int>, std::unique_ptr<yb::DeviceDomain>> domains;
+  // lane layouts by (value bytes, warps, page bytes); a null entry: the factor admits none
+  std::map<std::tuple<int, int, int>, std::unique_ptr<yb::DeviceLane>> lanes;
+  yb::DeviceArray<uint8_t> lane_work, lane_partial;  // the lane solve's work and partial arrays
   yb::DeviceArray<int32_t> error;  // the device error word (a bounded wait that ran out)
   long long *phase_clock = nullptr;  // diagnostics buffer of the caller's, or null
   yb::DeviceArray<double> scratch64;

@@ -1,0 +1,438 @@
+// The lane solve's layout (lane_solve.cuh): the factor's rows in one order that serves both sweeps,
+// cut into subtree domains that the warps of a block take in parallel under a top that one warp
+// takes, and each warp's part as a stream of records that every lane of the warp runs on its own
+// right-hand side.
+//
+// Order. The forest's parent of row c is the first row whose forward row reads c (for a Cholesky
+// factor, the elimination tree). A postorder visits each subtree whole, children with the larger
+// subtrees first, which keeps the values alive at any moment to a few tens for a power-network
+// factor: the forward accumulators of rows that have started to receive updates, and in the
+// backward sweep (the reverse order) the solutions that rows still to come will read.
+//
+// Cut. The subtrees whose work is at most a cap are the domains (the largest such subtrees); the
+// rows above them are the top. The domains go to the warps by work, largest first, and the cap is
+// the one whose estimate (the busiest warp's domains plus the top) is least. In the work array the
+// rows sit warp by warp, each warp's domains in postorder, then the top in postorder.
+//
+// Forward, right-looking: at row j, z_j = (b_j + acc_j) * dinv_j, acc_j read and zeroed, then for
+// every later row r that reads j, acc_r -= L_rj z_j. A domain's updates of top rows gather in its
+// warp's slots and go to the block's partial array when the domain ends (a flush); the top warp
+// adds a top row's partials, in a fixed order, before the row. Backward, left-looking, rows in
+// reverse order: x_j = (z_j - sum of U_jc x_c) * dinv_j, x_j kept in a slot while rows still to
+// come read it; a domain first imports the top solutions its rows read from the work array.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace yb {
+
+namespace {
+
+// Slot 0 is always zero (the accumulator of a row no update reaches), slot 1 takes solutions no
+// row reads; live values take the lowest free slot from 2 (interval colouring in visiting order:
+// exactly the peak of live values).
+struct Slots {
+  std::vector<uint8_t> used;
+  int32_t live = 0, peak = 0;
+  int32_t take() {
+    int32_t s = 0;
+    while (s < (int32_t)used.size() && used[s]) ++s;
+    if (s == (int32_t)used.size()) used.push_back(0);
+    used[s] = 1;
+    peak = std::max(peak, ++live);
+    return s + 2;
+  }
+  void give(int32_t s) {
+    used[s - 2] = 0;
+    --live;
+  }
+};
+
+// Writes one warp's records into fixed-size pages; a record never straddles a page, and a record
+// whose entries do not fit one page continues in the next records.
+template <class T> struct PageWriter {
+  static constexpr size_t kEntry = sizeof(T) == 8 ? 16 : 8;
+  int32_t page_bytes;
+  std::vector<uint8_t> &blob;
+  size_t pos = 0;
+  PageWriter(std::vector<uint8_t> &b, int32_t pb) : page_bytes(pb), blob(b) { open(); }
+  void open() {
+    blob.resize(blob.size() + page_bytes, 0);
+    pos = 0;
+  }
+  uint8_t *at() { return blob.data() + blob.size() - page_bytes + pos; }
+  void header(uint32_t self, uint32_t count, uint32_t kind, bool word, uint32_t w, T dinv) {
+    uint8_t *p = at();
+    const uint32_t h[2] = {self, count | kind << 16};
+    std::memcpy(p, h, 8);
+    if (word)
+      std::memcpy(p + 8, &w, 4);
+    else
+      std::memcpy(p + 8, &dinv, sizeof(T));
+  }
+  void room(size_t bytes) {
+    if (pos + bytes <= (size_t)page_bytes) return;
+    if (pos + 16 <= (size_t)page_bytes) header(0, 0, kLanePageEnd, true, 0, T(0));
+    open();
+  }
+  // A record with entries {val, or a 32-bit word in val's place; offset}, split over records of
+  // kinds (first, middle, last) when it does not fit a page, of kind `whole` when it does.
+  void record(uint32_t self, T dinv, const std::vector<std::pair<T, uint32_t>> &entries, const uint32_t *words,
+              uint32_t whole, uint32_t first, uint32_t middle, uint32_t last) {
+    const size_t per_page = (page_bytes - 16) / kEntry;
+    size_t done = 0;
+    do {
+      const size_t take = std::min(per_page, entries.size() - done);
+      const size_t bytes = 16 + ((take * kEntry + 15) & ~(size_t)15);
+      room(bytes);
+      const bool is_first = done == 0, is_last = done + take == entries.size();
+      const uint32_t kind = is_first && is_last ? whole : is_first ? first : is_last ? last : middle;
+      header(self, (uint32_t)take, kind, false, 0, dinv);
+      uint8_t *p = at();
+      for (size_t e = 0; e < take; ++e) {
+        uint8_t *q = p + 16 + e * kEntry;
+        if (words)
+          std::memcpy(q, &words[done + e], 4);
+        else
+          std::memcpy(q, &entries[done + e].first, sizeof(T));
+        std::memcpy(q + sizeof(T), &entries[done + e].second, 4);
+      }
+      pos += bytes;
+      done += take;
+    } while (done < entries.size());
+  }
+  void simple(uint32_t self, uint32_t kind, uint32_t word) {
+    room(16);
+    header(self, 0, kind, true, word, T(0));
+    pos += 16;
+  }
+};
+
+struct Cut {
+  std::vector<int32_t> roots;  // domain roots
+  std::vector<std::vector<int32_t>> warp_domains;
+  std::vector<uint8_t> is_top;
+  double cost = 0;
+};
+
+template <class V, class T>
+LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int32_t warps) {
+  const int32_t n = plan.n;
+  LaneLayout lay;
+  lay.page_bytes = page_bytes;
+  lay.value_bytes = (int32_t)sizeof(T);
+  lay.warps = warps;
+  struct Row {
+    int32_t p0 = 0, p1 = 0;
+    double dinv = 1;
+  };
+  std::vector<Row> frow(n), brow(n);
+  for (int32_t p = 0; p < n; ++p) {
+    frow[plan.fwd.row[p]] = {plan.fwd.ptr[p], plan.fwd.ptr[p + 1], (double)plan.fwd.dinv[p]};
+    brow[plan.bwd.row[p]] = {plan.bwd.ptr[p], plan.bwd.ptr[p + 1], (double)plan.bwd.dinv[p]};
+  }
+  // the forest, subtree sizes and the postorder with larger subtrees first
+  std::vector<int32_t> parent(n, -1);
+  for (int32_t r = 0; r < n; ++r)
+    for (int32_t q = frow[r].p0; q < frow[r].p1; ++q) {
+      const int32_t c = plan.fwd.col[q];
+      if (c >= r) throw host::Error(host::kInvalidArgument, "the forward sweep is not lower triangular");
+      if (parent[c] < 0 || r < parent[c]) parent[c] = r;
+    }
+  std::vector<int64_t> size(n, 1);
+  for (int32_t c = 0; c < n; ++c)
+    if (parent[c] >= 0) size[parent[c]] += size[c];
+  std::vector<int32_t> child_ptr(n + 2, 0), child(n);
+  for (int32_t c = 0; c < n; ++c) ++child_ptr[(parent[c] < 0 ? n : parent[c]) + 1];
+  for (int32_t i = 0; i <= n; ++i) child_ptr[i + 1] += child_ptr[i];
+  {
+    std::vector<int32_t> fill(child_ptr.begin(), child_ptr.end() - 1);
+    for (int32_t c = 0; c < n; ++c) child[fill[parent[c] < 0 ? n : parent[c]]++] = c;
+  }
+  for (int32_t v = 0; v <= n; ++v)
+    std::stable_sort(child.begin() + child_ptr[v], child.begin() + child_ptr[v + 1],
+                     [&](int32_t a, int32_t b) { return size[a] > size[b]; });
+  std::vector<int32_t> order;
+  order.reserve(n);
+  {
+    std::vector<std::pair<int32_t, int32_t>> stack{{n, child_ptr[n]}};
+    while (!stack.empty()) {
+      auto &top = stack.back();
+      const int32_t v = top.first;
+      if (top.second < child_ptr[v + 1]) {
+        const int32_t c = child[top.second++];
+        stack.push_back({c, child_ptr[c]});
+      } else {
+        if (v < n) order.push_back(v);
+        stack.pop_back();
+      }
+    }
+  }
+  std::vector<int32_t> pos(n);
+  for (int32_t t = 0; t < n; ++t) pos[order[t]] = t;
+  for (int32_t r = 0; r < n; ++r) {
+    for (int32_t q = frow[r].p0; q < frow[r].p1; ++q)
+      if (pos[plan.fwd.col[q]] >= pos[r]) throw host::Error(host::kInvalidArgument, "no postorder serves the forward sweep");
+    for (int32_t q = brow[r].p0; q < brow[r].p1; ++q)
+      if (pos[plan.bwd.col[q]] <= pos[r])
+        throw host::Error(host::kInvalidArgument, "the backward sweep does not run in the reverse postorder");
+  }
+  // forward columns: the rows each row updates
+  std::vector<int32_t> col_ptr(n + 1, 0), col_row;
+  std::vector<double> col_val;
+  for (int32_t r = 0; r < n; ++r)
+    for (int32_t q = frow[r].p0; q < frow[r].p1; ++q) ++col_ptr[plan.fwd.col[q] + 1];
+  for (int32_t c = 0; c < n; ++c) col_ptr[c + 1] += col_ptr[c];
+  col_row.resize(col_ptr[n]);
+  col_val.resize(col_ptr[n]);
+  {
+    std::vector<int32_t> fill(col_ptr.begin(), col_ptr.end() - 1);
+    for (int32_t r = 0; r < n; ++r)
+      for (int32_t q = frow[r].p0; q < frow[r].p1; ++q) {
+        const int32_t c = plan.fwd.col[q];
+        col_row[fill[c]] = r;
+        col_val[fill[c]++] = (double)plan.fwd.val[q];
+      }
+  }
+  // work of each row (both sweeps, in instruction-like units) and of each subtree
+  constexpr double kRowWork = 60, kEntryWork = 7;
+  std::vector<double> work(n), sub(n, 0.0);
+  for (int32_t v = 0; v < n; ++v)
+    work[v] = 2 * kRowWork + kEntryWork * ((col_ptr[v + 1] - col_ptr[v]) + (brow[v].p1 - brow[v].p0));
+  for (int32_t t = 0; t < n; ++t) {
+    const int32_t v = order[t];  // a postorder lists children first
+    sub[v] += work[v];
+    if (parent[v] >= 0) sub[parent[v]] += sub[v];
+  }
+  const double total = std::accumulate(work.begin(), work.end(), 0.0);
+  auto cut_at = [&](double cap) {
+    Cut c;
+    c.is_top.assign(n, 0);
+    double top_work = 0;
+    for (int32_t v = 0; v < n; ++v)
+      if (sub[v] > cap) c.is_top[v] = 1, top_work += work[v];
+    for (int32_t v = 0; v < n; ++v)
+      if (!c.is_top[v] && (parent[v] < 0 || c.is_top[parent[v]])) c.roots.push_back(v);
+    std::vector<int32_t> by_work(c.roots);
+    std::stable_sort(by_work.begin(), by_work.end(), [&](int32_t a, int32_t b) { return sub[a] > sub[b]; });
+    std::vector<double> load(warps, 0.0);
+    c.warp_domains.assign(warps, {});
+    for (int32_t r : by_work) {
+      const int32_t w = (int32_t)(std::min_element(load.begin(), load.end()) - load.begin());
+      load[w] += sub[r] + kRowWork;
+      c.warp_domains[w].push_back(r);
+    }
+    // each warp's domains in postorder, so its rows keep the whole postorder's order
+    for (auto &d : c.warp_domains) std::sort(d.begin(), d.end(), [&](int32_t a, int32_t b) { return pos[a] < pos[b]; });
+    c.cost = *std::max_element(load.begin(), load.end()) + top_work;
+    return c;
+  };
+  Cut best = cut_at(total + 1);  // one domain per tree of the forest, no top
+  if (warps > 1)
+    for (int k = 0; k <= 12; ++k) {
+      Cut c = cut_at(total / (warps * std::pow(2.0, k)));
+      if (c.cost < best.cost) best = std::move(c);
+    }
+  lay.cost = best.cost;
+  lay.domains = (int32_t)best.roots.size();
+  // the work array's order: warp by warp, each domain in postorder, then the top in postorder
+  std::vector<int32_t> newpos(n, -1), warp_start(warps + 1, 0);
+  std::vector<std::pair<int32_t, int32_t>> domain_range;  // first and last position of each domain
+  std::vector<std::vector<int32_t>> warp_dom_index(warps);
+  {
+    int32_t next = 0;
+    for (int32_t w = 0; w < warps; ++w) {
+      warp_start[w] = next;
+      for (int32_t r : best.warp_domains[w]) {
+        const int32_t first = pos[r] - (int32_t)size[r] + 1, d0 = next;
+        for (int32_t t = first; t <= pos[r]; ++t) newpos[order[t]] = next++;
+        warp_dom_index[w].push_back((int32_t)domain_range.size());
+        domain_range.push_back({d0, next - 1});
+      }
+    }
+    warp_start[warps] = next;
+    for (int32_t t = 0; t < n; ++t)
+      if (best.is_top[order[t]]) newpos[order[t]] = next++;
+    if (next != n) throw host::Error(host::kInternal, "the lane cut lost rows");
+  }
+  const int32_t top0 = warp_start[warps];
+  lay.top = n - top0;
+  std::vector<int32_t> at(n);
+  for (int32_t v = 0; v < n; ++v) at[newpos[v]] = v;
+  // partials: one per (domain, top row it updates), domains in warp order, top rows by position
+  std::vector<std::vector<uint32_t>> contributors(n);
+  std::vector<std::vector<std::pair<int32_t, uint32_t>>> domain_partials(domain_range.size());
+  {
+    uint32_t k = 0;
+    std::vector<int32_t> seen(n, -1);
+    for (size_t d = 0; d < domain_range.size(); ++d) {
+      std::vector<int32_t> tops;
+      for (int32_t p = domain_range[d].first; p <= domain_range[d].second; ++p) {
+        const int32_t j = at[p];
+        for (int32_t q = col_ptr[j]; q < col_ptr[j + 1]; ++q) {
+          const int32_t r = col_row[q];
+          if (best.is_top[r] && seen[r] != (int32_t)d) seen[r] = (int32_t)d, tops.push_back(r);
+        }
+      }
+      std::sort(tops.begin(), tops.end(), [&](int32_t a, int32_t b) { return newpos[a] < newpos[b]; });
+      for (int32_t r : tops) {
+        domain_partials[d].push_back({r, k});
+        contributors[r].push_back(k++);
+      }
+    }
+    lay.partials = (int32_t)k;
+  }
+  const uint32_t slot_bytes = 32u * (uint32_t)sizeof(T);
+  auto off = [&](int32_t s) { return (uint32_t)s * slot_bytes; };
+  std::vector<std::pair<T, uint32_t>> entries;
+  std::vector<uint32_t> words;
+  std::vector<int32_t> acc(n, -1), xslot(n, -1), readers(n, 0);
+  int32_t peak_f = 0, peak_b = 0;
+  auto forward_rows = [&](PageWriter<T> &pw, Slots &slots, int32_t p0, int32_t p1) {
+    for (int32_t p = p0; p <= p1; ++p) {
+      const int32_t j = at[p];
+      uint32_t self = off(0);
+      if (acc[j] >= 0) {
+        self = off(acc[j]);
+        slots.give(acc[j]);
+        acc[j] = -1;
+      }
+      entries.clear();
+      for (int32_t q = col_ptr[j]; q < col_ptr[j + 1]; ++q) {
+        const int32_t r = col_row[q];
+        if (acc[r] < 0) acc[r] = slots.take();
+        entries.push_back({(T)col_val[q], off(acc[r])});
+      }
+      lay.fwd_entries += (int64_t)entries.size();
+      pw.record(self, (T)frow[j].dinv, entries, nullptr, kLaneRow, kLaneRowBegin, kLaneRowMore, kLaneRowEnd);
+    }
+  };
+  // readers[c]: the rows still to come that read x_c
+  auto backward_rows = [&](PageWriter<T> &pw, Slots &slots, int32_t p0, int32_t p1) {
+    for (int32_t p = p1; p >= p0; --p) {
+      const int32_t j = at[p];
+      entries.clear();
+      for (int32_t q = brow[j].p0; q < brow[j].p1; ++q) entries.push_back({(T)plan.bwd.val[q], off(xslot[plan.bwd.col[q]])});
+      for (int32_t q = brow[j].p0; q < brow[j].p1; ++q) {
+        const int32_t c = plan.bwd.col[q];
+        if (--readers[c] == 0) {
+          slots.give(xslot[c]);
+          xslot[c] = -1;
+        }
+      }
+      uint32_t self = off(1);
+      if (readers[j] > 0) {
+        xslot[j] = slots.take();
+        self = off(xslot[j]);
+      }
+      lay.bwd_entries += (int64_t)entries.size();
+      pw.record(self, (T)brow[j].dinv, entries, nullptr, kLaneRow, kLaneRowBegin, kLaneRowMore, kLaneRowEnd);
+    }
+  };
+  lay.warp_page.assign(1, 0);
+  for (int32_t w = 0; w < warps; ++w) {
+    PageWriter<T> pw(lay.blob, page_bytes);
+    const int32_t p0 = warp_start[w], p1 = warp_start[w + 1] - 1;
+    {  // forward domains, each ending with its flush
+      Slots slots;
+      if (p1 >= p0) pw.simple((uint32_t)p0, kLanePhase, (uint32_t)(p1 - p0 + 1));
+      for (int32_t d : warp_dom_index[w]) {
+        forward_rows(pw, slots, domain_range[d].first, domain_range[d].second);
+        entries.clear();
+        words.clear();
+        for (auto [r, k] : domain_partials[d]) {
+          entries.push_back({T(0), off(acc[r])});
+          words.push_back(k);
+          slots.give(acc[r]);
+          acc[r] = -1;
+        }
+        if (!entries.empty()) pw.record(0, T(0), entries, words.data(), kLaneFlush, kLaneFlush, kLaneFlush, kLaneFlush);
+      }
+      peak_f = std::max(peak_f, slots.peak);
+    }
+    pw.simple(0, kLaneBarrier, 0);
+    if (w == 0 && top0 < n) {  // the top, forward then backward
+      Slots slots;
+      pw.simple((uint32_t)top0, kLanePhase, (uint32_t)(n - top0));
+      for (int32_t p = top0; p < n; ++p) {
+        const int32_t j = at[p];
+        if (!contributors[j].empty()) {
+          if (acc[j] < 0) acc[j] = slots.take();
+          entries.assign(contributors[j].size(), {T(0), 0u});
+          pw.record(off(acc[j]), T(0), entries, contributors[j].data(), kLanePartials, kLanePartials, kLanePartials,
+                    kLanePartials);
+        }
+        forward_rows(pw, slots, p, p);
+      }
+      peak_f = std::max(peak_f, slots.peak);
+      Slots bslots;
+      for (int32_t p = top0; p < n; ++p)
+        for (int32_t q = brow[at[p]].p0; q < brow[at[p]].p1; ++q) ++readers[plan.bwd.col[q]];
+      pw.simple((uint32_t)(n - 1), kLanePhase | kLaneBackward, (uint32_t)(n - top0));
+      backward_rows(pw, bslots, top0, n - 1);
+      peak_b = std::max(peak_b, bslots.peak);
+    }
+    pw.simple(0, kLaneBarrier, 0);
+    {  // backward domains in reverse, each starting with the top solutions it reads
+      Slots slots;
+      if (p1 >= p0) pw.simple((uint32_t)p1, kLanePhase | kLaneBackward, (uint32_t)(p1 - p0 + 1));
+      const auto &doms = warp_dom_index[w];
+      for (auto it = doms.rbegin(); it != doms.rend(); ++it) {
+        const int32_t d0 = domain_range[*it].first, d1 = domain_range[*it].second;
+        std::vector<int32_t> imports;
+        for (int32_t p = d0; p <= d1; ++p)
+          for (int32_t q = brow[at[p]].p0; q < brow[at[p]].p1; ++q) {
+            const int32_t c = plan.bwd.col[q];
+            if (readers[c]++ == 0 && best.is_top[c]) imports.push_back(c);
+          }
+        if (!imports.empty()) {
+          std::sort(imports.begin(), imports.end(), [&](int32_t a, int32_t b) { return newpos[a] < newpos[b]; });
+          entries.clear();
+          words.clear();
+          for (int32_t c : imports) {
+            xslot[c] = slots.take();
+            entries.push_back({T(0), off(xslot[c])});
+            words.push_back((uint32_t)newpos[c]);
+          }
+          pw.record(0, T(0), entries, words.data(), kLaneImport, kLaneImport, kLaneImport, kLaneImport);
+        }
+        backward_rows(pw, slots, d0, d1);
+      }
+      peak_b = std::max(peak_b, slots.peak);
+    }
+    pw.simple(0, kLaneEnd, 0);
+    lay.warp_page.push_back((int32_t)(lay.blob.size() / page_bytes));
+  }
+  lay.fwd_live = peak_f;
+  lay.bwd_live = peak_b;
+  lay.slots = 2 + std::max(peak_f, peak_b);
+  if (lay.slots > max_slots)
+    throw host::Error(host::kTooLarge, "the lane solve would keep more live values than its shared memory holds");
+  lay.in_pos.resize(n);
+  lay.out_pos.resize(n);
+  for (int32_t i = 0; i < n; ++i) {
+    lay.in_pos[i] = newpos[plan.in_slot[i]];
+    lay.out_pos[i] = newpos[plan.out_slot[i]];
+  }
+  return lay;
+}
+
+}  // namespace
+
+template <class T>
+LaneLayout lane_layout(const Plan<T> &plan, int32_t value_bytes, int32_t page_bytes, int32_t max_slots, int32_t warps) {
+  if (page_bytes < 256 || page_bytes % 16)
+    throw host::Error(host::kInvalidArgument, "pages must be 16-byte multiples of at least 256 bytes");
+  if (warps < 1 || warps > 32) throw host::Error(host::kInvalidArgument, "1 to 32 warps per block");
+  if (value_bytes == 8) return build<T, double>(plan, page_bytes, max_slots, warps);
+  if (value_bytes == 4) return build<T, float>(plan, page_bytes, max_slots, warps);
+  throw host::Error(host::kInvalidArgument, "values must be 8 or 4 bytes");
+}
+
+template LaneLayout lane_layout(const Plan<double> &, int32_t, int32_t, int32_t, int32_t);
+
+}  // namespace yb

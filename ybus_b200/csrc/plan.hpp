@@ -139,6 +139,51 @@ struct DomainLayout {
 template <class T>
 DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t warps, int32_t page_bytes, int32_t K);
 
+// The factor for the lane solve (lane_solve.cuh: one right-hand side per lane, every lane of a warp
+// taking the same rows, `warps` warps per block of 32 right-hand sides). The rows are in a
+// postorder of the forward elimination forest with larger subtrees first, cut into subtree domains
+// (dealt to the warps) under a top (taken by warp 0 between two block barriers); each warp's part
+// is one stream of records in fixed-size pages. A record: uint32 self, uint32 count | kind << 16,
+// then at byte 8 either T dinv or a 32-bit word, then `count` entries {T val (or a 32-bit word in
+// its place), uint32 offset} of 16 bytes (FP64) or 8 bytes (FP32). Offsets and `self` are byte
+// offsets of 32-value live slots; slot 0 is always zero, slot 1 a sink. Kinds:
+//   kLanePhase (self = first position, word = rows; | kLaneBackward for a backward phase): the next
+//     rows take the work array's positions from self upwards (forward) or downwards (backward).
+//   kLaneRow, split over records as kLaneRowBegin, kLaneRowMore..., kLaneRowEnd: forward, read and
+//     zero acc at self, z = (b + acc) * dinv into the work row, then acc[offset] -= val * z per
+//     entry; backward, acc = z from the work row minus val * x[offset] per entry, x = acc * dinv
+//     into the work row and into slot self.
+//   kLaneFlush: per entry, the partial array's value `word` takes slot `offset`, which is zeroed.
+//   kLanePartials: slot self += the partial array's values `word` of its entries, in order.
+//   kLaneImport: per entry, slot `offset` takes the work row at position `word`.
+//   kLaneBarrier: a block barrier (every warp's stream has two). kLaneEnd ends the stream;
+//   kLanePageEnd ends its page.
+enum LaneKind : uint32_t {
+  kLaneRow = 0,
+  kLaneRowBegin = 1,
+  kLaneRowMore = 2,
+  kLaneRowEnd = 3,
+  kLanePhase = 4,
+  kLanePartials = 5,
+  kLaneFlush = 6,
+  kLaneImport = 7,
+  kLaneBarrier = 8,
+  kLaneEnd = 9,
+  kLanePageEnd = 10,
+  kLaneBackward = 0x100
+};
+struct LaneLayout {
+  int32_t warps = 1, slots = 0, page_bytes = 0, value_bytes = 0;
+  int32_t domains = 0, top = 0, partials = 0;  // partials: partial-array values per block
+  int32_t fwd_live = 0, bwd_live = 0;          // the peak number of live values in each sweep
+  int64_t fwd_entries = 0, bwd_entries = 0;
+  double cost = 0;                             // the cut's estimate of a block's time (work units)
+  std::vector<uint8_t> blob;                   // every warp's pages
+  std::vector<int32_t> warp_page;              // [warps + 1] page ranges
+  std::vector<int32_t> in_pos;                 // [n] by row of b: its position in the work array
+  std::vector<int32_t> out_pos;                // [n] by row of x: its position
+};
+
 template <class T> struct Plan {
   int32_t n = 0;
   std::vector<int32_t> in_slot, out_slot;   // [n]
@@ -153,5 +198,11 @@ template <class T>
 Plan<T> build_plan(int64_t n, const host::Compressed<T> &lower, bool unit_lower,
                    const host::Compressed<T> &upper, const std::vector<int64_t> &in_perm,
                    const std::vector<int64_t> &out_perm);
+
+// Builds the lane layout of `plan` for values of `value_bytes` (8 or 4) and `warps` warps per block.
+// Throws host::Error (kInvalidArgument) when no postorder serves both sweeps, or (kTooLarge) when
+// more than `max_slots` slots would be needed.
+template <class T>
+LaneLayout lane_layout(const Plan<T> &plan, int32_t value_bytes, int32_t page_bytes, int32_t max_slots, int32_t warps);
 
 }  // namespace yb

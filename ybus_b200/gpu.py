@@ -237,6 +237,23 @@ class GpuFactor:
         return {"tile": w.value, "cut": cut.value, "top": top.value, "records": rec.value, "bytes": by.value,
                 "smem": sm.value, "model_cycles": cyc.value}
 
+    def lane_info(self, precision: int = FP64) -> dict:
+        """The lane solve's layout: slots, pages, peaks of live values, shared memory per block,
+        warps per block, domains, top rows and partial values per block."""
+        v = np.zeros(12, np.int64)
+        _check(lib().yb_factor_lane_info(self._h, precision, ptr(v)))
+        keys = ("slots", "pages", "page_bytes", "fwd_live", "bwd_live", "entries", "smem", "warps", "domains", "top",
+                "partials")
+        return dict(zip(keys, (int(a) for a in v)))
+
+    def set_lane(self, precision: int, warps: int, page_bytes: int = 2048) -> None:
+        """The lane solve's warps per block (1..8) and page bytes."""
+        _check(lib().yb_factor_set_lane(self._h, precision, warps, page_bytes))
+
+    def set_lane_min_count(self, precision: int, min_count: int) -> None:
+        """The number of right-hand sides from which the automatic choice takes the lane solve."""
+        _check(lib().yb_factor_set_lane_min_count(self._h, precision, min_count))
+
     def autotune(self, precision: int = FP64, count: int = 2048) -> dict:
         """Times the domain solve's shapes on `count` right-hand sides and keeps the fastest."""
         cfg = np.zeros(5, np.int32)
