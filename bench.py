@@ -35,6 +35,7 @@ WORKLOAD = "10k-bus PTDF block: B' 9,999 x 9,999 AMD Cholesky, 13,499 branch RHS
 N_BUS, EXTRA = 10000, 3500
 FALLBACK_HBM_GBS = 6650.0
 IR_TOLERANCE, IR_MAX_STEPS = 1e-10, 3
+LANE_MIN_COUNT, LANE_AUTO_SLOTS = 8192, 64  # the library's automatic choice of the lane solve
 
 
 def parse():
@@ -259,6 +260,24 @@ def main():
             elapsed_ms = float(t.item())
         return elapsed_ms, launch_ms
 
+    # which solve each mode runs: the plain FP64 solve takes the lane solve from the lane threshold
+    # on (three launches: gather, solve, scatter), else the domain solve; the refined solve is the
+    # domain solve with its refinement fused (one launch)
+    lane = None
+    try:
+        lane = factor.lane_info(FP64)
+    except Exception:
+        pass
+    use_lane = lane is not None and count >= LANE_MIN_COUNT and lane["slots"] <= LANE_AUTO_SLOTS
+
+    def solver_of(mode):
+        if mode == "fp64" and use_lane:
+            return {"solver": "lane", "kernel": "lane_solve_kernel<double>", "launches_per_step": 3,
+                    "lane": {k: lane[k] for k in ("warps", "slots", "domains", "top", "pages", "smem")}}
+        prec = FP64 if mode == "fp64" else FP32
+        return {"solver": "domain", "kernel": "domain_tile_kernel", "launches_per_step": 1,
+                "tile": factor.domain_info(prec)["tile"]}
+
     from oracle import oracle as orc  # the checker, outside the timed regions
     p, i, v = bp.arrays()
     sample = np.arange(0, count, max(1, count // 64))
@@ -282,7 +301,7 @@ def main():
             r["algorithmic_bytes_per_launch"] = algorithmic_bytes(n, count, info, "fp32_ir", float(steps.mean()), len(i))
         else:
             r["algorithmic_bytes_per_launch"] = algorithmic_bytes(n, count, info, "fp64")
-        r["tile"] = factor.domain_info(FP64 if mode == "fp64" else FP32)["tile"]
+        r.update(solver_of(mode))
         results[mode] = r
     clock_info = clocks.stop()
 
@@ -301,15 +320,15 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "rhs_per_step": count, "n": n, "mode": mode,
                        "nnz_factor_per_sweep": info["fwd_entries"] + n, "levels": [info["fwd_levels"], info["bwd_levels"]],
-                       "tile": best["tile"], "flush": "inputs (1.08 GB) > L2", "parallelism": f"replicas x{world}"},
+                       "solver": best["solver"], "flush": "inputs (1.08 GB) > L2", "parallelism": f"replicas x{world}"},
             "accuracy": {"max_rel_residual": best["max_rel_residual"], "max_rel_err_vs_oracle": best["max_rel_err_vs_oracle"]},
             "modes": results,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_source": peak_kind, "kernel": "domain_tile_kernel",
+                         "traffic": None, "peak_source": peak_kind, "kernel": best["kernel"],
                          "algorithmic_bytes_per_launch": best["algorithmic_bytes_per_launch"],
                          "launch_ms": best["launch_ms"], "compulsory_gbs": compulsory,
                          "compulsory_frac": compulsory / peak},
-            "clocks": clock_info, "gpu_launches": a.steps * len(modes)}
+            "clocks": clock_info, "gpu_launches": a.steps * sum(results[m]["launches_per_step"] for m in modes)}
 
     if not a.no_e2e:
         # every rank through the host-array call on its own GPU; the step time is the max over ranks

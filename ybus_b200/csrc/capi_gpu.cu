@@ -787,7 +787,13 @@ void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t
   auto run = [&](auto zero, const TileConfig &configured, auto &fwd, auto &bwd, auto &scratch, auto &cache) {
     using T = decltype(zero);
     if (configured.kind == kTileLane || (configured.kind == kTileAuto && count >= configured.lane_min_count)) {
-      DeviceLane *d = lane_for<T>(f, configured.lane_warps, configured.lane_page, stream);
+      // the configured warps per block, or fewer when the block's slots do not fit shared memory
+      DeviceLane *d = nullptr;
+      for (int warps = configured.lane_warps; warps >= 1; --warps) {
+        d = lane_for<T>(f, warps, configured.lane_page, stream);
+        if (!d || lane_smem<T>(d) <= (size_t)f->gpu->smem_optin) break;
+      }
+      if (d && lane_smem<T>(d) > (size_t)f->gpu->smem_optin) d = nullptr;
       if (d && (configured.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane<T>(f, d, b, ldb, x, ldx, count, stream);
         return;
