@@ -1,14 +1,17 @@
 """A host interpreter of the lane solve's records (the semantics of lane_solve.cuh), for checking
-layouts on the CPU: every right-hand side is one lane, each warp's live slots a (slots, lanes)
-array, the warps run between block barriers one after another."""
+layouts on the CPU: every right-hand side is one lane, each warp's live slots and prefetch ring
+(slots, lanes) arrays, the warps run between block barriers one after another. It also checks that
+every row is read from its ring slot after its prefetch and before the slot is refilled."""
 import numpy as np
 
-ROW, ROW_BEGIN, ROW_MORE, ROW_END, PHASE, PARTIALS, FLUSH, IMPORT, BARRIER, END, PAGE_END = range(11)
-BACKWARD = 0x100
+FWD_ROW0, FWD_ROWN, FWD_MORE = 0, 5, 6
+BWD_ROW0, BWD_ROWN, BWD_BEGIN, BWD_MORE, BWD_END = 7, 12, 13, 14, 15
+PREFETCH, PHASE, PARTIALS, FLUSH, IMPORT, BARRIER, END, PAGE_END = range(16, 24)
+RING, BATCH = 8, 4
 
 
 def records(lay, warp):
-    """Yields (kind, self, count, head_word, dinv, vals, words, offsets) for each record of a warp."""
+    """Yields (kind, ring, self, count, word, tail, vals, words, offsets) for each record of a warp."""
     pb, vb = lay["page_bytes"], lay["value_bytes"]
     ftype = np.float64 if vb == 8 else np.float32
     entry = 16 if vb == 8 else 8
@@ -16,18 +19,20 @@ def records(lay, warp):
     for k in range(lay["warp_page"][warp], lay["warp_page"][warp + 1]):
         page = blob[k * pb:(k + 1) * pb]
         pos = 0
-        while pos + 16 <= pb:
-            self_, word = (int(v) for v in page[pos:pos + 8].view(np.uint32))
-            kind, count = word >> 16, word & 0xFFFF
+        while True:
+            assert pos + 16 <= pb, "a page without its end record"
+            head, word = (int(v) for v in page[pos:pos + 8].view(np.uint32))
+            self_, kb, count = head & 0xFFFF, (head >> 16) & 0xFF, head >> 24
+            kind, ring = kb & 31, kb >> 5
             if kind == PAGE_END:
                 break
-            head_word = int(page[pos + 8:pos + 12].view(np.uint32)[0])
-            dinv = float(page[pos + 8:pos + 8 + vb].view(ftype)[0])
+            tail = page[pos + 8:pos + 16]
             body = page[pos + 16:pos + 16 + count * entry]
+            assert pos + 16 + count * entry <= pb, "a record past its page"
             vals = np.array([body[e * entry:e * entry + vb].view(ftype)[0] for e in range(count)], np.float64)
             words = np.array([body[e * entry:e * entry + 4].view(np.uint32)[0] for e in range(count)], np.int64)
             offs = np.array([body[e * entry + vb:e * entry + vb + 4].view(np.uint32)[0] for e in range(count)], np.int64)
-            yield kind, self_, count, head_word, dinv, vals, words, offs
+            yield kind, ring, self_, count, word, tail, vals, words, offs
             if kind == END:
                 return
             pos += 16 + ((count * entry + 15) & ~15)
@@ -35,50 +40,63 @@ def records(lay, warp):
 
 def warp_steps(lay, warp, work, partial, lanes):
     """Runs one warp's records, yielding at each block barrier."""
-    slot_bytes = 32 * lay["value_bytes"]
+    vb = lay["value_bytes"]
+    ftype = np.float64 if vb == 8 else np.float32
+    row = 32 * vb
     live = np.zeros((lay["slots"], lanes))
-    start = i = 0
-    backward = False
+    ring = np.full((RING, lanes), np.nan)
+    pending = np.zeros(RING, bool)  # a prefetched row not read yet
     z = None
-    cur = 0
-
-    def next_row():
-        nonlocal i, cur
-        cur = start - i if backward else start + i
-        i += 1
-        return work[cur].copy()
-
-    for kind, self_, count, head_word, dinv, vals, words, offs in records(lay, warp):
-        s = self_ // slot_bytes
-        if kind <= ROW_END:
-            if not backward:
-                if kind <= ROW_BEGIN:
-                    z = (next_row() + live[s]) * dinv
-                    live[s] = 0.0
-                    work[cur] = z
-                for v, o in zip(vals, offs):
-                    live[o // slot_bytes] -= v * z
-            else:
-                if kind <= ROW_BEGIN:
-                    z = next_row()
-                for v, o in zip(vals, offs):
-                    z = z - v * live[o // slot_bytes]
-                if kind in (ROW, ROW_END):
-                    x = z * dinv
-                    live[s] = x
-                    work[cur] = x
-        elif kind & 0xFF == PHASE:
-            start, i, backward = self_, 0, bool(kind & BACKWARD)
+    for kind, rs, self_, count, word, tail, vals, words, offs in records(lay, warp):
+        s, w = self_ * 16 // row, word // row
+        if kind <= BWD_END:
+            dinv = float(tail[:vb].view(ftype)[0])
+            assert 0 <= w < work.shape[0], "a row outside the work array"
+        if FWD_ROW0 <= kind <= FWD_ROWN:
+            assert pending[rs], "a row read before its prefetch"
+            pending[rs] = False
+            z = (ring[rs] + live[s]) * dinv
+            live[s] = 0.0
+            work[w] = z
+        if FWD_ROW0 <= kind <= FWD_MORE:
+            if FWD_ROW0 <= kind < FWD_ROWN:
+                assert count == kind - FWD_ROW0
+            for v, o in zip(vals, offs):
+                live[o // row] -= v * z
+        elif BWD_ROW0 <= kind <= BWD_END:
+            if BWD_ROW0 <= kind < BWD_ROWN:
+                assert count == kind - BWD_ROW0
+            if kind <= BWD_BEGIN:
+                assert pending[rs], "a row read before its prefetch"
+                pending[rs] = False
+                z = ring[rs].copy()
+            for v, o in zip(vals, offs):
+                z = z - v * live[o // row]
+            if kind < BWD_BEGIN or kind == BWD_END:
+                x = z * dinv
+                live[s] = x
+                work[w] = x
+        elif kind == PREFETCH:
+            flags = int(tail[:4].view(np.uint32)[0])
+            step, base = (-1 if flags & 1 else 1), (BATCH if flags & 2 else 0)
+            for q in range(self_):
+                assert not pending[base + q], "a prefetch over a row not read yet"
+                assert 0 <= w + q * step < work.shape[0], "a prefetch outside the work array"
+                ring[base + q] = work[w + q * step]
+                pending[base + q] = True
+        elif kind == PHASE:
+            assert not pending.any(), "a phase that leaves prefetched rows unread"
+            ring[:] = np.nan
         elif kind == PARTIALS:
             for k in words:
-                live[s] = live[s] + partial[k]
+                live[s] = live[s] + partial[k // row]
         elif kind == FLUSH:
             for k, o in zip(words, offs):
-                partial[k] = live[o // slot_bytes]
-                live[o // slot_bytes] = 0.0
+                partial[k // row] = live[o // row]
+                live[o // row] = 0.0
         elif kind == IMPORT:
             for p, o in zip(words, offs):
-                live[o // slot_bytes] = work[p]
+                live[o // row] = work[p // row]
         elif kind == BARRIER:
             yield
         elif kind == END:

@@ -52,63 +52,112 @@ struct Slots {
   }
 };
 
-// Writes one warp's records into fixed-size pages; a record never straddles a page, and a record
-// whose entries do not fit one page continues in the next records.
+// Writes one warp's records into fixed-size pages. Every page ends with a kLanePageEnd record (room
+// for it is always kept); a record never straddles a page, and a record whose entries do not fit one
+// page continues in the next records. The writer follows the phase (first position, direction and
+// length) so that each row record carries its work-row offset and prefetch-ring slot, and puts a
+// kLanePrefetch record before every kLaneBatch rows.
 template <class T> struct PageWriter {
-  static constexpr size_t kEntry = sizeof(T) == 8 ? 16 : 8;
+  static constexpr uint32_t kEntry = sizeof(T) == 8 ? 16 : 8, kRow = 32 * sizeof(T);
   int32_t page_bytes;
   std::vector<uint8_t> &blob;
   size_t pos = 0;
+  int32_t start = 0, len = 0, step = 1, row_i = 0;
   PageWriter(std::vector<uint8_t> &b, int32_t pb) : page_bytes(pb), blob(b) { open(); }
   void open() {
     blob.resize(blob.size() + page_bytes, 0);
     pos = 0;
   }
   uint8_t *at() { return blob.data() + blob.size() - page_bytes + pos; }
-  void header(uint32_t self, uint32_t count, uint32_t kind, bool word, uint32_t w, T dinv) {
+  void put(uint32_t self, uint32_t kind, uint32_t count, uint32_t word, const void *tail, size_t tail_bytes) {
     uint8_t *p = at();
-    const uint32_t h[2] = {self, count | kind << 16};
+    const uint32_t h[2] = {self | kind << 16 | count << 24, word};
     std::memcpy(p, h, 8);
-    if (word)
-      std::memcpy(p + 8, &w, 4);
-    else
-      std::memcpy(p + 8, &dinv, sizeof(T));
+    if (tail_bytes) std::memcpy(p + 8, tail, tail_bytes);
   }
   void room(size_t bytes) {
-    if (pos + bytes <= (size_t)page_bytes) return;
-    if (pos + 16 <= (size_t)page_bytes) header(0, 0, kLanePageEnd, true, 0, T(0));
+    if (pos + bytes + 16 <= (size_t)page_bytes) return;
+    put(0, kLanePageEnd, 0, 0, nullptr, 0);
     open();
   }
-  // A record with entries {val, or a 32-bit word in val's place; offset}, split over records of
-  // kinds (first, middle, last) when it does not fit a page, of kind `whole` when it does.
-  void record(uint32_t self, T dinv, const std::vector<std::pair<T, uint32_t>> &entries, const uint32_t *words,
-              uint32_t whole, uint32_t first, uint32_t middle, uint32_t last) {
-    const size_t per_page = (page_bytes - 16) / kEntry;
-    size_t done = 0;
-    do {
-      const size_t take = std::min(per_page, entries.size() - done);
-      const size_t bytes = 16 + ((take * kEntry + 15) & ~(size_t)15);
-      room(bytes);
-      const bool is_first = done == 0, is_last = done + take == entries.size();
-      const uint32_t kind = is_first && is_last ? whole : is_first ? first : is_last ? last : middle;
-      header(self, (uint32_t)take, kind, false, 0, dinv);
-      uint8_t *p = at();
-      for (size_t e = 0; e < take; ++e) {
-        uint8_t *q = p + 16 + e * kEntry;
-        if (words)
-          std::memcpy(q, &words[done + e], 4);
-        else
-          std::memcpy(q, &entries[done + e].first, sizeof(T));
-        std::memcpy(q + sizeof(T), &entries[done + e].second, 4);
-      }
-      pos += bytes;
-      done += take;
-    } while (done < entries.size());
+  size_t most_entries() const { return std::min<size_t>(255, (page_bytes - 32) / kEntry); }
+  static size_t bytes_of(size_t count) { return 16 + ((count * kEntry + 15) & ~(size_t)15); }
+  void entries_at(uint8_t *p, const std::vector<std::pair<T, uint32_t>> &entries, const uint32_t *words, size_t from,
+                  size_t take) {
+    for (size_t e = 0; e < take; ++e) {
+      uint8_t *q = p + 16 + e * kEntry;
+      if (words)
+        std::memcpy(q, &words[from + e], 4);
+      else
+        std::memcpy(q, &entries[from + e].first, sizeof(T));
+      std::memcpy(q + sizeof(T), &entries[from + e].second, 4);
+    }
   }
-  void simple(uint32_t self, uint32_t kind, uint32_t word) {
+  void simple(uint32_t kind) {
     room(16);
-    header(self, 0, kind, true, word, T(0));
+    put(0, kind, 0, 0, nullptr, 0);
     pos += 16;
+  }
+  void prefetch(int32_t batch) {
+    const int32_t r0 = batch * kLaneBatch;
+    const int32_t count = std::max(0, std::min(kLaneBatch, len - r0));
+    const uint32_t first = count > 0 ? (uint32_t)(start + step * r0) * kRow : 0;
+    const uint32_t flags = (step < 0 ? 1u : 0u) | ((r0 & (kLaneRows - 1)) ? 2u : 0u);
+    room(16);
+    put((uint32_t)count, kLanePrefetch, 0, first, &flags, 4);
+    pos += 16;
+  }
+  void phase(int32_t first, int32_t rows, bool backward) {
+    simple(kLanePhase);
+    start = first, len = rows, step = backward ? -1 : 1, row_i = 0;
+    prefetch(0);
+    prefetch(1);
+  }
+  // Records with entries {a 32-bit word in val's place, offset}, split as the pages need.
+  void words(uint32_t kind, uint32_t self, const std::vector<std::pair<T, uint32_t>> &entries,
+             const std::vector<uint32_t> &w) {
+    size_t done = 0;
+    while (done < entries.size()) {
+      const size_t take = std::min(most_entries(), entries.size() - done);
+      room(bytes_of(take));
+      put(self, kind, (uint32_t)take, 0, nullptr, 0);
+      entries_at(at(), entries, w.data(), done, take);
+      pos += bytes_of(take);
+      done += take;
+    }
+  }
+  // One row of the phase: its records carry its work-row offset, its ring slot and its diagonal's
+  // reciprocal; rows of up to 4 entries take the kinds for their exact count.
+  void row(uint32_t self, T dinv, const std::vector<std::pair<T, uint32_t>> &entries, bool backward) {
+    if (row_i % kLaneBatch == 0 && row_i > 0) prefetch(row_i / kLaneBatch + 1);
+    const uint32_t ring = (uint32_t)(row_i & (kLaneRows - 1)) << 5;
+    const uint32_t wpos = (uint32_t)(start + step * row_i) * kRow;
+    ++row_i;
+    const size_t count = entries.size();
+    uint8_t tail[8] = {};
+    std::memcpy(tail, &dinv, sizeof(T));
+    if (count <= 4) {
+      room(bytes_of(count));
+      put(self, (backward ? kLaneBwdRow0 : kLaneFwdRow0) + (uint32_t)count + ring, (uint32_t)count, wpos, tail, 8);
+      entries_at(at(), entries, nullptr, 0, count);
+      pos += bytes_of(count);
+      return;
+    }
+    size_t done = 0;
+    while (done < count) {
+      const size_t take = std::min(most_entries(), count - done);
+      const bool first = done == 0, last = done + take == count;
+      uint32_t kind;
+      if (!backward)
+        kind = first ? kLaneFwdRowN : kLaneFwdMore;
+      else
+        kind = first && last ? kLaneBwdRowN : first ? kLaneBwdBegin : last ? kLaneBwdEnd : kLaneBwdMore;
+      room(bytes_of(take));
+      put(self, kind + ring, (uint32_t)take, wpos, tail, 8);
+      entries_at(at(), entries, nullptr, done, take);
+      pos += bytes_of(take);
+      done += take;
+    }
   }
 };
 
@@ -286,8 +335,9 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
     }
     lay.partials = (int32_t)k;
   }
-  const uint32_t slot_bytes = 32u * (uint32_t)sizeof(T);
-  auto off = [&](int32_t s) { return (uint32_t)s * slot_bytes; };
+  const uint32_t row_bytes = 32u * (uint32_t)sizeof(T);  // a live slot, or a work or partial row
+  auto off = [&](int32_t s) { return (uint32_t)s * row_bytes; };
+  auto self_of = [&](int32_t s) { return (uint32_t)s * row_bytes / 16; };  // headers hold slot offsets / 16
   std::vector<std::pair<T, uint32_t>> entries;
   std::vector<uint32_t> words;
   std::vector<int32_t> acc(n, -1), xslot(n, -1), readers(n, 0);
@@ -295,9 +345,9 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   auto forward_rows = [&](PageWriter<T> &pw, Slots &slots, int32_t p0, int32_t p1) {
     for (int32_t p = p0; p <= p1; ++p) {
       const int32_t j = at[p];
-      uint32_t self = off(0);
+      uint32_t self = self_of(0);
       if (acc[j] >= 0) {
-        self = off(acc[j]);
+        self = self_of(acc[j]);
         slots.give(acc[j]);
         acc[j] = -1;
       }
@@ -308,7 +358,7 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
         entries.push_back({(T)col_val[q], off(acc[r])});
       }
       lay.fwd_entries += (int64_t)entries.size();
-      pw.record(self, (T)frow[j].dinv, entries, nullptr, kLaneRow, kLaneRowBegin, kLaneRowMore, kLaneRowEnd);
+      pw.row(self, (T)frow[j].dinv, entries, false);
     }
   };
   // readers[c]: the rows still to come that read x_c
@@ -324,13 +374,13 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
           xslot[c] = -1;
         }
       }
-      uint32_t self = off(1);
+      uint32_t self = self_of(1);
       if (readers[j] > 0) {
         xslot[j] = slots.take();
-        self = off(xslot[j]);
+        self = self_of(xslot[j]);
       }
       lay.bwd_entries += (int64_t)entries.size();
-      pw.record(self, (T)brow[j].dinv, entries, nullptr, kLaneRow, kLaneRowBegin, kLaneRowMore, kLaneRowEnd);
+      pw.row(self, (T)brow[j].dinv, entries, true);
     }
   };
   lay.warp_page.assign(1, 0);
@@ -339,32 +389,33 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
     const int32_t p0 = warp_start[w], p1 = warp_start[w + 1] - 1;
     {  // forward domains, each ending with its flush
       Slots slots;
-      if (p1 >= p0) pw.simple((uint32_t)p0, kLanePhase, (uint32_t)(p1 - p0 + 1));
+      if (p1 >= p0) pw.phase(p0, p1 - p0 + 1, false);
       for (int32_t d : warp_dom_index[w]) {
         forward_rows(pw, slots, domain_range[d].first, domain_range[d].second);
         entries.clear();
         words.clear();
         for (auto [r, k] : domain_partials[d]) {
           entries.push_back({T(0), off(acc[r])});
-          words.push_back(k);
+          words.push_back(k * row_bytes);
           slots.give(acc[r]);
           acc[r] = -1;
         }
-        if (!entries.empty()) pw.record(0, T(0), entries, words.data(), kLaneFlush, kLaneFlush, kLaneFlush, kLaneFlush);
+        pw.words(kLaneFlush, 0, entries, words);
       }
       peak_f = std::max(peak_f, slots.peak);
     }
-    pw.simple(0, kLaneBarrier, 0);
+    pw.simple(kLaneBarrier);
     if (w == 0 && top0 < n) {  // the top, forward then backward
       Slots slots;
-      pw.simple((uint32_t)top0, kLanePhase, (uint32_t)(n - top0));
+      pw.phase(top0, n - top0, false);
       for (int32_t p = top0; p < n; ++p) {
         const int32_t j = at[p];
         if (!contributors[j].empty()) {
           if (acc[j] < 0) acc[j] = slots.take();
           entries.assign(contributors[j].size(), {T(0), 0u});
-          pw.record(off(acc[j]), T(0), entries, contributors[j].data(), kLanePartials, kLanePartials, kLanePartials,
-                    kLanePartials);
+          words.clear();
+          for (uint32_t k : contributors[j]) words.push_back(k * row_bytes);
+          pw.words(kLanePartials, self_of(acc[j]), entries, words);
         }
         forward_rows(pw, slots, p, p);
       }
@@ -372,14 +423,14 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
       Slots bslots;
       for (int32_t p = top0; p < n; ++p)
         for (int32_t q = brow[at[p]].p0; q < brow[at[p]].p1; ++q) ++readers[plan.bwd.col[q]];
-      pw.simple((uint32_t)(n - 1), kLanePhase | kLaneBackward, (uint32_t)(n - top0));
+      pw.phase(n - 1, n - top0, true);
       backward_rows(pw, bslots, top0, n - 1);
       peak_b = std::max(peak_b, bslots.peak);
     }
-    pw.simple(0, kLaneBarrier, 0);
+    pw.simple(kLaneBarrier);
     {  // backward domains in reverse, each starting with the top solutions it reads
       Slots slots;
-      if (p1 >= p0) pw.simple((uint32_t)p1, kLanePhase | kLaneBackward, (uint32_t)(p1 - p0 + 1));
+      if (p1 >= p0) pw.phase(p1, p1 - p0 + 1, true);
       const auto &doms = warp_dom_index[w];
       for (auto it = doms.rbegin(); it != doms.rend(); ++it) {
         const int32_t d0 = domain_range[*it].first, d1 = domain_range[*it].second;
@@ -396,21 +447,21 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
           for (int32_t c : imports) {
             xslot[c] = slots.take();
             entries.push_back({T(0), off(xslot[c])});
-            words.push_back((uint32_t)newpos[c]);
+            words.push_back((uint32_t)newpos[c] * row_bytes);
           }
-          pw.record(0, T(0), entries, words.data(), kLaneImport, kLaneImport, kLaneImport, kLaneImport);
+          pw.words(kLaneImport, 0, entries, words);
         }
         backward_rows(pw, slots, d0, d1);
       }
       peak_b = std::max(peak_b, slots.peak);
     }
-    pw.simple(0, kLaneEnd, 0);
+    pw.simple(kLaneEnd);
     lay.warp_page.push_back((int32_t)(lay.blob.size() / page_bytes));
   }
   lay.fwd_live = peak_f;
   lay.bwd_live = peak_b;
   lay.slots = 2 + std::max(peak_f, peak_b);
-  if (lay.slots > max_slots)
+  if (lay.slots > std::min(max_slots, 255))
     throw host::Error(host::kTooLarge, "the lane solve would keep more live values than its shared memory holds");
   lay.in_pos.resize(n);
   lay.out_pos.resize(n);

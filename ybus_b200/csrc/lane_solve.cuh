@@ -25,8 +25,6 @@
 
 namespace yb {
 
-constexpr int kLaneBatch = 4;                // rows per prefetch batch
-constexpr int kLaneRows = 2 * kLaneBatch;    // rows of the per-warp prefetch ring
 constexpr int kLaneBarriers = 2;             // block barriers in every warp's stream
 constexpr int kLaneMaxWarps = 8;             // warps per block at most
 
@@ -52,95 +50,68 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// One entry {val or a 32-bit word, byte offset}: 16 bytes for FP64, 8 for FP32.
-__device__ __forceinline__ void lane_entry(const uint8_t *p, double &v, uint32_t &o) {
-  const double2 e = *reinterpret_cast<const double2 *>(p);
-  v = e.x;
-  o = (uint32_t)__double_as_longlong(e.y);
+// The block's dynamic shared memory. Every shared access of the lane solve is a 32-bit byte offset
+// into it, so the compiler addresses shared memory directly.
+extern __shared__ __align__(128) unsigned char lane_shared[];
+
+template <class T> __device__ __forceinline__ T &lane_at(uint32_t off) { return *reinterpret_cast<T *>(lane_shared + off); }
+
+// An entry {val or a 32-bit word, offset} at shared offset e: 16 bytes for FP64, 8 for FP32.
+__device__ __forceinline__ void lane_entry(uint32_t e, double &v, uint32_t &word, uint32_t &o) {
+  const uint4 x = lane_at<uint4>(e);
+  v = __hiloint2double((int)x.y, (int)x.x);
+  word = x.x, o = x.z;
 }
-__device__ __forceinline__ void lane_entry(const uint8_t *p, float &v, uint32_t &o) {
-  const float2 e = *reinterpret_cast<const float2 *>(p);
-  v = e.x;
-  o = __float_as_uint(e.y);
-}
-template <class T> __device__ __forceinline__ void lane_word(const uint8_t *p, uint32_t &word, uint32_t &o) {
-  const uint2 *q = reinterpret_cast<const uint2 *>(p);
-  if constexpr (sizeof(T) == 8) {
-    const uint4 e = *reinterpret_cast<const uint4 *>(p);
-    word = e.x, o = e.z;
-  } else {
-    const uint2 e = *q;
-    word = e.x, o = e.y;
-  }
+__device__ __forceinline__ void lane_entry(uint32_t e, float &v, uint32_t &word, uint32_t &o) {
+  const uint2 x = lane_at<uint2>(e);
+  v = __uint_as_float(x.x);
+  word = x.x, o = x.y;
 }
 
 // The block barrier, in its form that warps may reach from different instructions (the error path
 // takes the barriers its stream did not reach at the kernel's end).
 __device__ __forceinline__ void lane_barrier() { asm volatile("barrier.sync 0;" ::: "memory"); }
 
-template <class T> __device__ __forceinline__ T &lane_slot(uint8_t *live_lane, uint32_t off) {
-  return *reinterpret_cast<T *>(live_lane + off);
+// acc[offset] -= val * z for C entries (C known at compile time) at shared offset e; the offsets of
+// one record are distinct, so every accumulator is read before any is written.
+template <class T, int C> __device__ __forceinline__ void lane_scatter_n(uint32_t e, T z, uint32_t live) {
+  constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8;
+  T v[C], a[C];
+  uint32_t o[C], w;
+#pragma unroll
+  for (int c = 0; c < C; ++c) lane_entry(e + c * E, v[c], w, o[c]);
+#pragma unroll
+  for (int c = 0; c < C; ++c) a[c] = lane_at<T>(live + o[c]);
+#pragma unroll
+  for (int c = 0; c < C; ++c) lane_at<T>(live + o[c]) = fma(-v[c], z, a[c]);
 }
 
-// acc[offset] -= val * z for a record's entries; the offsets of one record are distinct, so all of
-// a group's accumulators are read before any is written.
-template <class T> __device__ __forceinline__ void lane_scatter(const uint8_t *e, int count, T z, uint8_t *live_lane) {
-  constexpr int E = sizeof(T) == 8 ? 16 : 8;
-  int i = 0;
-  for (; i + 4 <= count; i += 4) {
-    T v[4], a[4];
-    uint32_t o[4];
+// acc -= val * x[offset] over C entries, in stored order.
+template <class T, int C> __device__ __forceinline__ T lane_gather_n(uint32_t e, T acc, uint32_t live) {
+  constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8;
+  T v[C], x[C];
+  uint32_t o[C], w;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) lane_entry(e + (i + q) * E, v[q], o[q]);
+  for (int c = 0; c < C; ++c) lane_entry(e + c * E, v[c], w, o[c]);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) a[q] = lane_slot<T>(live_lane, o[q]);
+  for (int c = 0; c < C; ++c) x[c] = lane_at<T>(live + o[c]);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) lane_slot<T>(live_lane, o[q]) = fma(-v[q], z, a[q]);
-  }
-  const int left = count - i;
-  if (left > 0) {
-    T v[3], a[3];
-    uint32_t o[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-      if (q < left) lane_entry(e + (i + q) * E, v[q], o[q]);
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-      if (q < left) a[q] = lane_slot<T>(live_lane, o[q]);
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-      if (q < left) lane_slot<T>(live_lane, o[q]) = fma(-v[q], z, a[q]);
-  }
+  for (int c = 0; c < C; ++c) acc = fma(-v[c], x[c], acc);
+  return acc;
 }
 
-// acc -= val * x[offset] over a record's entries, in stored order.
-template <class T> __device__ __forceinline__ T lane_gather(const uint8_t *e, int count, T acc, uint8_t *live_lane) {
-  constexpr int E = sizeof(T) == 8 ? 16 : 8;
-  int i = 0;
-  for (; i + 4 <= count; i += 4) {
-    T v[4], x[4];
-    uint32_t o[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) lane_entry(e + (i + q) * E, v[q], o[q]);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) x[q] = lane_slot<T>(live_lane, o[q]);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc = fma(-v[q], x[q], acc);
-  }
-  const int left = count - i;
-  if (left > 0) {
-    T v[3], x[3];
-    uint32_t o[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-      if (q < left) lane_entry(e + (i + q) * E, v[q], o[q]);
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-      if (q < left) x[q] = lane_slot<T>(live_lane, o[q]);
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-      if (q < left) acc = fma(-v[q], x[q], acc);
-  }
+// The same for any count, four at a time.
+template <class T> __device__ __forceinline__ void lane_scatter(uint32_t e, uint32_t count, T z, uint32_t live) {
+  constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8;
+  uint32_t i = 0;
+  for (; i + 4 <= count; i += 4) lane_scatter_n<T, 4>(e + i * E, z, live);
+  for (; i < count; ++i) lane_scatter_n<T, 1>(e + i * E, z, live);
+}
+template <class T> __device__ __forceinline__ T lane_gather(uint32_t e, uint32_t count, T acc, uint32_t live) {
+  constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8;
+  uint32_t i = 0;
+  for (; i + 4 <= count; i += 4) acc = lane_gather_n<T, 4>(e + i * E, acc, live);
+  for (; i < count; ++i) acc = lane_gather_n<T, 1>(e + i * E, acc, live);
   return acc;
 }
 
@@ -149,169 +120,159 @@ template <class T> __device__ __forceinline__ T lane_gather(const uint8_t *e, in
 template <class T>
 __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs a, T *__restrict__ work,
                                                                        T *__restrict__ partial) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  constexpr int B = kLaneBatch, R = kLaneRows, E = sizeof(T) == 8 ? 16 : 8;
+  constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8, ROW = 32 * sizeof(T);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int n = a.n, S = a.ring, PB = a.page_bytes;
-  uint8_t *base = smem_raw + (size_t)warp * lane_warp_bytes<T>(a.slots, S, PB);
-  uint8_t *live_lane = base + lane * sizeof(T);
-  T *rows = reinterpret_cast<T *>(base + (size_t)a.slots * 32 * sizeof(T));
-  uint8_t *ring = reinterpret_cast<uint8_t *>(rows + R * 32);
-  uint64_t *full = reinterpret_cast<uint64_t *>(ring + (size_t)S * PB);
-  T *w = work + (size_t)blockIdx.x * n * 32;
-  T *part = partial + (size_t)blockIdx.x * a.partials * 32;
+  const int S = a.ring, PB = a.page_bytes;
+  const uint32_t base = (uint32_t)(warp * lane_warp_bytes<T>(a.slots, S, PB));
+  const uint32_t live = base + lane * (uint32_t)sizeof(T);                     // this lane's slot 0
+  const uint32_t rows = base + (uint32_t)a.slots * ROW + lane * (uint32_t)sizeof(T);  // its ring slot 0
+  const uint32_t ring = base + (uint32_t)a.slots * ROW + (uint32_t)kLaneRows * ROW;  // the page ring
+  uint64_t *full = &lane_at<uint64_t>(ring + (uint32_t)S * PB);
+  const uint32_t smem_s = smem_u32(lane_shared);  // the shared window address of offset 0
+  uint8_t *w_lane = reinterpret_cast<uint8_t *>(work + (size_t)blockIdx.x * a.n * 32 + lane);
+  uint8_t *part_lane = reinterpret_cast<uint8_t *>(partial + (size_t)blockIdx.x * a.partials * 32 + lane);
   const int p0 = __ldg(a.warp_page + warp), np = __ldg(a.warp_page + warp + 1) - p0;
   const uint8_t *stream = a.blob + (size_t)p0 * PB;
 
-  for (int s = 0; s < a.slots; ++s) lane_slot<T>(live_lane, s * 32 * sizeof(T)) = T(0);
+  for (int s = 0; s < a.slots; ++s) lane_at<T>(live + s * ROW) = T(0);
   if (lane == 0) {
     for (int s = 0; s < S; ++s) mbar_init(full + s, 1);
     mbar_fence_init();
   }
   __syncwarp();
   if (lane == 0)
-    for (int s = 0; s < S && s < np; ++s) bulk_page(ring + (size_t)s * PB, stream + (size_t)s * PB, (uint32_t)PB, full + s);
+    for (int s = 0; s < S && s < np; ++s)
+      bulk_page(lane_shared + ring + s * PB, stream + (size_t)s * PB, (uint32_t)PB, full + s);
   int issued = min(S, np);
   __syncwarp();
 
-  int k = 0;  // the page being read
-  const uint8_t *page = ring;
-  int off = 0;
+  int k = 0;               // the page being read
+  uint32_t page = ring;    // the record being read
   bool ok = np > 0 && mbar_wait_bounded(full, 0, a.error);
-  auto advance = [&]() {  // the finished page's slot takes page k + S
-    __syncwarp();
-    if (k + S < np) {
-      if (lane == 0) {
-        fence_proxy_async();
-        bulk_page(ring + (size_t)(k % S) * PB, stream + (size_t)(k + S) * PB, (uint32_t)PB, full + k % S);
-      }
-      issued = k + S + 1;
-    }
-    ++k;
-    ok = k < np && mbar_wait_bounded(full + k % S, (uint32_t)((k / S) & 1), a.error);
-    page = ring + (size_t)(k % S) * PB;
-    off = 0;
-  };
-
-  // the phase: rows from `start` up (forward) or down (backward); row i of the phase is prefetched
-  // into ring row i % R by batch i / B
-  int start = 0, len = 0, i = 0, cur = 0, barriers = 0;
-  bool backward = false, ended = false;
-  auto issue_batch = [&](int batch) {
+  bool ended = false;
+  int barriers = 0;
+  T z = T(0);  // the forward row's result, or the backward row's running sum
+  while (ok) {
+    const uint4 h = lane_at<uint4>(page);
+    const uint32_t kind = (h.x >> 16) & 31u, count = h.x >> 24;
+    const uint32_t self = live + ((h.x & 0xffffu) << 4);
+    const uint32_t b_at = rows + ((h.x >> 21) & 7u) * ROW;
+    const uint32_t e = page + 16;
+    const uint32_t next = page + 16 + ((count * E + 15) & ~15u);
+    T dinv;
+    if constexpr (sizeof(T) == 8)
+      dinv = __hiloint2double((int)h.w, (int)h.z);
+    else
+      dinv = __uint_as_float(h.z);
+    // the start of a forward row: z from b and the row's accumulator, into the work row
+    auto forward = [&]() {
+      T &acc = lane_at<T>(self);
+      const T b = lane_at<T>(b_at) + acc;
+      acc = T(0);
+      z = b * dinv;
+      *reinterpret_cast<T *>(w_lane + h.y) = z;
+    };
+    // the end of a backward row: x into its slot and the work row
+    auto backward = [&]() {
+      const T x = z * dinv;
+      lane_at<T>(self) = x;
+      *reinterpret_cast<T *>(w_lane + h.y) = x;
+    };
+    switch (kind) {
+      case kLaneFwdRow0: forward(); break;
+      case kLaneFwdRow0 + 1: forward(); lane_scatter_n<T, 1>(e, z, live); break;
+      case kLaneFwdRow0 + 2: forward(); lane_scatter_n<T, 2>(e, z, live); break;
+      case kLaneFwdRow0 + 3: forward(); lane_scatter_n<T, 3>(e, z, live); break;
+      case kLaneFwdRow0 + 4: forward(); lane_scatter_n<T, 4>(e, z, live); break;
+      case kLaneFwdRowN: forward(); lane_scatter<T>(e, count, z, live); break;
+      case kLaneFwdMore: lane_scatter<T>(e, count, z, live); break;
+      case kLaneBwdRow0: z = lane_at<T>(b_at); backward(); break;
+      case kLaneBwdRow0 + 1: z = lane_gather_n<T, 1>(e, lane_at<T>(b_at), live); backward(); break;
+      case kLaneBwdRow0 + 2: z = lane_gather_n<T, 2>(e, lane_at<T>(b_at), live); backward(); break;
+      case kLaneBwdRow0 + 3: z = lane_gather_n<T, 3>(e, lane_at<T>(b_at), live); backward(); break;
+      case kLaneBwdRow0 + 4: z = lane_gather_n<T, 4>(e, lane_at<T>(b_at), live); backward(); break;
+      case kLaneBwdRowN: z = lane_gather<T>(e, count, lane_at<T>(b_at), live); backward(); break;
+      case kLaneBwdBegin: z = lane_gather<T>(e, count, lane_at<T>(b_at), live); break;
+      case kLaneBwdMore: z = lane_gather<T>(e, count, z, live); break;
+      case kLaneBwdEnd: z = lane_gather<T>(e, count, z, live); backward(); break;
+      case kLanePrefetch: {
+        const int64_t step = (h.z & 1u) ? -(int64_t)ROW : (int64_t)ROW;
+        const uint32_t dst = smem_s + rows + ((h.z & 2u) ? (uint32_t)kLaneBatch * ROW : 0u);
+        const uint32_t nrows = h.x & 0xffffu;
 #pragma unroll
-    for (int q = 0; q < B; ++q) {
-      const int r = batch * B + q;
-      if (r < len)
-        cp_async_lane<sizeof(T)>(rows + (r & (R - 1)) * 32 + lane, w + (size_t)(backward ? start - r : start + r) * 32 + lane);
-    }
-    cp_async_commit();
-  };
-  auto next_row = [&]() -> T {
-    if ((i & (B - 1)) == 0) {
-      if (i > 0) issue_batch(i / B + 1);
-      cp_async_wait<1>();
-    }
-    cur = backward ? start - i : start + i;
-    return rows[(i++ & (R - 1)) * 32 + lane];
-  };
-
-  T z = T(0);  // the row's forward result, or its backward running sum
-  while (ok && !ended) {
-    if (off + 16 > PB) {
-      advance();
-      continue;
-    }
-    const uint2 h = *reinterpret_cast<const uint2 *>(page + off);
-    const uint32_t kind = h.y >> 16;
-    const int count = (int)(h.y & 0xffffu);
-    const uint8_t *e = page + off + 16;
-    if (kind <= kLaneRowEnd) {
-      const T dinv = *reinterpret_cast<const T *>(page + off + 8);
-      if (!backward) {
-        if (kind <= kLaneRowBegin) {
-          T b = next_row();
-          T &acc = lane_slot<T>(live_lane, h.x);
-          b += acc;
-          acc = T(0);
-          z = b * dinv;
-          w[(size_t)cur * 32 + lane] = z;
-        }
-        lane_scatter<T>(e, count, z, live_lane);
-      } else {
-        if (kind <= kLaneRowBegin) z = next_row();
-        z = lane_gather<T>(e, count, z, live_lane);
-        if (kind == kLaneRow || kind == kLaneRowEnd) {
-          const T x = z * dinv;
-          lane_slot<T>(live_lane, h.x) = x;
-          w[(size_t)cur * 32 + lane] = x;
-        }
+        for (int q = 0; q < kLaneBatch; ++q)
+          if (q < (int)nrows)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst + q * ROW),
+                         "l"(w_lane + (int64_t)h.y + q * step), "n"(sizeof(T))
+                         : "memory");
+        cp_async_commit();
+        cp_async_wait<1>();
+        break;
       }
-      off += 16 + ((count * E + 15) & ~15);
-      continue;
-    }
-    switch (kind & 0xffu) {
-      case kLanePhase: {
+      case kLanePhase:
         cp_async_wait<0>();
         __threadfence();  // the rows this lane stored are what the phase's copies read
-        start = (int)h.x;
-        len = (int)*reinterpret_cast<const uint32_t *>(page + off + 8);
-        backward = (kind & kLaneBackward) != 0;
-        i = 0;
-        issue_batch(0);
-        issue_batch(1);
-        off += 16;
         break;
-      }
       case kLanePartials: {
-        T acc = lane_slot<T>(live_lane, h.x);
-        for (int q = 0; q < count; ++q) {
-          uint32_t word, o;
-          lane_word<T>(e + q * E, word, o);
-          acc += part[(size_t)word * 32 + lane];
+        T acc = lane_at<T>(self);
+        for (uint32_t c = 0; c < count; ++c) {
+          T v;
+          uint32_t w, o;
+          lane_entry(e + c * E, v, w, o);
+          acc += *reinterpret_cast<const T *>(part_lane + w);
         }
-        lane_slot<T>(live_lane, h.x) = acc;
-        off += 16 + ((count * E + 15) & ~15);
+        lane_at<T>(self) = acc;
         break;
       }
-      case kLaneFlush: {
-        for (int q = 0; q < count; ++q) {
-          uint32_t word, o;
-          lane_word<T>(e + q * E, word, o);
-          part[(size_t)word * 32 + lane] = lane_slot<T>(live_lane, o);
-          lane_slot<T>(live_lane, o) = T(0);
+      case kLaneFlush:
+        for (uint32_t c = 0; c < count; ++c) {
+          T v;
+          uint32_t w, o;
+          lane_entry(e + c * E, v, w, o);
+          *reinterpret_cast<T *>(part_lane + w) = lane_at<T>(live + o);
+          lane_at<T>(live + o) = T(0);
         }
-        off += 16 + ((count * E + 15) & ~15);
         break;
-      }
-      case kLaneImport: {
-        for (int q = 0; q < count; ++q) {
-          uint32_t word, o;
-          lane_word<T>(e + q * E, word, o);
-          lane_slot<T>(live_lane, o) = w[(size_t)word * 32 + lane];
+      case kLaneImport:
+        for (uint32_t c = 0; c < count; ++c) {
+          T v;
+          uint32_t w, o;
+          lane_entry(e + c * E, v, w, o);
+          lane_at<T>(live + o) = *reinterpret_cast<const T *>(w_lane + w);
         }
-        off += 16 + ((count * E + 15) & ~15);
         break;
-      }
       case kLaneBarrier:
         lane_barrier();
         ++barriers;
-        off += 16;
         break;
       case kLaneEnd:
         ended = true;
         break;
-      case kLanePageEnd:
-        advance();
-        break;
+      case kLanePageEnd: {  // the finished page's slot takes page k + S
+        __syncwarp();
+        if (k + S < np) {
+          if (lane == 0) {
+            fence_proxy_async();
+            bulk_page(lane_shared + ring + (k % S) * PB, stream + (size_t)(k + S) * PB, (uint32_t)PB, full + k % S);
+          }
+          issued = k + S + 1;
+        }
+        ++k;
+        ok = k < np && mbar_wait_bounded(full + k % S, (uint32_t)((k / S) & 1), a.error);
+        page = ring + (uint32_t)(k % S) * PB;
+        continue;
+      }
       default:  // a malformed stream
-        if (lane == 0) atomicExch(a.error, 1);
         ok = false;
-        break;
+        continue;
     }
+    if (ended) break;
+    page = next;
   }
   cp_async_wait<0>();
   if (!ended) {
-    // a wait that ran out: let the copies still in flight land before the block's memory is reused
+    // a wait that ran out, or a malformed stream: let the copies still in flight land before the
+    // block's memory is reused
     if (lane == 0) atomicExch(a.error, 1);
     for (int p = k; p < issued; ++p) mbar_wait_bounded(full + p % S, (uint32_t)((p / S) & 1), a.error);
   }

@@ -140,38 +140,52 @@ template <class T>
 DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t warps, int32_t page_bytes, int32_t K);
 
 // The factor for the lane solve (lane_solve.cuh: one right-hand side per lane, every lane of a warp
-// taking the same rows, `warps` warps per block of 32 right-hand sides). The rows are in a
-// postorder of the forward elimination forest with larger subtrees first, cut into subtree domains
-// (dealt to the warps) under a top (taken by warp 0 between two block barriers); each warp's part
-// is one stream of records in fixed-size pages. A record: uint32 self, uint32 count | kind << 16,
-// then at byte 8 either T dinv or a 32-bit word, then `count` entries {T val (or a 32-bit word in
-// its place), uint32 offset} of 16 bytes (FP64) or 8 bytes (FP32). Offsets and `self` are byte
-// offsets of 32-value live slots; slot 0 is always zero, slot 1 a sink. Kinds:
-//   kLanePhase (self = first position, word = rows; | kLaneBackward for a backward phase): the next
-//     rows take the work array's positions from self upwards (forward) or downwards (backward).
-//   kLaneRow, split over records as kLaneRowBegin, kLaneRowMore..., kLaneRowEnd: forward, read and
-//     zero acc at self, z = (b + acc) * dinv into the work row, then acc[offset] -= val * z per
-//     entry; backward, acc = z from the work row minus val * x[offset] per entry, x = acc * dinv
-//     into the work row and into slot self.
-//   kLaneFlush: per entry, the partial array's value `word` takes slot `offset`, which is zeroed.
-//   kLanePartials: slot self += the partial array's values `word` of its entries, in order.
-//   kLaneImport: per entry, slot `offset` takes the work row at position `word`.
-//   kLaneBarrier: a block barrier (every warp's stream has two). kLaneEnd ends the stream;
-//   kLanePageEnd ends its page.
+// taking the same rows, `warps` warps per block of 32 right-hand sides). The rows are in a postorder
+// of the forward elimination forest with larger subtrees first, cut into subtree domains (dealt to
+// the warps) under a top (taken by warp 0 between two block barriers); each warp's part is one
+// stream of records in fixed-size pages.
+//
+// A record is a 16-byte header, then `count` entries of 16 bytes (FP64) or 8 (FP32): {T val, or a
+// 32-bit word in its place; uint32 offset}. The header: uint32 {self (16 bits), kind (5 bits), ring
+// slot (3 bits), count (8 bits)}, uint32 word, then 8 bytes: T dinv for rows, uint32 flags for a
+// prefetch. Offsets are byte offsets of 32-value live slots (slot 0 is always zero, slot 1 a sink),
+// `self` such an offset / 16; words are byte offsets of 32-value rows of the work or partial array.
+//   kLaneFwdRow0 + c (c = 0..4 entries), kLaneFwdRowN, kLaneFwdMore: a forward row at work offset
+//     `word`: read and zero acc at self, z = (b + acc) * dinv with b from its ring slot, z into the
+//     work row, then acc[offset] -= val * z per entry (kLaneFwdMore: more entries of the last row).
+//   kLaneBwdRow0 + c, kLaneBwdRowN, or kLaneBwdBegin, kLaneBwdMore..., kLaneBwdEnd: a backward row:
+//     acc = z from its ring slot minus val * x[offset] per entry, x = acc * dinv into the work row
+//     and into slot self.
+//   kLanePrefetch: copies `self` work rows (up to kLaneBatch) from offset `word` on, upwards (or
+//     downwards, flag bit 0), into the ring's lower (or, flag bit 1, upper) kLaneBatch slots, then
+//     waits for the batch before it.
+//   kLanePhase: a new run of rows: earlier copies are finished and this lane's stores are visible
+//     to its copies.
+//   kLaneFlush: per entry, the partial row `word` takes slot `offset`, which is zeroed.
+//   kLanePartials: slot self += the partial rows `word` of its entries, in order.
+//   kLaneImport: per entry, slot `offset` takes the work row `word`.
+//   kLaneBarrier: a block barrier (every warp's stream has two); kLaneEnd ends the stream;
+//   kLanePageEnd ends its page (every page has one).
 enum LaneKind : uint32_t {
-  kLaneRow = 0,
-  kLaneRowBegin = 1,
-  kLaneRowMore = 2,
-  kLaneRowEnd = 3,
-  kLanePhase = 4,
-  kLanePartials = 5,
-  kLaneFlush = 6,
-  kLaneImport = 7,
-  kLaneBarrier = 8,
-  kLaneEnd = 9,
-  kLanePageEnd = 10,
-  kLaneBackward = 0x100
+  kLaneFwdRow0 = 0,  // .. kLaneFwdRow0 + 4
+  kLaneFwdRowN = 5,
+  kLaneFwdMore = 6,
+  kLaneBwdRow0 = 7,  // .. kLaneBwdRow0 + 4
+  kLaneBwdRowN = 12,
+  kLaneBwdBegin = 13,
+  kLaneBwdMore = 14,
+  kLaneBwdEnd = 15,
+  kLanePrefetch = 16,
+  kLanePhase = 17,
+  kLanePartials = 18,
+  kLaneFlush = 19,
+  kLaneImport = 20,
+  kLaneBarrier = 21,
+  kLaneEnd = 22,
+  kLanePageEnd = 23
 };
+constexpr int kLaneBatch = 4;              // work rows per prefetch
+constexpr int kLaneRows = 2 * kLaneBatch;  // slots of a warp's prefetch ring
 struct LaneLayout {
   int32_t warps = 1, slots = 0, page_bytes = 0, value_bytes = 0;
   int32_t domains = 0, top = 0, partials = 0;  // partials: partial-array values per block
