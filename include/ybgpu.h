@@ -162,8 +162,9 @@ int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int32_t kind);
  * YB_ERROR_INVALID_ARGUMENT if the factor admits no lane layout (no postorder serves both sweeps,
  * or too many live values). */
 int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t *info);
-/* No ybus counterpart: the lane solve's shape for a precision: warps per block (1..8, default 6)
- * and page bytes (256..16384, a multiple of 16, default 2048). */
+/* No ybus counterpart: the lane solve's shape for a precision: warps per block (1..8, default 8)
+ * and page bytes (256..16384, a multiple of 16; default 0: the largest of 2048, 1024, 768, 512 with
+ * which three blocks fit an SM). */
 int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32_t page_bytes);
 /* No ybus counterpart: the number of right-hand sides from which the automatic choice takes the
  * lane solve (default 8192). */

@@ -719,6 +719,27 @@ void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, doub
   }
 }
 
+// The lane layout a solve takes: the configured warps per block, or fewer when a block does not
+// fit shared memory; with page bytes 0, the largest page of 2048, 1024, 768 or 512 bytes with which
+// three blocks fit an SM (each block's rows are a long chain, so the grid should be one wave of as
+// many warps as fit), else 512. Null when the factor admits no lane layout.
+template <class T> DeviceLane *lane_pick(yb_factor *f, const TileConfig &cfg, cudaStream_t stream) {
+  for (int warps = cfg.lane_warps; warps >= 1; --warps) {
+    DeviceLane *d = nullptr;
+    if (cfg.lane_page > 0) {
+      d = lane_for<T>(f, warps, cfg.lane_page, stream);
+    } else {
+      for (int page : {2048, 1024, 768, 512}) {
+        d = lane_for<T>(f, warps, page, stream);
+        if (!d || 3 * (lane_smem<T>(d) + 1024) <= (size_t)f->gpu->smem_per_sm) break;
+      }
+    }
+    if (!d) return nullptr;
+    if (lane_smem<T>(d) <= (size_t)f->gpu->smem_optin) return d;
+  }
+  return nullptr;
+}
+
 template <class T> TileConfig resolve(yb_factor *f, TileConfig cfg) {
   if (cfg.kind == kTileLane) cfg.kind = kTileAuto;  // callers other than the plain solve
   if (cfg.kind == kTileGlobal) return cfg;
@@ -787,13 +808,7 @@ void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t
   auto run = [&](auto zero, const TileConfig &configured, auto &fwd, auto &bwd, auto &scratch, auto &cache) {
     using T = decltype(zero);
     if (configured.kind == kTileLane || (configured.kind == kTileAuto && count >= configured.lane_min_count)) {
-      // the configured warps per block, or fewer when the block's slots do not fit shared memory
-      DeviceLane *d = nullptr;
-      for (int warps = configured.lane_warps; warps >= 1; --warps) {
-        d = lane_for<T>(f, warps, configured.lane_page, stream);
-        if (!d || lane_smem<T>(d) <= (size_t)f->gpu->smem_optin) break;
-      }
-      if (d && lane_smem<T>(d) > (size_t)f->gpu->smem_optin) d = nullptr;
+      DeviceLane *d = lane_pick<T>(f, configured, stream);
       if (d && (configured.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane<T>(f, d, b, ldb, x, ldx, count, stream);
         return;
@@ -1094,8 +1109,7 @@ extern "C" int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t 
     require(!f->is_complex, "a complex factor has no lane solve");
     cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
     const TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
-    DeviceLane *d = precision == YB_FP64 ? lane_for<double>(f, t.lane_warps, t.lane_page, f->gpu->stream)
-                                         : lane_for<float>(f, t.lane_warps, t.lane_page, f->gpu->stream);
+    DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, t, f->gpu->stream) : lane_pick<float>(f, t, f->gpu->stream);
     if (!d) throw host::Error(host::kInvalidArgument, "the factor admits no lane layout");
     const size_t smem = precision == YB_FP64 ? lane_smem<double>(d) : lane_smem<float>(d);
     const int64_t v[12] = {d->slots, d->pages, d->page_bytes, d->fwd_live, d->bwd_live, d->entries, (int64_t)smem,
@@ -1110,7 +1124,8 @@ extern "C" int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t w
     require(f != nullptr, "null factor");
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
     require(warps >= 1 && warps <= kLaneMaxWarps, "1 to 8 warps per block");
-    require(page_bytes >= 256 && page_bytes <= 16384 && page_bytes % 16 == 0, "pages of 256 to 16384 bytes, a multiple of 16");
+    require(page_bytes == 0 || (page_bytes >= 256 && page_bytes <= 16384 && page_bytes % 16 == 0),
+            "pages of 256 to 16384 bytes, a multiple of 16, or 0 for the automatic choice");
     TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
     t.lane_warps = warps, t.lane_page = page_bytes;
     return YB_OK;

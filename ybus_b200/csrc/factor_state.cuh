@@ -91,7 +91,7 @@ struct TileConfig {
   // the automatic choice takes the lane solve from this many right-hand sides on (one warp per 32:
   // fewer leave SMs idle, where the domain solve's tiles spread over all of them)
   int64_t lane_min_count = 8192;
-  int lane_warps = 6, lane_page = 2048;  // the lane solve's warps per block (one group of 32 right-hand sides), page bytes
+  int lane_warps = 8, lane_page = 0;  // the lane solve's warps per block (one group of 32 right-hand sides), page bytes
 };
 
 // A lane layout on the device (LaneLayout in plan.hpp).

@@ -282,8 +282,8 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   };
   Cut best = cut_at(total + 1);  // one domain per tree of the forest, no top
   if (warps > 1)
-    for (int k = 0; k <= 12; ++k) {
-      Cut c = cut_at(total / (warps * std::pow(2.0, k)));
+    for (int k = 0; k <= 48; ++k) {  // caps a quarter octave apart
+      Cut c = cut_at(total / (warps * std::pow(2.0, k / 4.0)));
       if (c.cost < best.cost) best = std::move(c);
     }
   lay.cost = best.cost;
