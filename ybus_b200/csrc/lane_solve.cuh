@@ -178,19 +178,35 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
       lane_at<T>(self) = x;
       *reinterpret_cast<T *>(w_lane + h.y) = x;
     };
+    // the common records first: rows of at most 4 entries
+    if (kind <= kLaneFwdRow0 + 4) {
+      forward();
+      switch (count) {
+        case 1: lane_scatter_n<T, 1>(e, z, live); break;
+        case 2: lane_scatter_n<T, 2>(e, z, live); break;
+        case 3: lane_scatter_n<T, 3>(e, z, live); break;
+        case 4: lane_scatter_n<T, 4>(e, z, live); break;
+        default: break;
+      }
+      page = next;
+      continue;
+    }
+    if (kind - kLaneBwdRow0 <= 4u) {
+      const T b = lane_at<T>(b_at);
+      switch (count) {
+        case 1: z = lane_gather_n<T, 1>(e, b, live); break;
+        case 2: z = lane_gather_n<T, 2>(e, b, live); break;
+        case 3: z = lane_gather_n<T, 3>(e, b, live); break;
+        case 4: z = lane_gather_n<T, 4>(e, b, live); break;
+        default: z = b; break;
+      }
+      backward();
+      page = next;
+      continue;
+    }
     switch (kind) {
-      case kLaneFwdRow0: forward(); break;
-      case kLaneFwdRow0 + 1: forward(); lane_scatter_n<T, 1>(e, z, live); break;
-      case kLaneFwdRow0 + 2: forward(); lane_scatter_n<T, 2>(e, z, live); break;
-      case kLaneFwdRow0 + 3: forward(); lane_scatter_n<T, 3>(e, z, live); break;
-      case kLaneFwdRow0 + 4: forward(); lane_scatter_n<T, 4>(e, z, live); break;
       case kLaneFwdRowN: forward(); lane_scatter<T>(e, count, z, live); break;
       case kLaneFwdMore: lane_scatter<T>(e, count, z, live); break;
-      case kLaneBwdRow0: z = lane_at<T>(b_at); backward(); break;
-      case kLaneBwdRow0 + 1: z = lane_gather_n<T, 1>(e, lane_at<T>(b_at), live); backward(); break;
-      case kLaneBwdRow0 + 2: z = lane_gather_n<T, 2>(e, lane_at<T>(b_at), live); backward(); break;
-      case kLaneBwdRow0 + 3: z = lane_gather_n<T, 3>(e, lane_at<T>(b_at), live); backward(); break;
-      case kLaneBwdRow0 + 4: z = lane_gather_n<T, 4>(e, lane_at<T>(b_at), live); backward(); break;
       case kLaneBwdRowN: z = lane_gather<T>(e, count, lane_at<T>(b_at), live); backward(); break;
       case kLaneBwdBegin: z = lane_gather<T>(e, count, lane_at<T>(b_at), live); break;
       case kLaneBwdMore: z = lane_gather<T>(e, count, z, live); break;
