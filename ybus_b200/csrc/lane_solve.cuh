@@ -121,7 +121,10 @@ template <class T>
 __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs a, T *__restrict__ work,
                                                                        T *__restrict__ partial) {
   constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8, ROW = 32 * sizeof(T);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // The warp index through a shuffle from lane 0: the compiler then knows it (and the shared
+  // offsets, record fields and branches derived from it) to be the same across the warp, and keeps
+  // the records' decoding on the uniform datapath instead of every lane's registers.
+  const int lane = threadIdx.x & 31, warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
   const int S = a.ring, PB = a.page_bytes;
   const uint32_t base = (uint32_t)(warp * lane_warp_bytes<T>(a.slots, S, PB));
   const uint32_t live = base + lane * (uint32_t)sizeof(T);                     // this lane's slot 0
