@@ -592,7 +592,10 @@ __global__ void __launch_bounds__(512, 1) domain_tile_kernel(DomainArgs a, IO io
   static_assert(32 % W == 0, "W divides a warp");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int n = a.n;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  // the warp index through a shuffle from lane 0, so the compiler keeps what derives from it (the
+  // warp's ring, its pages, the record headers) on the uniform datapath
+  const int lane = threadIdx.x & 31, warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0),
+            warps = blockDim.x >> 5;
   const int S = a.ring, PB = a.page_bytes;
   const int m = a.tail;
   const size_t y_bytes = (((size_t)(n + 2) * W * sizeof(T)) + 127) & ~(size_t)127;
