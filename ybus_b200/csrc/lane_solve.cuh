@@ -155,13 +155,17 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
   bool ended = false;
   int barriers = 0;
   T z = T(0);  // the forward row's result, or the backward row's running sum
+  // the header of the record being read, loaded while the record before it runs (pages are written
+  // only by the bulk copies, never by a record)
+  uint4 hn = lane_at<uint4>(page);
   while (ok) {
-    const uint4 h = lane_at<uint4>(page);
+    const uint4 h = hn;
     const uint32_t kind = (h.x >> 16) & 31u, count = h.x >> 24;
     const uint32_t self = live + ((h.x & 0xffffu) << 4);
     const uint32_t b_at = rows + ((h.x >> 21) & 7u) * ROW;
     const uint32_t e = page + 16;
     const uint32_t next = page + 16 + ((count * E + 15) & ~15u);
+    if (kind != kLanePageEnd) hn = lane_at<uint4>(next);  // within the page: every page ends with its end record
     T dinv;
     if constexpr (sizeof(T) == 8)
       dinv = __hiloint2double((int)h.w, (int)h.z);
@@ -279,6 +283,7 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
         ++k;
         ok = k < np && mbar_wait_bounded(full + k % S, (uint32_t)((k / S) & 1), a.error);
         page = ring + (uint32_t)(k % S) * PB;
+        if (ok) hn = lane_at<uint4>(page);
         continue;
       }
       default:  // a malformed stream
