@@ -307,11 +307,9 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from ybus_b200 import FP32, FP64, Gpu, GpuFactor
+    from ybus_b200 import FP32, FP64, Gpu, GpuFactor, replicas
 
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
+    rank, world, local = replicas.rank_info()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -363,12 +361,8 @@ def main():
         torch.cuda.synchronize()
         elapsed_ms = start.elapsed_time(end)
         launch_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs)
-        if world > 1:
-            dist.barrier()
-            t = torch.tensor([elapsed_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            elapsed_ms = float(t.item())
-        return elapsed_ms, launch_ms
+        replicas.barrier()
+        return replicas.max_over_ranks(elapsed_ms), launch_ms
 
     # which solve each mode runs: the plain FP64 solve takes the lane solve from the lane threshold
     # on (three launches: gather, solve, scatter), else the domain solve; the refined solve is the
@@ -455,11 +449,7 @@ def main():
         t0 = time.perf_counter()
         for _ in range(reps):
             factor.solve_many_into(bn, xn)
-        dt = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([dt], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = replicas.max_over_ranks(time.perf_counter() - t0)
         t = factor.timings()
         e2e_err = float(max(np.abs(xn[k] - c).max() / np.abs(c).max() for k, c in zip(sample, cpu)))
         line["e2e"] = {"value": world * count * reps / dt, "unit": UNIT, "h2d_bytes_per_step": int(rhs.nbytes),
