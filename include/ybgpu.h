@@ -192,11 +192,13 @@ int32_t yb_factor_set_domain(yb_factor *f, int32_t precision, int32_t warps, int
  * cost model's cycles per tile; YB_ERROR_INVALID_ARGUMENT if that choice is not the domain solve. */
 int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_t *tile_width, int32_t *cut, int32_t *top_rows,
                               int64_t *records, int64_t *bytes, int64_t *smem_bytes, double *model_cycles);
-/* No ybus counterpart: the autotuner. Times the domain solve of `count` right-hand sides for a
- * precision over its shapes (warps 8/12/16, pages 1536/2048 bytes, 2 or 3 pages in flight, the
- * widest tile that fits and half of it) and keeps the fastest for the factor; config receives
- * {kind, tile width, warps, ring, page bytes} and best_ms its time (either may be NULL). With no
- * domain solve to tune, the configuration is left as it was. */
+/* No ybus counterpart: the autotuner. Times the solve of `count` right-hand sides for a precision
+ * over the domain solve's shapes (warps 8/12/16, pages 1536/2048 bytes, 2 or 3 pages in flight, the
+ * widest tile that fits and half of it) and the lane solve's (4, 6 or 8 warps per block, when the
+ * factor admits a lane layout) and keeps the fastest for the factor, for solves of about that many
+ * right-hand sides. config receives {kind, tile width (0 for the lane solve), warps, ring, page
+ * bytes} and best_ms its time (either may be NULL). With nothing to time, the configuration is left
+ * as it was. */
 int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t count, int32_t *config, double *best_ms);
 /* No ybus counterpart, diagnostics on the host (no GPU needed): the lane solve's layout for a
  * Cholesky factor given as to yb_factor_from_cholesky, values of `value_bytes` (8 or 4), `warps`

@@ -1248,6 +1248,18 @@ extern "C" int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t c
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
     cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+    // times one configuration (a warm-up, then the mean of three solves) and keeps the fastest
+    auto time_config = [&](const TileConfig &run) {
+      t = run;
+      solve_device(f, b.get(), n, x.get(), n, count, precision, s);
+      cuda_check(cudaEventRecord(e0, s), "cudaEventRecord");
+      for (int rep = 0; rep < 3; ++rep) solve_device(f, b.get(), n, x.get(), n, count, precision, s);
+      cuda_check(cudaEventRecord(e1, s), "cudaEventRecord");
+      cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+      float ms = 0;
+      cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+      if (ms / 3 < best_time) best_time = ms / 3, best = run;
+    };
     const int warps_list[] = {8, 12, 16}, page_list[] = {1536, 2048}, ring_list[] = {2, 3};
     for (int warps : warps_list)
       for (int page : page_list)
@@ -1265,23 +1277,28 @@ extern "C" int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t c
           for (int w = r.width; w >= 1 && w >= r.width / 2; w /= 2) {
             TileConfig run = r;
             run.width = w;
-            t = run;
-            solve_device(f, b.get(), n, x.get(), n, count, precision, s);  // warm-up
-            cuda_check(cudaEventRecord(e0, s), "cudaEventRecord");
-            for (int rep = 0; rep < 3; ++rep) solve_device(f, b.get(), n, x.get(), n, count, precision, s);
-            cuda_check(cudaEventRecord(e1, s), "cudaEventRecord");
-            cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
-            float ms = 0;
-            cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-            if (ms / 3 < best_time) best_time = ms / 3, best = run;
+            time_config(run);
           }
         }
+    // the lane solve, when the factor admits it, at 4, 6 and 8 warps per block
+    for (int warps : {4, 6, 8}) {
+      TileConfig run = saved;
+      run.kind = kTileLane, run.lane_warps = warps, run.lane_page = 0;
+      DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, run, s) : lane_pick<float>(f, run, s);
+      if (!d || d->warps != warps) continue;  // none, or the block took fewer warps (timed on its own)
+      time_config(run);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     t = std::isfinite(best_time) ? best : saved;
     if (config) {
-      config[0] = t.kind, config[1] = t.width, config[2] = t.domain_warps, config[3] = t.domain_ring,
-      config[4] = t.domain_page;
+      if (t.kind == kTileLane) {
+        DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, t, s) : lane_pick<float>(f, t, s);
+        config[0] = t.kind, config[1] = 0, config[2] = t.lane_warps, config[3] = kLaneRing, config[4] = d->page_bytes;
+      } else {
+        config[0] = t.kind, config[1] = t.width, config[2] = t.domain_warps, config[3] = t.domain_ring,
+        config[4] = t.domain_page;
+      }
     }
     if (best_ms) *best_ms = best_time;
     return YB_OK;

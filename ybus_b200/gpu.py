@@ -255,7 +255,7 @@ class GpuFactor:
         _check(lib().yb_factor_set_lane_min_count(self._h, precision, min_count))
 
     def autotune(self, precision: int = FP64, count: int = 2048) -> dict:
-        """Times the domain solve's shapes on `count` right-hand sides and keeps the fastest."""
+        """Times the domain and lane solves' shapes on `count` right-hand sides and keeps the fastest."""
         cfg = np.zeros(5, np.int32)
         ms = C.c_double()
         _check(lib().yb_factor_autotune(self._h, precision, count, ptr(cfg), C.byref(ms)))
