@@ -167,7 +167,7 @@ int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t *info);
  * which three blocks fit an SM). */
 int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32_t page_bytes);
 /* No ybus counterpart: the number of right-hand sides from which the automatic choice takes the
- * lane solve (default 8192). */
+ * lane solve (default 4096). */
 int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t min_count);
 /* No ybus counterpart: the streamed solve's shape for a precision: warps per block (1..16), pages
  * in flight per warp (2..16), page bytes (512..16384, a multiple of 16), and the row count under
