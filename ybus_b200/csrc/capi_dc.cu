@@ -486,6 +486,8 @@ struct yb_dc_adjoint {
   DeviceArray<double> p, limits, theta, g, lambda, flows, loss_part, gb_part, grad_b;
   DeviceArray<int32_t> inc_ptr, inc_branch;
   DeviceArray<double> inc_value;
+  DeviceArray<int32_t> unknown;  // per bus: its unknown, -1 for the slack
+  DeviceArray<double> grad_p;    // dL/dp by bus, count x n_bus
 };
 
 namespace {
@@ -558,6 +560,16 @@ __global__ void grad_b_reduce_kernel(const double *__restrict__ gb_part, int32_t
   grad_b[l] = s;
 }
 
+// dL/dp by bus: lambda's entry of the bus's unknown, 0 at the slack
+__global__ void grad_p_kernel(const double *__restrict__ lambda, int64_t n, const int32_t *__restrict__ unknown,
+                              int64_t n_bus, int64_t total, double *__restrict__ grad_p) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= total) return;
+  const int64_t r = k / n_bus, i = k - r * n_bus;
+  const int32_t u = unknown[i];
+  grad_p[k] = u < 0 ? 0.0 : lambda[r * n + u];
+}
+
 }  // namespace
 
 extern "C" int32_t yb_dc_adjoint_new(yb_dc_network *net, int64_t count, yb_dc_adjoint **out) {
@@ -586,6 +598,8 @@ extern "C" int32_t yb_dc_adjoint_new(yb_dc_network *net, int64_t count, yb_dc_ad
     adj->inc_ptr.upload(ptr, s);
     adj->inc_branch.upload(br.empty() ? std::vector<int32_t>{0} : br, s);
     adj->inc_value.upload(val.empty() ? std::vector<double>{0.0} : val, s);
+    std::vector<int32_t> unknown(net->unknown.begin(), net->unknown.end());
+    adj->unknown.upload(unknown, s);
     adj->p.resize((size_t)(net->n_bus * count));
     adj->limits.resize((size_t)nl);
     adj->theta.resize((size_t)(n * count));
@@ -661,20 +675,20 @@ extern "C" int32_t yb_dc_adjoint_backward(yb_dc_adjoint *adj, double *grad_injec
     grad_b_reduce_kernel<<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(adj->gb_part.get(), (int32_t)nl, chunks,
                                                                       adj->grad_b.get());
     cuda_check(cudaGetLastError(), "grad_b_reduce_kernel launch");
-    std::vector<double> lam;
     if (grad_injections) {
-      lam.resize((size_t)(n * count));
-      cuda_check(cudaMemcpyAsync(lam.data(), adj->lambda.get(), sizeof(double) * n * count, cudaMemcpyDeviceToHost, s),
-                 "download lambda");
+      // dL/dp in bus order on the device, then one copy into the caller's array
+      const int64_t total = net->n_bus * count;
+      adj->grad_p.reserve((size_t)total);
+      grad_p_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(adj->lambda.get(), n, adj->unknown.get(), net->n_bus,
+                                                                   total, adj->grad_p.get());
+      cuda_check(cudaGetLastError(), "grad_p_kernel launch");
+      cuda_check(cudaMemcpyAsync(grad_injections, adj->grad_p.get(), sizeof(double) * total, cudaMemcpyDeviceToHost, s),
+                 "download dL/dp");
     }
     if (grad_susceptance)
       cuda_check(cudaMemcpyAsync(grad_susceptance, adj->grad_b.get(), sizeof(double) * nl, cudaMemcpyDeviceToHost, s),
                  "download dL/db");
     cuda_check(cudaStreamSynchronize(s), "adjoint backward");
-    if (grad_injections)
-      for (int64_t r = 0; r < count; ++r)
-        for (int64_t i = 0; i < net->n_bus; ++i)
-          grad_injections[r * net->n_bus + i] = net->unknown[i] < 0 ? 0.0 : lam[r * n + net->unknown[i]];
     return YB_OK;
   });
 }

@@ -122,8 +122,14 @@ class FlowLoss:
         _check(lib().yb_dc_adjoint_forward(self._h, ptr(p), ptr(lim), float(margin), C.byref(loss), ptr(f)))
         return (loss.value, f) if flows else loss.value
 
-    def backward(self):
-        gp = np.zeros((self.count, self.net.n_bus))
-        gb = np.zeros(self.net.n_branch)
+    def backward(self, grad_injections=None, grad_susceptance=None):
+        """(dL/dp, dL/db); either may be given as a caller's float64 array of the right shape
+        (pinned host memory, for instance) to receive it."""
+        gp = np.zeros((self.count, self.net.n_bus)) if grad_injections is None else grad_injections
+        gb = np.zeros(self.net.n_branch) if grad_susceptance is None else grad_susceptance
+        if gp.shape != (self.count, self.net.n_bus) or gp.dtype != np.float64 or not gp.flags.c_contiguous:
+            raise ValueError("dL/dp is a contiguous float64 (count, n_bus) array")
+        if gb.shape != (self.net.n_branch,) or gb.dtype != np.float64:
+            raise ValueError("dL/db is a float64 array over the branches")
         _check(lib().yb_dc_adjoint_backward(self._h, ptr(gp), ptr(gb)))
         return gp, gb
