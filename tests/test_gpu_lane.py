@@ -130,3 +130,29 @@ def test_a_factor_with_too_many_live_values_takes_another_solve(gpu):
     with pytest.raises(CudaError):
         factor.lane_info(FP64)
     assert worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs)) < BAR
+
+
+def test_a_block_larger_than_one_launch_of_work(gpu):
+    # 27,000 right-hand sides of the 10,000-bus grid need 2.2 GB of work array, over the 2 GB one
+    # launch fills: two launches, checked on both sides of their boundary
+    import torch
+    g = grids.make_grid(10000, 3500, grids.SEED_BASE + 2)
+    r, c, v = grids.bbus_triplets(g)
+    keep = np.arange(1, 10000)
+    chol = host.cholesky(host.Matrix.from_triplets(10000, 10000, r, c, v).select(keep, keep))
+    count = 27000
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    b = torch.randn((count, chol.n), dtype=torch.float64, device="cuda", generator=gen)
+    x = torch.full_like(b, float("nan"))
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.set_tile_kind(FP64, LANE)
+    factor.solve_many_device(b.data_ptr(), x.data_ptr(), count, FP64, None)
+    gpu.synchronize()
+    factor.check_error()
+    per_launch = (2 << 30) // (chol.n * 32 * 8) * 32  # right-hand sides one launch takes
+    assert per_launch < count
+    sample = np.unique(np.r_[0, 1, per_launch - 1, per_launch, per_launch + 1, count - 1, np.arange(5, count, 1777)])
+    idx = torch.from_numpy(sample).cuda()
+    bs, xs = b[idx].cpu().numpy(), x[idx].cpu().numpy()
+    assert not np.isnan(xs).any()
+    assert worst_relative_difference(xs, orc.solve_many(chol, bs, threads=8)) < BAR
