@@ -1,5 +1,4 @@
-"""The adjoint of the flow loss Σ softplus(|f| − 0.8·limit)² (BASELINE's differentiation workload,
-on the synthetic 2,000-bus grid): the GPU's loss and gradients with respect to the injections
+"""The adjoint of the flow loss Σ softplus(|f| − 0.8·limit)² on the synthetic 2,000-bus grid: the GPU's loss and gradients with respect to the injections
 and the branch susceptances against the CPU's, computed from the oracle's solves and transposed
 solve, and against central finite differences (h = 1e-6) at random coordinates."""
 import numpy as np
