@@ -461,6 +461,17 @@ def main():
                        "max_rel_err_vs_oracle": e2e_err, "chunks_per_step": t.blocks // reps,
                        "stage_ms_per_step": {"upload": t.upload / reps * 1e3, "solve": t.solve / reps * 1e3,
                                              "download": t.download / reps * 1e3}}
+    if world == 1 and not a.no_e2e:
+        # for comparison: ybus_cuda's own route to the solve (cuSPARSE SpSM, lower then upper, in
+        # blocks), on the same factor and device arrays; its best block width of 64, 256 and 1024
+        spsm = {}
+        for width in (64, 256, 1024):
+            factor.reference_spsm_solve_device(d_b.data_ptr(), d_x.data_ptr(), count, width)
+            spsm[width] = factor.reference_spsm_solve_device(d_b.data_ptr(), d_x.data_ptr(), count, width)
+        width = min(spsm, key=spsm.get)
+        line["reference_gpu_spsm"] = {"value": count / (spsm[width] / 1e3), "unit": UNIT, "ms_per_step": spsm[width],
+                                      "width": width, "ms_by_width": spsm,
+                                      "route": "cuSPARSE SpSM lower + upper on CSR triangles (ybus_cuda's Block::solve)"}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(chol, rhs)
     if rank == 0:

@@ -377,6 +377,15 @@ int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rhs, int64_t 
                                      int64_t count, int32_t max_steps, double tolerance, double *d_ratio,
                                      int32_t *d_steps, void *stream);
 
+/* For comparison only, not a solve path of this library: ybus_cuda's own route to the solve
+ * (`Block::solve`, ybus_cuda/src/sparse.rs:371-420: cuSPARSE SpSM on the lower, then the upper
+ * triangle as CSR, blocks of `width` right-hand sides, the last block padded with zeros), on a
+ * Cholesky factor and device arrays as yb_solve_many_device takes them, the permutations applied on
+ * the device. cuSPARSE is opened at the first call (YB_ERROR_INVALID_ARGUMENT without it). solve_ms
+ * (may be NULL) receives the time of the solves, their analysis excluded. */
+int32_t yb_reference_spsm_solve(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
+                                int64_t count, int64_t width, double *solve_ms);
+
 /* No counterpart in ybus. The device-array solve for callers that must not have the library
  * allocate device memory: programs whose own pool allocator has reserved the GPU's memory (so a
  * cudaMalloc from here could fail or fragment their pool) and latency-bound loops that cannot take

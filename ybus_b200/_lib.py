@@ -79,6 +79,7 @@ SIGNATURES: dict[str, tuple] = {
     "yb_factor_set_tail_level": (i32, [vp, i32, i32]),
     "yb_factor_set_domain": (i32, [vp, i32, i32, i32, i32, i32]),
     "yb_factor_autotune": (i32, [vp, i32, i64, vp, P_dbl]),
+    "yb_reference_spsm_solve": (i32, [vp, vp, i64, vp, i64, i64, i64, P_dbl]),
     "yb_factor_lane_info": (i32, [vp, i32, vp]),
     "yb_factor_set_lane_min_count": (i32, [vp, i32, i64]),
     "yb_factor_set_lane": (i32, [vp, i32, i32, i32]),

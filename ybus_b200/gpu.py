@@ -237,6 +237,14 @@ class GpuFactor:
         return {"tile": w.value, "cut": cut.value, "top": top.value, "records": rec.value, "bytes": by.value,
                 "smem": sm.value, "model_cycles": cyc.value}
 
+    def reference_spsm_solve_device(self, d_rhs: int, d_out: int, count: int, width: int = 1024) -> float:
+        """For comparison only: ybus_cuda's route (cuSPARSE SpSM, lower then upper, blocks of
+        `width`) on this factor's device arrays. Returns the solves' time in ms."""
+        n = self.dim()
+        ms = C.c_double()
+        _check(lib().yb_reference_spsm_solve(self._h, d_rhs, n, d_out, n, count, width, C.byref(ms)))
+        return ms.value
+
     def lane_info(self, precision: int = FP64) -> dict:
         """The lane solve's layout: slots, pages, peaks of live values, shared memory per block,
         warps per block, domains, top rows and partial values per block."""
