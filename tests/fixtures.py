@@ -51,6 +51,20 @@ def random_spd(n: int, fill_percent: int, seed: int) -> host.Matrix:
     return host.Matrix.from_triplets(n, n, r, c, v, by_rows=True)
 
 
+def star_spd(n: int) -> host.Matrix:
+    """A diagonally dominant star: row 0 coupled to every other row, no other couplings."""
+    r, c, v = [], [], []
+    hub = 1.0
+    for i in range(1, n):
+        w = -(1.0 + (i % 7) / 7.0)
+        r += [0, i, i]
+        c += [i, 0, i]
+        v += [w, w, 2.0 - w]
+        hub -= w
+    r.append(0), c.append(0), v.append(hub)
+    return host.Matrix.from_triplets(n, n, r, c, v, by_rows=True)
+
+
 def random_square(n: int, fill_percent: int, seed: int) -> host.Matrix:
     """A pseudo-random unsymmetric matrix with a small diagonal, so the LU pivots off it (CSC)."""
     rng = Lcg(seed)

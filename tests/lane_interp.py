@@ -6,7 +6,7 @@ import numpy as np
 
 FWD_ROW0, FWD_ROWN, FWD_MORE = 0, 5, 6
 BWD_ROW0, BWD_ROWN, BWD_BEGIN, BWD_MORE, BWD_END = 7, 12, 13, 14, 15
-PREFETCH, PHASE, PARTIALS, FLUSH, IMPORT, BARRIER, END, PAGE_END = range(16, 24)
+PREFETCH, PHASE, TOP_SUM, FLUSH, IMPORT, BARRIER, END, PAGE_END = range(16, 24)
 RING, BATCH = 8, 4
 
 
@@ -87,9 +87,10 @@ def warp_steps(lay, warp, work, partial, lanes):
         elif kind == PHASE:
             assert not pending.any(), "a phase that leaves prefetched rows unread"
             ring[:] = np.nan
-        elif kind == PARTIALS:
+        elif kind == TOP_SUM:
+            assert 0 <= w < work.shape[0], "a row outside the work array"
             for k in words:
-                live[s] = live[s] + partial[k // row]
+                work[w] = work[w] + partial[k // row]
         elif kind == FLUSH:
             for k, o in zip(words, offs):
                 partial[k // row] = live[o // row]
@@ -114,7 +115,7 @@ def run(lay, n, rhs):
     work[lay["in_pos"]] = rhs.T
     partial = np.zeros((max(lay["partials"], 1), lanes))
     warps = [warp_steps(lay, w, work, partial, lanes) for w in range(lay["warps"])]
-    for _ in range(3):  # the epochs between the two barriers
+    for _ in range(4):  # the epochs around the three barriers
         for g in warps:
             next(g, None)
     return work[lay["out_pos"]].T.copy()

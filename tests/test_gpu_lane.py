@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle.oracle as orc
-from fixtures import random_spd, random_square, right_hand_sides, worst_relative_difference
+from fixtures import random_spd, random_square, right_hand_sides, star_spd, worst_relative_difference
 from ybus_b200 import FP32, FP64, CudaError, GpuFactor, grids, host
 
 pytestmark = pytest.mark.gpu
@@ -40,6 +40,22 @@ def test_dense_columns_over_several_records(gpu, warps):
     assert info["slots"] >= 1 and info["pages"] >= 1 and info["page_bytes"] == 512
     d = worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs))
     assert d < BAR, f"{d:e}"
+
+
+@pytest.mark.parametrize("prec,bar", [(FP64, BAR), (FP32, 1e-4)])
+def test_a_top_row_with_partials_over_several_records(gpu, prec, bar):
+    # a star: 199 one-row domains update the hub, the one top row; on 256-byte pages its partial
+    # sums take several records in a row, run by one warp
+    chol = host.cholesky(star_spd(200))
+    rhs = right_hand_sides(200, 70, 5)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.set_tile_kind(prec, LANE)
+    factor.set_lane(prec, 8, 256)
+    info = factor.lane_info(prec)
+    assert info["top"] >= 1 and info["partials"] > 14
+    d = worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs))
+    assert d < bar, f"{d:e}"
+    factor.check_error()
 
 
 def test_device_arrays_with_leading_dimensions_and_fp32(gpu):

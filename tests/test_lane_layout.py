@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle.oracle as orc
-from fixtures import random_spd, right_hand_sides, worst_relative_difference
+from fixtures import random_spd, right_hand_sides, star_spd, worst_relative_difference
 from lane_interp import run
 from ybus_b200 import YbError, grids, host
 
@@ -65,3 +65,13 @@ def test_a_single_row_and_a_diagonal_matrix():
             rhs = right_hand_sides(n, 3, 2)
             lay = host.lane_layout(chol, 8, 512, warps=warps)
             assert worst_relative_difference(run(lay, n, rhs), orc.solve_many(chol, rhs)) < 1e-12
+
+
+def test_a_top_row_with_more_partials_than_a_record_holds():
+    # a star: every leaf is a domain of its own and the hub, the one top row, takes a partial from
+    # each; on 256-byte pages its sums span several records, each adding into what the last stored
+    chol = host.cholesky(star_spd(200))
+    rhs = right_hand_sides(200, 4, 3)
+    lay = host.lane_layout(chol, 8, 256, warps=8)
+    assert lay["top"] >= 1 and lay["partials"] > 14
+    assert worst_relative_difference(run(lay, 200, rhs), orc.solve_many(chol, rhs)) < 1e-12

@@ -16,8 +16,10 @@
 //
 // Forward, right-looking: at row j, z_j = (b_j + acc_j) * dinv_j, acc_j read and zeroed, then for
 // every later row r that reads j, acc_r -= L_rj z_j. A domain's updates of top rows gather in its
-// warp's slots and go to the block's partial array when the domain ends (a flush); the top warp
-// adds a top row's partials, in a fixed order, before the row. Backward, left-looking, rows in
+// warp's slots and go to the block's partial array when the domain ends (a flush); once every
+// domain has ended, the warps add each top row's partials, in a fixed order, into the row's right-
+// hand side in the work array (the top rows dealt to the warps by their count of partials), so the
+// top warp's chain of rows waits on no partial. Backward, left-looking, rows in
 // reverse order: x_j = (z_j - sum of U_jc x_c) * dinv_j, x_j kept in a slot while rows still to
 // come read it; a domain first imports the top solutions its rows read from the work array.
 #include <algorithm>
@@ -112,6 +114,19 @@ template <class T> struct PageWriter {
     start = first, len = rows, step = backward ? -1 : 1, row_i = 0;
     prefetch(0);
     prefetch(1);
+  }
+  // A top row's partial sums: work row `row` += the partial rows `w`, split as the pages need (the
+  // records of one row run in order, each adding into what the one before stored).
+  void sums(uint32_t row, const std::vector<std::pair<T, uint32_t>> &entries, const std::vector<uint32_t> &w) {
+    size_t done = 0;
+    while (done < entries.size()) {
+      const size_t take = std::min(most_entries(), entries.size() - done);
+      room(bytes_of(take));
+      put(0, kLaneTopSum, (uint32_t)take, row, nullptr, 0);
+      entries_at(at(), entries, w.data(), done, take);
+      pos += bytes_of(take);
+      done += take;
+    }
   }
   // Records with entries {a 32-bit word in val's place, offset}, split as the pages need.
   void words(uint32_t kind, uint32_t self, const std::vector<std::pair<T, uint32_t>> &entries,
@@ -335,6 +350,23 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
     }
     lay.partials = (int32_t)k;
   }
+  // the top rows with partials, dealt to the warps by their count of partials (largest first, each
+  // to the warp with the fewest so far), each warp's share in position order
+  std::vector<std::vector<int32_t>> top_sums(warps);
+  {
+    std::vector<int32_t> rows;
+    for (int32_t p = top0; p < n; ++p)
+      if (!contributors[at[p]].empty()) rows.push_back(at[p]);
+    std::stable_sort(rows.begin(), rows.end(),
+                     [&](int32_t a, int32_t b) { return contributors[a].size() > contributors[b].size(); });
+    std::vector<size_t> load(warps, 0);
+    for (int32_t j : rows) {
+      const int32_t w = (int32_t)(std::min_element(load.begin(), load.end()) - load.begin());
+      load[w] += 1 + contributors[j].size();
+      top_sums[w].push_back(j);
+    }
+    for (auto &t : top_sums) std::sort(t.begin(), t.end(), [&](int32_t a, int32_t b) { return newpos[a] < newpos[b]; });
+  }
   const uint32_t row_bytes = 32u * (uint32_t)sizeof(T);  // a live slot, or a work or partial row
   auto off = [&](int32_t s) { return (uint32_t)s * row_bytes; };
   auto self_of = [&](int32_t s) { return (uint32_t)s * row_bytes / 16; };  // headers hold slot offsets / 16
@@ -405,20 +437,17 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
       peak_f = std::max(peak_f, slots.peak);
     }
     pw.simple(kLaneBarrier);
+    for (int32_t j : top_sums[w]) {  // this warp's share of the top rows' partial sums
+      entries.assign(contributors[j].size(), {T(0), 0u});
+      words.clear();
+      for (uint32_t k : contributors[j]) words.push_back(k * row_bytes);
+      pw.sums((uint32_t)newpos[j] * row_bytes, entries, words);
+    }
+    pw.simple(kLaneBarrier);
     if (w == 0 && top0 < n) {  // the top, forward then backward
       Slots slots;
       pw.phase(top0, n - top0, false);
-      for (int32_t p = top0; p < n; ++p) {
-        const int32_t j = at[p];
-        if (!contributors[j].empty()) {
-          if (acc[j] < 0) acc[j] = slots.take();
-          entries.assign(contributors[j].size(), {T(0), 0u});
-          words.clear();
-          for (uint32_t k : contributors[j]) words.push_back(k * row_bytes);
-          pw.words(kLanePartials, self_of(acc[j]), entries, words);
-        }
-        forward_rows(pw, slots, p, p);
-      }
+      forward_rows(pw, slots, top0, n - 1);
       peak_f = std::max(peak_f, slots.peak);
       Slots bslots;
       for (int32_t p = top0; p < n; ++p)

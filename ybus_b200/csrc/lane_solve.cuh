@@ -4,7 +4,8 @@
 // need no barriers, no reductions across lanes and no divergence. The warps of a block take
 // different subtree domains of the elimination tree on the same 32 right-hand sides; warp 0 takes
 // the top above them between two block barriers, with the domains' updates of top rows handed over
-// through a partial array and the top's solutions handed back through the work array (LaneLayout in
+// through a partial array (which all warps add into the top rows' right-hand sides between the
+// first two barriers) and the top's solutions handed back through the work array (LaneLayout in
 // plan.hpp). The order keeps a few tens of values alive per lane, in shared memory; the right-hand
 // sides, the forward results and the solutions stream through the work array in HBM laid out
 // [group][position][lane], so every row a warp reads or writes is one contiguous 32-value line.
@@ -25,7 +26,7 @@
 
 namespace yb {
 
-constexpr int kLaneBarriers = 2;             // block barriers in every warp's stream
+constexpr int kLaneBarriers = 3;             // block barriers in every warp's stream
 constexpr int kLaneMaxWarps = 8;             // warps per block at most
 
 struct LaneArgs {
@@ -236,15 +237,23 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
         cp_async_wait<0>();
         __threadfence();  // the rows this lane stored are what the phase's copies read
         break;
-      case kLanePartials: {
-        T acc = lane_at<T>(self);
-        for (uint32_t c = 0; c < count; ++c) {
-          T v;
-          uint32_t w, o;
-          lane_entry(e + c * E, v, w, o);
-          acc += *reinterpret_cast<const T *>(part_lane + w);
+      case kLaneTopSum: {  // the row and up to four partials in flight at a time, added in order
+        T *row = reinterpret_cast<T *>(w_lane + h.y);
+        T acc = *row;
+        for (uint32_t c = 0; c < count; c += 4) {
+          T p[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            T v;
+            uint32_t w, o;
+            lane_entry(e + min(c + q, count - 1) * E, v, w, o);
+            p[q] = *reinterpret_cast<const T *>(part_lane + w);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (c + q < count) acc += p[q];
         }
-        lane_at<T>(self) = acc;
+        *row = acc;
         break;
       }
       case kLaneFlush:
@@ -256,12 +265,20 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
           lane_at<T>(live + o) = T(0);
         }
         break;
-      case kLaneImport:
-        for (uint32_t c = 0; c < count; ++c) {
-          T v;
-          uint32_t w, o;
-          lane_entry(e + c * E, v, w, o);
-          lane_at<T>(live + o) = *reinterpret_cast<const T *>(w_lane + w);
+      case kLaneImport:  // four loads in flight at a time
+        for (uint32_t c = 0; c < count; c += 4) {
+          T x[4];
+          uint32_t o[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            T v;
+            uint32_t w;
+            lane_entry(e + min(c + q, count - 1) * E, v, w, o[q]);
+            x[q] = *reinterpret_cast<const T *>(w_lane + w);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (c + q < count) lane_at<T>(live + o[q]) = x[q];
         }
         break;
       case kLaneBarrier:

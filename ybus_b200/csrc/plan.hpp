@@ -142,8 +142,9 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
 // The factor for the lane solve (lane_solve.cuh: one right-hand side per lane, every lane of a warp
 // taking the same rows, `warps` warps per block of 32 right-hand sides). The rows are in a postorder
 // of the forward elimination forest with larger subtrees first, cut into subtree domains (dealt to
-// the warps) under a top (taken by warp 0 between two block barriers); each warp's part is one
-// stream of records in fixed-size pages.
+// the warps) under a top (taken by warp 0 between the second and third block barriers; between the
+// first and second, every warp adds the domains' partial sums of a share of the top rows into their
+// right-hand sides); each warp's part is one stream of records in fixed-size pages.
 //
 // A record is a 16-byte header, then `count` entries of 16 bytes (FP64) or 8 (FP32): {T val, or a
 // 32-bit word in its place; uint32 offset}. The header: uint32 {self (16 bits), kind (5 bits), ring
@@ -162,9 +163,9 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
 //   kLanePhase: a new run of rows: earlier copies are finished and this lane's stores are visible
 //     to its copies.
 //   kLaneFlush: per entry, the partial row `word` takes slot `offset`, which is zeroed.
-//   kLanePartials: slot self += the partial rows `word` of its entries, in order.
+//   kLaneTopSum: the work row `word` += the partial rows of its entries' words, in order.
 //   kLaneImport: per entry, slot `offset` takes the work row `word`.
-//   kLaneBarrier: a block barrier (every warp's stream has two); kLaneEnd ends the stream;
+//   kLaneBarrier: a block barrier (every warp's stream has three); kLaneEnd ends the stream;
 //   kLanePageEnd ends its page (every page has one).
 enum LaneKind : uint32_t {
   kLaneFwdRow0 = 0,  // .. kLaneFwdRow0 + 4
@@ -177,7 +178,7 @@ enum LaneKind : uint32_t {
   kLaneBwdEnd = 15,
   kLanePrefetch = 16,
   kLanePhase = 17,
-  kLanePartials = 18,
+  kLaneTopSum = 18,
   kLaneFlush = 19,
   kLaneImport = 20,
   kLaneBarrier = 21,
