@@ -11,7 +11,7 @@ RING, BATCH = 8, 4
 
 
 def records(lay, warp):
-    """Yields (kind, ring, self, count, word, tail, vals, words, offsets) for each record of a warp."""
+    """Yields (kind, ring, self, count, word, tail, vals, words, offsets, body) for each record of a warp."""
     pb, vb = lay["page_bytes"], lay["value_bytes"]
     ftype = np.float64 if vb == 8 else np.float32
     entry = 16 if vb == 8 else 8
@@ -32,7 +32,7 @@ def records(lay, warp):
             vals = np.array([body[e * entry:e * entry + vb].view(ftype)[0] for e in range(count)], np.float64)
             words = np.array([body[e * entry:e * entry + 4].view(np.uint32)[0] for e in range(count)], np.int64)
             offs = np.array([body[e * entry + vb:e * entry + vb + 4].view(np.uint32)[0] for e in range(count)], np.int64)
-            yield kind, ring, self_, count, word, tail, vals, words, offs
+            yield kind, ring, self_, count, word, tail, vals, words, offs, body
             if kind == END:
                 return
             pos += 16 + ((count * entry + 15) & ~15)
@@ -47,7 +47,7 @@ def warp_steps(lay, warp, work, partial, lanes):
     ring = np.full((RING, lanes), np.nan)
     pending = np.zeros(RING, bool)  # a prefetched row not read yet
     z = None
-    for kind, rs, self_, count, word, tail, vals, words, offs in records(lay, warp):
+    for kind, rs, self_, count, word, tail, vals, words, offs, body in records(lay, warp):
         s, w = self_ * 16 // row, word // row
         if kind <= BWD_END:
             dinv = float(tail[:vb].view(ftype)[0])
@@ -78,11 +78,13 @@ def warp_steps(lay, warp, work, partial, lanes):
                 work[w] = x
         elif kind == PREFETCH:
             flags = int(tail[:4].view(np.uint32)[0])
-            step, base = (-1 if flags & 1 else 1), (BATCH if flags & 2 else 0)
+            base = BATCH if flags & 2 else 0
+            assert len(body) == 16 and self_ <= BATCH
+            rows = body.view(np.uint32) // row
             for q in range(self_):
                 assert not pending[base + q], "a prefetch over a row not read yet"
-                assert 0 <= w + q * step < work.shape[0], "a prefetch outside the work array"
-                ring[base + q] = work[w + q * step]
+                assert 0 <= rows[q] < work.shape[0], "a prefetch outside the work array"
+                ring[base + q] = work[rows[q]]
                 pending[base + q] = True
         elif kind == PHASE:
             assert not pending.any(), "a phase that leaves prefetched rows unread"

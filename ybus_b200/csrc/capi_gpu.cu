@@ -709,12 +709,12 @@ void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, doub
   for (int64_t g0 = 0; g0 < groups_all; g0 += per_launch) {
     const int64_t groups = std::min(per_launch, groups_all - g0);
     const int64_t cols = std::min(count - g0 * 32, groups * 32);
-    const dim3 io_grid((unsigned)((n + 63) / 64), (unsigned)std::min<int64_t>(groups, 65535));
-    lane_in_kernel<T><<<io_grid, 256, 0, stream>>>(b + g0 * 32 * ldb, ldb, cols, (int32_t)n, groups, d->in_pos.get(), work);
+    const unsigned io_grid = (unsigned)lane_io_blocks(groups, n);
+    lane_in_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(b + g0 * 32 * ldb, ldb, cols, (int32_t)n, groups, d->in_pos.get(), work);
     cuda_check(cudaGetLastError(), "lane_in_kernel launch");
     lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
     cuda_check(cudaGetLastError(), "lane_solve_kernel launch");
-    lane_out_kernel<T><<<io_grid, 256, 0, stream>>>(work, cols, (int32_t)n, groups, d->out_pos.get(), x + g0 * 32 * ldx, ldx);
+    lane_out_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(work, cols, (int32_t)n, groups, d->out_pos.get(), x + g0 * 32 * ldx, ldx);
     cuda_check(cudaGetLastError(), "lane_out_kernel launch");
   }
 }

@@ -57,15 +57,19 @@ struct Slots {
 // Writes one warp's records into fixed-size pages. Every page ends with a kLanePageEnd record (room
 // for it is always kept); a record never straddles a page, and a record whose entries do not fit one
 // page continues in the next records. The writer follows the phase (first position, direction and
-// length) so that each row record carries its work-row offset and prefetch-ring slot, and puts a
-// kLanePrefetch record before every kLaneBatch rows.
+// length) so that each row record carries its work-row offset (the work row of the row at position
+// p is work_row[p]) and prefetch-ring slot, and puts a kLanePrefetch record, with the offsets of the
+// rows it copies, before every kLaneBatch rows.
 template <class T> struct PageWriter {
   static constexpr uint32_t kEntry = sizeof(T) == 8 ? 16 : 8, kRow = 32 * sizeof(T);
   int32_t page_bytes;
   std::vector<uint8_t> &blob;
+  const std::vector<int32_t> &work_row;
   size_t pos = 0;
   int32_t start = 0, len = 0, step = 1, row_i = 0;
-  PageWriter(std::vector<uint8_t> &b, int32_t pb) : page_bytes(pb), blob(b) { open(); }
+  PageWriter(std::vector<uint8_t> &b, int32_t pb, const std::vector<int32_t> &wr) : page_bytes(pb), blob(b), work_row(wr) {
+    open();
+  }
   void open() {
     blob.resize(blob.size() + page_bytes, 0);
     pos = 0;
@@ -101,13 +105,16 @@ template <class T> struct PageWriter {
     pos += 16;
   }
   void prefetch(int32_t batch) {
+    static_assert(kLaneBatch == 4, "a prefetch record holds four row offsets");
     const int32_t r0 = batch * kLaneBatch;
     const int32_t count = std::max(0, std::min(kLaneBatch, len - r0));
-    const uint32_t first = count > 0 ? (uint32_t)(start + step * r0) * kRow : 0;
-    const uint32_t flags = (step < 0 ? 1u : 0u) | ((r0 & (kLaneRows - 1)) ? 2u : 0u);
-    room(16);
-    put((uint32_t)count, kLanePrefetch, 0, first, &flags, 4);
-    pos += 16;
+    uint32_t rows[kLaneBatch] = {};
+    for (int32_t q = 0; q < count; ++q) rows[q] = (uint32_t)work_row[start + step * (r0 + q)] * kRow;
+    const uint32_t flags = (r0 & (kLaneRows - 1)) ? 2u : 0u;
+    room(32);
+    put((uint32_t)count, kLanePrefetch, 16 / kEntry, 0, &flags, 4);
+    std::memcpy(at() + 16, rows, 16);
+    pos += 32;
   }
   void phase(int32_t first, int32_t rows, bool backward) {
     simple(kLanePhase);
@@ -146,7 +153,7 @@ template <class T> struct PageWriter {
   void row(uint32_t self, T dinv, const std::vector<std::pair<T, uint32_t>> &entries, bool backward) {
     if (row_i % kLaneBatch == 0 && row_i > 0) prefetch(row_i / kLaneBatch + 1);
     const uint32_t ring = (uint32_t)(row_i & (kLaneRows - 1)) << 5;
-    const uint32_t wpos = (uint32_t)(start + step * row_i) * kRow;
+    const uint32_t wpos = (uint32_t)work_row[start + step * row_i] * kRow;
     ++row_i;
     const size_t count = entries.size();
     uint8_t tail[8] = {};
@@ -327,6 +334,16 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   lay.top = n - top0;
   std::vector<int32_t> at(n);
   for (int32_t v = 0; v < n; ++v) at[newpos[v]] = v;
+  // the work array in b's own row order: row v's right-hand side, forward result and solution sit
+  // in the work row of the row of b that feeds it, so the gather of b and (when b and x share
+  // their permutation) the scatter of x copy whole runs of rows
+  std::vector<int32_t> work_of(n, -1), work_row(n);
+  for (int32_t i = 0; i < n; ++i) {
+    const int32_t v = plan.in_slot[i];
+    if (v < 0 || v >= n || work_of[v] >= 0) throw host::Error(host::kInvalidArgument, "the solve's input order is not a permutation");
+    work_of[v] = i;
+  }
+  for (int32_t p = 0; p < n; ++p) work_row[p] = work_of[at[p]];
   // partials: one per (domain, top row it updates), domains in warp order, top rows by position
   std::vector<std::vector<uint32_t>> contributors(n);
   std::vector<std::vector<std::pair<int32_t, uint32_t>>> domain_partials(domain_range.size());
@@ -417,7 +434,7 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   };
   lay.warp_page.assign(1, 0);
   for (int32_t w = 0; w < warps; ++w) {
-    PageWriter<T> pw(lay.blob, page_bytes);
+    PageWriter<T> pw(lay.blob, page_bytes, work_row);
     const int32_t p0 = warp_start[w], p1 = warp_start[w + 1] - 1;
     {  // forward domains, each ending with its flush
       Slots slots;
@@ -441,7 +458,7 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
       entries.assign(contributors[j].size(), {T(0), 0u});
       words.clear();
       for (uint32_t k : contributors[j]) words.push_back(k * row_bytes);
-      pw.sums((uint32_t)newpos[j] * row_bytes, entries, words);
+      pw.sums((uint32_t)work_of[j] * row_bytes, entries, words);
     }
     pw.simple(kLaneBarrier);
     if (w == 0 && top0 < n) {  // the top, forward then backward
@@ -476,7 +493,7 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
           for (int32_t c : imports) {
             xslot[c] = slots.take();
             entries.push_back({T(0), off(xslot[c])});
-            words.push_back((uint32_t)newpos[c] * row_bytes);
+            words.push_back((uint32_t)work_of[c] * row_bytes);
           }
           pw.words(kLaneImport, 0, entries, words);
         }
@@ -495,8 +512,8 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   lay.in_pos.resize(n);
   lay.out_pos.resize(n);
   for (int32_t i = 0; i < n; ++i) {
-    lay.in_pos[i] = newpos[plan.in_slot[i]];
-    lay.out_pos[i] = newpos[plan.out_slot[i]];
+    lay.in_pos[i] = work_of[plan.in_slot[i]];
+    lay.out_pos[i] = work_of[plan.out_slot[i]];
   }
   return lay;
 }

@@ -8,10 +8,12 @@
 // first two barriers) and the top's solutions handed back through the work array (LaneLayout in
 // plan.hpp). The order keeps a few tens of values alive per lane, in shared memory; the right-hand
 // sides, the forward results and the solutions stream through the work array in HBM laid out
-// [group][position][lane], so every row a warp reads or writes is one contiguous 32-value line.
+// [group][work row][lane], a row's values in the work row of the row of b that feeds it, so every
+// row a warp reads or writes is one contiguous 32-value line.
 //
-// Three launches make a solve: the gather of b (natural rows, column-major) into the work array in
-// solve order, the lane solve in place, and the scatter of the work array into x. Each warp's
+// Three launches make a solve: the gather of b (natural rows, column-major) into the work array,
+// the lane solve in place, and the scatter of the work array into x; with the work rows in b's own
+// row order the gather and scatter are plain transposes of 32-column blocks. Each warp's
 // records stream into its ring of pages by TMA bulk copies (no multicast); the work rows come
 // through a per-warp ring of cp.async copies, a batch of kLaneBatch rows at a time, one to two
 // batches ahead of use.
@@ -219,15 +221,16 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
       case kLaneBwdBegin: z = lane_gather<T>(e, count, lane_at<T>(b_at), live); break;
       case kLaneBwdMore: z = lane_gather<T>(e, count, z, live); break;
       case kLaneBwdEnd: z = lane_gather<T>(e, count, z, live); backward(); break;
-      case kLanePrefetch: {
-        const int64_t step = (h.z & 1u) ? -(int64_t)ROW : (int64_t)ROW;
+      case kLanePrefetch: {  // the batch's work-row offsets follow the header
         const uint32_t dst = smem_s + rows + ((h.z & 2u) ? (uint32_t)kLaneBatch * ROW : 0u);
         const uint32_t nrows = h.x & 0xffffu;
+        const uint4 o = lane_at<uint4>(e);
+        const uint32_t off[kLaneBatch] = {o.x, o.y, o.z, o.w};
 #pragma unroll
         for (int q = 0; q < kLaneBatch; ++q)
           if (q < (int)nrows)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst + q * ROW),
-                         "l"(w_lane + (int64_t)h.y + q * step), "n"(sizeof(T))
+            asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst + q * ROW), "l"(w_lane + off[q]),
+                         "n"(sizeof(T))
                          : "memory");
         cp_async_commit();
         cp_async_wait<1>();
@@ -323,48 +326,90 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
   }
 }
 
-// b (natural rows, column-major, ldb) into the work array [group][position][lane] in solve order;
-// right-hand sides past `count` are zero. Blocks of 256 threads take 64 rows of one group.
-template <class T>
-__global__ void __launch_bounds__(256) lane_in_kernel(const double *__restrict__ b, int64_t ldb, int64_t count, int32_t n,
-                                                      int64_t groups, const int32_t *__restrict__ in_pos,
-                                                      T *__restrict__ work) {
-  __shared__ T tile[64][33];
-  const int i0 = blockIdx.x * 64;
-  for (int64_t g = blockIdx.y; g < groups; g += gridDim.y) {
-    for (int e = threadIdx.x; e < 64 * 32; e += 256) {
-      const int c = e >> 6, q = e & 63, i = i0 + q;
-      const int64_t col = g * 32 + c;
-      tile[q][c] = (i < n && col < count) ? T(b[col * ldb + i]) : T(0);
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < 64 * 32; e += 256) {
-      const int q = e >> 5, c = e & 31, i = i0 + q;
-      if (i < n) work[((size_t)g * n + __ldg(in_pos + i)) * 32 + c] = tile[q][c];
-    }
-    __syncthreads();
+// A lane's work row in 32-byte pieces (256-bit global accesses): 8 for FP64, 4 for FP32.
+__device__ __forceinline__ void lane_row_store(double *row, const double (&v)[32]) {
+#pragma unroll
+  for (int c = 0; c < 32; c += 4)
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(row + c), "d"(v[c]), "d"(v[c + 1]), "d"(v[c + 2]),
+                 "d"(v[c + 3])
+                 : "memory");
+}
+__device__ __forceinline__ void lane_row_store(float *row, const double (&v)[32]) {
+#pragma unroll
+  for (int c = 0; c < 32; c += 8)
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(row + c), "f"((float)v[c]),
+                 "f"((float)v[c + 1]), "f"((float)v[c + 2]), "f"((float)v[c + 3]), "f"((float)v[c + 4]),
+                 "f"((float)v[c + 5]), "f"((float)v[c + 6]), "f"((float)v[c + 7])
+                 : "memory");
+}
+__device__ __forceinline__ void lane_row_load(const double *row, double (&v)[32]) {
+#pragma unroll
+  for (int c = 0; c < 32; c += 4)
+    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(v[c]), "=d"(v[c + 1]), "=d"(v[c + 2]), "=d"(v[c + 3])
+                 : "l"(row + c));
+}
+__device__ __forceinline__ void lane_row_load(const float *row, double (&v)[32]) {
+#pragma unroll
+  for (int c = 0; c < 32; c += 8) {
+    float f[8];
+    asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]), "=f"(f[6]), "=f"(f[7])
+                 : "l"(row + c));
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[c + k] = f[k];
   }
 }
 
-// The work array (solutions in solve order) into x (natural rows, column-major, ldx).
+// The warps of the gather and the scatter: warp w takes rows 32 (w % chunks) + lane of group
+// w / chunks, chunks = ceil(n / 32), each lane one row; blocks of kLaneIoWarps warps.
+constexpr int kLaneIoWarps = 8;
+__host__ __device__ inline int64_t lane_io_blocks(int64_t groups, int64_t n) {
+  return (groups * ((n + 31) / 32) + kLaneIoWarps - 1) / kLaneIoWarps;
+}
+
+// b (natural rows, column-major, ldb) into the work array [group][work row][lane] (b's row i to
+// work row in_pos[i]); right-hand sides past `count` are zero. Each lane reads its row of the
+// group's 32 right-hand sides, one coalesced load across the warp per right-hand side, and stores
+// the whole 32-value work row in 32-byte pieces: no shared memory, no barrier.
 template <class T>
-__global__ void __launch_bounds__(256) lane_out_kernel(const T *__restrict__ work, int64_t count, int32_t n,
-                                                       int64_t groups, const int32_t *__restrict__ out_pos,
-                                                       double *__restrict__ x, int64_t ldx) {
-  __shared__ T tile[64][33];
-  const int i0 = blockIdx.x * 64;
-  for (int64_t g = blockIdx.y; g < groups; g += gridDim.y) {
-    for (int e = threadIdx.x; e < 64 * 32; e += 256) {
-      const int q = e >> 5, c = e & 31, i = i0 + q;
-      tile[q][c] = i < n ? work[((size_t)g * n + __ldg(out_pos + i)) * 32 + c] : T(0);
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < 64 * 32; e += 256) {
-      const int c = e >> 6, q = e & 63, i = i0 + q;
-      const int64_t col = g * 32 + c;
-      if (i < n && col < count) x[col * ldx + i] = (double)tile[q][c];
-    }
-    __syncthreads();
+__global__ void __launch_bounds__(kLaneIoWarps * 32) lane_in_kernel(const double *__restrict__ b, int64_t ldb, int64_t count,
+                                                                   int32_t n, int64_t groups,
+                                                                   const int32_t *__restrict__ in_pos,
+                                                                   T *__restrict__ work) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (int64_t)blockIdx.x * kLaneIoWarps + (threadIdx.x >> 5);
+  const int64_t chunks = (n + 31) / 32, g = w / chunks;
+  if (g >= groups) return;
+  const int i = (int)(w % chunks) * 32 + lane;
+  if (i >= n) return;
+  double v[32];
+#pragma unroll
+  for (int c = 0; c < 32; ++c) {
+    const int64_t col = g * 32 + c;
+    v[c] = col < count ? b[col * ldb + i] : 0.0;
+  }
+  lane_row_store(work + ((size_t)g * n + __ldg(in_pos + i)) * 32, v);
+}
+
+// The work array (solutions in their work rows) into x (natural rows, column-major, ldx): x's
+// row i from work row out_pos[i], the mirror of lane_in_kernel.
+template <class T>
+__global__ void __launch_bounds__(kLaneIoWarps * 32) lane_out_kernel(const T *__restrict__ work, int64_t count, int32_t n,
+                                                                    int64_t groups, const int32_t *__restrict__ out_pos,
+                                                                    double *__restrict__ x, int64_t ldx) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (int64_t)blockIdx.x * kLaneIoWarps + (threadIdx.x >> 5);
+  const int64_t chunks = (n + 31) / 32, g = w / chunks;
+  if (g >= groups) return;
+  const int i = (int)(w % chunks) * 32 + lane;
+  if (i >= n) return;
+  double v[32];
+  lane_row_load(work + ((size_t)g * n + __ldg(out_pos + i)) * 32, v);
+#pragma unroll
+  for (int c = 0; c < 32; ++c) {
+    const int64_t col = g * 32 + c;
+    if (col < count) x[col * ldx + i] = v[c];
   }
 }
 

@@ -157,9 +157,9 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
 //   kLaneBwdRow0 + c, kLaneBwdRowN, or kLaneBwdBegin, kLaneBwdMore..., kLaneBwdEnd: a backward row:
 //     acc = z from its ring slot minus val * x[offset] per entry, x = acc * dinv into the work row
 //     and into slot self.
-//   kLanePrefetch: copies `self` work rows (up to kLaneBatch) from offset `word` on, upwards (or
-//     downwards, flag bit 0), into the ring's lower (or, flag bit 1, upper) kLaneBatch slots, then
-//     waits for the batch before it.
+//   kLanePrefetch: copies `self` work rows (up to kLaneBatch), at the kLaneBatch uint32 offsets
+//     that fill its 16 bytes of entries, into the ring's lower (or, flag bit 1, upper) kLaneBatch
+//     slots, then waits for the batch before it.
 //   kLanePhase: a new run of rows: earlier copies are finished and this lane's stores are visible
 //     to its copies.
 //   kLaneFlush: per entry, the partial row `word` takes slot `offset`, which is zeroed.
