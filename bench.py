@@ -146,6 +146,18 @@ def algorithmic_bytes(n: int, count: int, info: dict, mode: str, steps: float = 
     return int(count * (24 * n + steps * 48 * n) + entries * 8 + 8 * (n + 1) + a_bytes)
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one lane_solve_kernel<double> launch on
+# the 10,000-bus block of 13,499 right-hand sides, from one ncu capture of this kernel (2.180 GB read,
+# 2.118 GB written); other kernels and workloads report none
+LANE_FP64_TRAFFIC = {(9999, 13499): 4.298141e9}
+
+
+def traffic_of(result: dict, count: int, n: int):
+    if result.get("kernel") == "lane_solve_kernel<double>":
+        return LANE_FP64_TRAFFIC.get((n, count))
+    return None
+
+
 def cpu_baseline(chol, rhs, seconds_target: float = 10.0) -> dict:
     from oracle import oracle as orc
     cores = os.cpu_count() or 1
@@ -346,13 +358,15 @@ def main():
     }
     modes = ["fp64", "fp32_ir"] if a.mode == "auto" else [a.mode]
 
-    def timed(run):
+    def timed(run, lane_timing=False):
         for _ in range(max(a.warmup, 3)):
             run()
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        if lane_timing:  # events around each launch's gather, solve and scatter kernels
+            factor.time_lane(True)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
@@ -364,8 +378,15 @@ def main():
         torch.cuda.synchronize()
         elapsed_ms = start.elapsed_time(end)
         launch_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs)
+        kernels = None
+        if lane_timing:
+            t = factor.lane_times()
+            factor.time_lane(False)
+            k = max(t["launches"], 1)
+            kernels = {"gather_ms": t["gather_ms"] / k, "solve_ms": t["solve_ms"] / k, "scatter_ms": t["scatter_ms"] / k,
+                       "launches": t["launches"]}
         replicas.barrier()
-        return replicas.max_over_ranks(elapsed_ms), launch_ms
+        return replicas.max_over_ranks(elapsed_ms), launch_ms, kernels
 
     # which solve each mode runs: the plain FP64 solve takes the lane solve from the lane threshold
     # on (three launches: gather, solve, scatter), else the domain solve; the refined solve is the
@@ -394,7 +415,8 @@ def main():
     time.sleep(0.3)
     results = {}
     for mode in modes:
-        elapsed_ms, launch_ms = timed(runs[mode])
+        on_lane = mode == "fp64" and use_lane
+        elapsed_ms, launch_ms, kernels = timed(runs[mode], lane_timing=on_lane)
         # check the timed results: relative residual of every 13th column, the oracle on a sample
         xs = d_x.cpu().numpy()
         resid = max(orc.relative_residual(p, i, v, xs[k], rhs[k]) for k in range(0, count, 13))
@@ -409,6 +431,15 @@ def main():
         else:
             r["algorithmic_bytes_per_launch"] = algorithmic_bytes(n, count, info, "fp64")
         r.update(solver_of(mode))
+        # the dominant kernel's own launch time: the lane solve kernel (events around it in every
+        # launch), else the one launch of the step
+        r["kernel_ms"] = launch_ms
+        if kernels:
+            r["kernels"] = kernels
+            r["kernel_ms"] = kernels["solve_ms"]
+            io_bytes = count * 16 * n  # each of the gather and the scatter reads and writes 8 n per RHS
+            r["kernels"]["gather_gbs"] = io_bytes / (kernels["gather_ms"] / 1e3) / 1e9
+            r["kernels"]["scatter_gbs"] = io_bytes / (kernels["scatter_ms"] / 1e3) / 1e9
         results[mode] = r
     clock_info = clocks.stop()
 
@@ -416,7 +447,7 @@ def main():
     passing = [m for m in modes if results[m]["max_rel_residual"] <= 1e-10]
     mode = max(passing, key=lambda m: results[m]["rhs_s"]) if passing else modes[0]
     best = results[mode]
-    achieved = best["algorithmic_bytes_per_launch"] / (best["launch_ms"] / 1e3) / 1e9
+    achieved = best["algorithmic_bytes_per_launch"] / (best["kernel_ms"] / 1e3) / 1e9
     compulsory = count * 16 * n / (best["launch_ms"] / 1e3) / 1e9
     if "fp64" in results and "fp32_ir" in results:
         results["fp32_ir_over_fp64"] = results["fp32_ir"]["rhs_s"] / results["fp64"]["rhs_s"]
@@ -431,9 +462,9 @@ def main():
             "accuracy": {"max_rel_residual": best["max_rel_residual"], "max_rel_err_vs_oracle": best["max_rel_err_vs_oracle"]},
             "modes": results,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_source": peak_kind, "kernel": best["kernel"],
+                         "traffic": traffic_of(best, count, n), "peak_source": peak_kind, "kernel": best["kernel"],
                          "algorithmic_bytes_per_launch": best["algorithmic_bytes_per_launch"],
-                         "launch_ms": best["launch_ms"], "compulsory_gbs": compulsory,
+                         "kernel_ms": best["kernel_ms"], "launch_ms": best["launch_ms"], "compulsory_gbs": compulsory,
                          "compulsory_frac": compulsory / peak},
             "clocks": clock_info, "gpu_launches": a.steps * sum(results[m]["launches_per_step"] for m in modes)}
 

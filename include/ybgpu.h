@@ -169,6 +169,15 @@ int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32
 /* No ybus counterpart: the number of right-hand sides from which the automatic choice takes the
  * lane solve (default 4096). */
 int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t min_count);
+/* No ybus counterpart: with on = 1, every lane-solve launch from now on records CUDA events around
+ * its three kernels (gather, solve, scatter) on the caller's stream, for up to 4096 launches;
+ * on = 0 stops. Either way the record so far is cleared. */
+int32_t yb_factor_time_lane(yb_factor *f, int32_t on);
+/* No ybus counterpart: waits for the recorded lane-solve launches and returns the total device
+ * milliseconds of their gathers, solves and scatters, and how many launches they were; then clears
+ * the record (timing stays on if it was). */
+int32_t yb_factor_lane_times(yb_factor *f, double *gather_ms, double *solve_ms, double *scatter_ms,
+                             int64_t *launches);
 /* No ybus counterpart: the streamed solve's shape for a precision: warps per block (1..16), pages
  * in flight per warp (2..16), page bytes (512..16384, a multiple of 16), and the row count under
  * which a level is taken by one warp alone (0: twice a slice's rows). */

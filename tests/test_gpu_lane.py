@@ -172,3 +172,22 @@ def test_a_block_larger_than_one_launch_of_work(gpu):
     bs, xs = b[idx].cpu().numpy(), x[idx].cpu().numpy()
     assert not np.isnan(xs).any()
     assert worst_relative_difference(xs, orc.solve_many(chol, bs, threads=8)) < BAR
+
+
+def test_lane_launch_times_are_recorded_when_asked(gpu):
+    chol = host.cholesky(random_spd(300, 3, 7))
+    rhs = right_hand_sides(300, 100, 11)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.set_tile_kind(FP64, LANE)
+    factor.solve_many(rhs)
+    assert factor.lane_times()["launches"] == 0, "nothing is recorded while timing is off"
+    factor.time_lane(True)
+    x = factor.solve_many(rhs)
+    factor.solve_many(rhs)
+    t = factor.lane_times()
+    assert t["launches"] == 2 and t["gather_ms"] > 0 and t["solve_ms"] > 0 and t["scatter_ms"] > 0
+    assert factor.lane_times()["launches"] == 0, "a read clears the record"
+    factor.time_lane(False)
+    factor.solve_many(rhs)
+    assert factor.lane_times()["launches"] == 0
+    assert worst_relative_difference(x, orc.solve_many(chol, rhs)) < BAR

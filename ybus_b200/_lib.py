@@ -82,6 +82,8 @@ SIGNATURES: dict[str, tuple] = {
     "yb_reference_spsm_solve": (i32, [vp, vp, i64, vp, i64, i64, i64, P_dbl]),
     "yb_factor_lane_info": (i32, [vp, i32, vp]),
     "yb_factor_set_lane_min_count": (i32, [vp, i32, i64]),
+    "yb_factor_time_lane": (i32, [vp, i32]),
+    "yb_factor_lane_times": (i32, [vp, P_dbl, P_dbl, P_dbl, P_i64]),
     "yb_factor_set_lane": (i32, [vp, i32, i32, i32]),
     "yb_factor_domain_info": (i32, [vp, i32, P_i32, P_i32, P_i32, P_i64, P_i64, P_i64, P_dbl]),
     "yb_domain_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp, vp]),

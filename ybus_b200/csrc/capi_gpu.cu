@@ -256,6 +256,38 @@ extern "C" int32_t yb_factor_timings(const yb_factor *f, double *upload_s, doubl
   });
 }
 
+extern "C" int32_t yb_factor_time_lane(yb_factor *f, int32_t on) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    f->lane_timing.on = on != 0;
+    f->lane_timing.used = 0;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_lane_times(yb_factor *f, double *gather_ms, double *solve_ms, double *scatter_ms,
+                                        int64_t *launches) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    LaneTiming &t = f->lane_timing;
+    double ms[3] = {0, 0, 0};
+    if (t.used > 0) cuda_check(cudaEventSynchronize(t.ev[t.used - 1][3]), "cudaEventSynchronize");
+    for (size_t k = 0; k < t.used; ++k)
+      for (int p = 0; p < 3; ++p) {
+        float e = 0;
+        cuda_check(cudaEventElapsedTime(&e, t.ev[k][p], t.ev[k][p + 1]), "cudaEventElapsedTime");
+        ms[p] += e;
+      }
+    if (gather_ms) *gather_ms = ms[0];
+    if (solve_ms) *solve_ms = ms[1];
+    if (scatter_ms) *scatter_ms = ms[2];
+    if (launches) *launches = (int64_t)t.used;
+    t.used = 0;
+    return YB_OK;
+  });
+}
+
 extern "C" int32_t yb_factor_reset_timings(yb_factor *f) {
   return guard([&] {
     require(f != nullptr, "null factor");
@@ -685,6 +717,18 @@ template <class T> size_t lane_smem(const DeviceLane *d) {
 }
 
 // The lane solve of `count` right-hand sides: gather into the work array, solve in place, scatter.
+// The events of the next timed lane launch, or null when timing is off or its slots are full.
+cudaEvent_t *lane_timing_slot(yb_factor *f) {
+  LaneTiming &t = f->lane_timing;
+  if (!t.on || t.used >= (size_t)LaneTiming::kSlots) return nullptr;
+  if (t.used == t.ev.size()) {
+    std::array<cudaEvent_t, 4> slot{};
+    for (auto &e : slot) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+    t.ev.push_back(slot);
+  }
+  return t.ev[t.used++].data();
+}
+
 template <class T>
 void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
                  cudaStream_t stream) {
@@ -710,12 +754,17 @@ void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, doub
     const int64_t groups = std::min(per_launch, groups_all - g0);
     const int64_t cols = std::min(count - g0 * 32, groups * 32);
     const unsigned io_grid = (unsigned)lane_io_blocks(groups, n);
+    cudaEvent_t *ev = lane_timing_slot(f);
+    if (ev) cuda_check(cudaEventRecord(ev[0], stream), "cudaEventRecord");
     lane_in_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(b + g0 * 32 * ldb, ldb, cols, (int32_t)n, groups, d->in_pos.get(), work);
     cuda_check(cudaGetLastError(), "lane_in_kernel launch");
+    if (ev) cuda_check(cudaEventRecord(ev[1], stream), "cudaEventRecord");
     lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
     cuda_check(cudaGetLastError(), "lane_solve_kernel launch");
+    if (ev) cuda_check(cudaEventRecord(ev[2], stream), "cudaEventRecord");
     lane_out_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(work, cols, (int32_t)n, groups, d->out_pos.get(), x + g0 * 32 * ldx, ldx);
     cuda_check(cudaGetLastError(), "lane_out_kernel launch");
+    if (ev) cuda_check(cudaEventRecord(ev[3], stream), "cudaEventRecord");
   }
 }
 

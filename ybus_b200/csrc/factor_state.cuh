@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <map>
 #include <memory>
 #include <string>
@@ -39,6 +40,24 @@ namespace yb {
 struct Timings {
   double upload = 0, solve = 0, download = 0;
   int64_t blocks = 0;
+};
+
+// Per-launch times of the lane solve, when switched on: events before the gather and after the
+// gather, the solve and the scatter of every launch, kept for up to kSlots launches between reads.
+struct LaneTiming {
+  static constexpr int kSlots = 4096;
+  bool on = false;
+  int device = -1;
+  std::vector<std::array<cudaEvent_t, 4>> ev;
+  size_t used = 0;
+  LaneTiming() = default;
+  LaneTiming(const LaneTiming &) = delete;
+  LaneTiming &operator=(const LaneTiming &) = delete;
+  ~LaneTiming() {
+    for (auto &slot : ev)
+      for (auto &e : slot)
+        if (e) cudaEventDestroy(e);
+  }
 };
 
 // The host-array solve's overlap: chunks of right-hand sides pass through an upload stream, the
@@ -153,6 +172,7 @@ struct yb_factor {
   // lane layouts by (value bytes, warps, page bytes); a null entry: the factor admits none
   std::map<std::tuple<int, int, int>, std::unique_ptr<yb::DeviceLane>> lanes;
   yb::DeviceArray<uint8_t> lane_work, lane_partial;  // the lane solve's work and partial arrays
+  yb::LaneTiming lane_timing;
   yb::DeviceArray<int32_t> error;  // the device error word (a bounded wait that ran out)
   long long *phase_clock = nullptr;  // diagnostics buffer of the caller's, or null
   yb::DeviceArray<double> scratch64;

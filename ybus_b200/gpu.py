@@ -262,6 +262,18 @@ class GpuFactor:
         """The number of right-hand sides from which the automatic choice takes the lane solve."""
         _check(lib().yb_factor_set_lane_min_count(self._h, precision, min_count))
 
+    def time_lane(self, on: bool = True) -> None:
+        """Records CUDA events around the gather, solve and scatter of every lane-solve launch
+        (on), or stops; either way clears the record."""
+        _check(lib().yb_factor_time_lane(self._h, 1 if on else 0))
+
+    def lane_times(self) -> dict:
+        """Total device milliseconds of the recorded lane launches' gathers, solves and scatters
+        and their count (waits for them); clears the record."""
+        g, s_, o, k = C.c_double(), C.c_double(), C.c_double(), C.c_int64()
+        _check(lib().yb_factor_lane_times(self._h, C.byref(g), C.byref(s_), C.byref(o), C.byref(k)))
+        return {"gather_ms": g.value, "solve_ms": s_.value, "scatter_ms": o.value, "launches": k.value}
+
     def autotune(self, precision: int = FP64, count: int = 2048) -> dict:
         """Times the domain and lane solves' shapes on `count` right-hand sides and keeps the fastest."""
         cfg = np.zeros(5, np.int32)
