@@ -4,9 +4,9 @@ layouts on the CPU: every right-hand side is one lane, each warp's live slots an
 every row is read from its ring slot after its prefetch and before the slot is refilled."""
 import numpy as np
 
-FWD_ROW0, FWD_ROWN, FWD_MORE = 0, 5, 6
-BWD_ROW0, BWD_ROWN, BWD_BEGIN, BWD_MORE, BWD_END = 7, 12, 13, 14, 15
-PREFETCH, PHASE, TOP_SUM, FLUSH, IMPORT, BARRIER, END, PAGE_END = range(16, 24)
+FWD_ROW0, FWD_PRE1, BWD_ROW0, BWD_PRE1 = 0, 5, 9, 14
+FWD_ROWN, FWD_MORE, BWD_ROWN, BWD_BEGIN, BWD_MORE, BWD_END = range(18, 24)
+PREFETCH, PHASE, TOP_SUM, FLUSH, IMPORT, BARRIER, END, PAGE_END = range(24, 32)
 RING, BATCH = 8, 4
 
 
@@ -27,7 +27,7 @@ def records(lay, warp):
             if kind == PAGE_END:
                 break
             tail = page[pos + 8:pos + 16]
-            body = page[pos + 16:pos + 16 + count * entry]
+            body = page[pos + 16:pos + 16 + ((count * entry + 15) & ~15)]
             assert pos + 16 + count * entry <= pb, "a record past its page"
             vals = np.array([body[e * entry:e * entry + vb].view(ftype)[0] for e in range(count)], np.float64)
             words = np.array([body[e * entry:e * entry + 4].view(np.uint32)[0] for e in range(count)], np.int64)
@@ -47,45 +47,57 @@ def warp_steps(lay, warp, work, partial, lanes):
     ring = np.full((RING, lanes), np.nan)
     pending = np.zeros(RING, bool)  # a prefetched row not read yet
     z = None
+
+    def prefetch(block):
+        assert len(block) == 16
+        words = block.view(np.uint32).copy()
+        nrows, base = int(words[0] & 7), BATCH if words[0] & 8 else 0
+        words[0] &= ~np.uint32(15)
+        assert nrows <= BATCH
+        for q in range(nrows):
+            assert words[q] % row == 0
+            assert not pending[base + q], "a prefetch over a row not read yet"
+            assert 0 <= words[q] // row < work.shape[0], "a prefetch outside the work array"
+            ring[base + q] = work[words[q] // row]
+            pending[base + q] = True
+
     for kind, rs, self_, count, word, tail, vals, words, offs, body in records(lay, warp):
         s, w = self_ * 16 // row, word // row
-        if kind <= BWD_END:
+        fwd = kind < BWD_ROW0 or kind in (FWD_ROWN, FWD_MORE)
+        bwd = BWD_ROW0 <= kind < FWD_ROWN or BWD_ROWN <= kind <= BWD_END
+        if fwd or bwd:
             dinv = float(tail[:vb].view(ftype)[0])
             assert 0 <= w < work.shape[0], "a row outside the work array"
-        if FWD_ROW0 <= kind <= FWD_ROWN:
+        if kind in range(FWD_ROW0, FWD_PRE1) or kind in range(BWD_ROW0, BWD_PRE1):
+            assert count == kind - (FWD_ROW0 if fwd else BWD_ROW0)
+        if kind in range(FWD_PRE1, BWD_ROW0) or kind in range(BWD_PRE1, FWD_ROWN):
+            c = kind - (FWD_PRE1 if fwd else BWD_PRE1) + 1
+            pad = (c * (16 if vb == 8 else 8) + 15) // 16 * 16
+            assert len(body) == pad + 16, "a row's prefetch block after its entries"
+            prefetch(body[pad:pad + 16])
+            vals, offs = vals[:c], offs[:c]
+        if fwd and kind != FWD_MORE:
             assert pending[rs], "a row read before its prefetch"
             pending[rs] = False
             z = (ring[rs] + live[s]) * dinv
             live[s] = 0.0
             work[w] = z
-        if FWD_ROW0 <= kind <= FWD_MORE:
-            if FWD_ROW0 <= kind < FWD_ROWN:
-                assert count == kind - FWD_ROW0
+        if fwd:
             for v, o in zip(vals, offs):
                 live[o // row] -= v * z
-        elif BWD_ROW0 <= kind <= BWD_END:
-            if BWD_ROW0 <= kind < BWD_ROWN:
-                assert count == kind - BWD_ROW0
-            if kind <= BWD_BEGIN:
+        elif bwd:
+            if kind not in (BWD_MORE, BWD_END):
                 assert pending[rs], "a row read before its prefetch"
                 pending[rs] = False
                 z = ring[rs].copy()
             for v, o in zip(vals, offs):
                 z = z - v * live[o // row]
-            if kind < BWD_BEGIN or kind == BWD_END:
+            if kind not in (BWD_BEGIN, BWD_MORE):
                 x = z * dinv
                 live[s] = x
                 work[w] = x
         elif kind == PREFETCH:
-            flags = int(tail[:4].view(np.uint32)[0])
-            base = BATCH if flags & 2 else 0
-            assert len(body) == 16 and self_ <= BATCH
-            rows = body.view(np.uint32) // row
-            for q in range(self_):
-                assert not pending[base + q], "a prefetch over a row not read yet"
-                assert 0 <= rows[q] < work.shape[0], "a prefetch outside the work array"
-                ring[base + q] = work[rows[q]]
-                pending[base + q] = True
+            prefetch(body)
         elif kind == PHASE:
             assert not pending.any(), "a phase that leaves prefetched rows unread"
             ring[:] = np.nan

@@ -684,7 +684,7 @@ void launch_domain(yb_factor *f, const TileConfig &cfg, int64_t count, const IO 
 // The lane solve's page ring, the most slots a layout may take (the automatic choice takes the lane
 // solve only up to kLaneAutoSlots, which leave room for several blocks per SM), and the largest
 // work array one launch fills (larger solves run in several launches)
-constexpr int32_t kLaneRing = 2, kLaneMaxSlots = 256, kLaneAutoSlots = 64;
+constexpr int32_t kLaneMaxSlots = 256, kLaneAutoSlots = 64;
 constexpr size_t kLaneWorkBytes = size_t(2) << 30;
 
 template <class T> DeviceLane *lane_for(yb_factor *f, int warps, int page_bytes, cudaStream_t stream) {
@@ -746,7 +746,7 @@ void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, doub
              "cudaFuncSetAttribute");
   LaneArgs a{};
   a.n = (int32_t)n;
-  a.slots = d->slots, a.page_bytes = d->page_bytes, a.ring = kLaneRing, a.partials = d->partials;
+  a.slots = d->slots, a.page_bytes = d->page_bytes, a.partials = d->partials;
   a.blob = d->blob.get();
   a.warp_page = d->warp_page.get();
   a.error = f->error.get();

@@ -104,16 +104,29 @@ template <class T> struct PageWriter {
     put(0, kind, 0, 0, nullptr, 0);
     pos += 16;
   }
-  void prefetch(int32_t batch) {
-    static_assert(kLaneBatch == 4, "a prefetch record holds four row offsets");
+  // The work-row offsets of a batch of the phase (rows past its end: none), its row count and
+  // whether it fills the ring's upper half.
+  int32_t batch_rows(int32_t batch, uint32_t (&rows)[kLaneBatch], bool &upper) const {
+    static_assert(kLaneBatch == 4, "a prefetch holds four row offsets");
     const int32_t r0 = batch * kLaneBatch;
     const int32_t count = std::max(0, std::min(kLaneBatch, len - r0));
-    uint32_t rows[kLaneBatch] = {};
-    for (int32_t q = 0; q < count; ++q) rows[q] = (uint32_t)work_row[start + step * (r0 + q)] * kRow;
-    const uint32_t flags = (r0 & (kLaneRows - 1)) ? 2u : 0u;
+    for (int32_t q = 0; q < kLaneBatch; ++q) rows[q] = q < count ? (uint32_t)work_row[start + step * (r0 + q)] * kRow : 0;
+    upper = (r0 & (kLaneRows - 1)) != 0;
+    return count;
+  }
+  // A batch's prefetch block: its four row offsets, the row count in bits 0-2 of the first and the
+  // upper-half flag in bit 3 (row offsets are multiples of 128 bytes).
+  void prefetch_block(int32_t batch, uint32_t (&block)[kLaneBatch]) const {
+    bool upper;
+    const int32_t count = batch_rows(batch, block, upper);
+    block[0] |= (uint32_t)count | (upper ? 8u : 0u);
+  }
+  void prefetch(int32_t batch) {
+    uint32_t block[kLaneBatch];
+    prefetch_block(batch, block);
     room(32);
-    put((uint32_t)count, kLanePrefetch, 16 / kEntry, 0, &flags, 4);
-    std::memcpy(at() + 16, rows, 16);
+    put(0, kLanePrefetch, 16 / kEntry, 0, nullptr, 0);
+    std::memcpy(at() + 16, block, 16);
     pos += 32;
   }
   void phase(int32_t first, int32_t rows, bool backward) {
@@ -151,13 +164,28 @@ template <class T> struct PageWriter {
   // One row of the phase: its records carry its work-row offset, its ring slot and its diagonal's
   // reciprocal; rows of up to 4 entries take the kinds for their exact count.
   void row(uint32_t self, T dinv, const std::vector<std::pair<T, uint32_t>> &entries, bool backward) {
-    if (row_i % kLaneBatch == 0 && row_i > 0) prefetch(row_i / kLaneBatch + 1);
+    const size_t count = entries.size();
+    const bool opens_batch = row_i % kLaneBatch == 0 && row_i > 0;
+    // a batch's prefetch rides on the row that opens it when that row has 1 to 4 entries
+    const bool carries = opens_batch && count >= 1 && count <= 4;
+    if (opens_batch && !carries) prefetch(row_i / kLaneBatch + 1);
+    uint32_t pre[kLaneBatch] = {};
+    if (carries) prefetch_block(row_i / kLaneBatch + 1, pre);
     const uint32_t ring = (uint32_t)(row_i & (kLaneRows - 1)) << 5;
     const uint32_t wpos = (uint32_t)work_row[start + step * row_i] * kRow;
     ++row_i;
-    const size_t count = entries.size();
     uint8_t tail[8] = {};
     std::memcpy(tail, &dinv, sizeof(T));
+    if (carries) {
+      const size_t body = ((count * kEntry + 15) & ~(size_t)15) + 16;
+      room(16 + body);
+      put(self, (backward ? kLaneBwdPre1 : kLaneFwdPre1) + (uint32_t)count - 1 + ring, (uint32_t)(count + 16 / kEntry),
+          wpos, tail, 8);
+      entries_at(at(), entries, nullptr, 0, count);
+      std::memcpy(at() + 16 + body - 16, pre, 16);
+      pos += 16 + body;
+      return;
+    }
     if (count <= 4) {
       room(bytes_of(count));
       put(self, (backward ? kLaneBwdRow0 : kLaneFwdRow0) + (uint32_t)count + ring, (uint32_t)count, wpos, tail, 8);

@@ -29,10 +29,11 @@
 namespace yb {
 
 constexpr int kLaneBarriers = 3;             // block barriers in every warp's stream
+constexpr int kLaneRing = 2;                 // pages in flight per warp (a power of two)
 constexpr int kLaneMaxWarps = 8;             // warps per block at most
 
 struct LaneArgs {
-  int32_t n, slots, page_bytes, ring, partials;
+  int32_t n, slots, page_bytes, partials;
   const uint8_t *__restrict__ blob;       // every warp's pages
   const int32_t *__restrict__ warp_page;  // [warps + 1]
   int32_t *error;                         // set to 1 if a wait ran out or a stream is malformed
@@ -128,7 +129,8 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
   // offsets, record fields and branches derived from it) to be the same across the warp, and keeps
   // the records' decoding on the uniform datapath instead of every lane's registers.
   const int lane = threadIdx.x & 31, warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
-  const int S = a.ring, PB = a.page_bytes;
+  constexpr int S = kLaneRing;  // known here, so the ring's slot and phase are a mask and a shift
+  const int PB = a.page_bytes;
   const uint32_t base = (uint32_t)(warp * lane_warp_bytes<T>(a.slots, S, PB));
   const uint32_t live = base + lane * (uint32_t)sizeof(T);                     // this lane's slot 0
   const uint32_t rows = base + (uint32_t)a.slots * ROW + lane * (uint32_t)sizeof(T);  // its ring slot 0
@@ -188,10 +190,32 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
       lane_at<T>(self) = x;
       *reinterpret_cast<T *>(w_lane + h.y) = x;
     };
-    // the common records first: rows of at most 4 entries
-    if (kind <= kLaneFwdRow0 + 4) {
+    // a prefetch block: the batch's rows into their half of the ring, then the batch before waited for
+    auto prefetch = [&](uint32_t at) {
+      const uint4 o = lane_at<uint4>(at);
+      const uint32_t nrows = o.x & 7u;
+      const uint32_t dst = smem_s + rows + ((o.x & 8u) ? (uint32_t)kLaneBatch * ROW : 0u);
+      const uint32_t off[kLaneBatch] = {o.x & ~15u, o.y, o.z, o.w};
+#pragma unroll
+      for (int q = 0; q < kLaneBatch; ++q)
+        if (q < (int)nrows)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst + q * ROW), "l"(w_lane + off[q]),
+                       "n"(sizeof(T))
+                       : "memory");
+      cp_async_commit();
+      cp_async_wait<1>();
+    };
+    // the entries' bytes of a row of c entries, to the 16-byte boundary
+    auto padded = [&](uint32_t c) { return (c * E + 15) & ~15u; };
+    // the common records first: rows of at most 4 entries, some opening a batch with its prefetch
+    if (kind <= kLaneFwdPre1 + 3) {
+      uint32_t c = kind - kLaneFwdRow0;
+      if (kind >= kLaneFwdPre1) {
+        c = kind - kLaneFwdPre1 + 1;
+        prefetch(e + padded(c));
+      }
       forward();
-      switch (count) {
+      switch (c) {
         case 1: lane_scatter_n<T, 1>(e, z, live); break;
         case 2: lane_scatter_n<T, 2>(e, z, live); break;
         case 3: lane_scatter_n<T, 3>(e, z, live); break;
@@ -201,9 +225,14 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
       page = next;
       continue;
     }
-    if (kind - kLaneBwdRow0 <= 4u) {
+    if (kind - kLaneBwdRow0 <= kLaneBwdPre1 + 3 - kLaneBwdRow0) {
+      uint32_t c = kind - kLaneBwdRow0;
+      if (kind >= kLaneBwdPre1) {
+        c = kind - kLaneBwdPre1 + 1;
+        prefetch(e + padded(c));
+      }
       const T b = lane_at<T>(b_at);
-      switch (count) {
+      switch (c) {
         case 1: z = lane_gather_n<T, 1>(e, b, live); break;
         case 2: z = lane_gather_n<T, 2>(e, b, live); break;
         case 3: z = lane_gather_n<T, 3>(e, b, live); break;
@@ -221,21 +250,7 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32) lane_solve_kernel(LaneArgs
       case kLaneBwdBegin: z = lane_gather<T>(e, count, lane_at<T>(b_at), live); break;
       case kLaneBwdMore: z = lane_gather<T>(e, count, z, live); break;
       case kLaneBwdEnd: z = lane_gather<T>(e, count, z, live); backward(); break;
-      case kLanePrefetch: {  // the batch's work-row offsets follow the header
-        const uint32_t dst = smem_s + rows + ((h.z & 2u) ? (uint32_t)kLaneBatch * ROW : 0u);
-        const uint32_t nrows = h.x & 0xffffu;
-        const uint4 o = lane_at<uint4>(e);
-        const uint32_t off[kLaneBatch] = {o.x, o.y, o.z, o.w};
-#pragma unroll
-        for (int q = 0; q < kLaneBatch; ++q)
-          if (q < (int)nrows)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst + q * ROW), "l"(w_lane + off[q]),
-                         "n"(sizeof(T))
-                         : "memory");
-        cp_async_commit();
-        cp_async_wait<1>();
-        break;
-      }
+      case kLanePrefetch: prefetch(e); break;
       case kLanePhase:
         cp_async_wait<0>();
         __threadfence();  // the rows this lane stored are what the phase's copies read

@@ -148,8 +148,7 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
 //
 // A record is a 16-byte header, then `count` entries of 16 bytes (FP64) or 8 (FP32): {T val, or a
 // 32-bit word in its place; uint32 offset}. The header: uint32 {self (16 bits), kind (5 bits), ring
-// slot (3 bits), count (8 bits)}, uint32 word, then 8 bytes: T dinv for rows, uint32 flags for a
-// prefetch. Offsets are byte offsets of 32-value live slots (slot 0 is always zero, slot 1 a sink),
+// slot (3 bits), count (8 bits)}, uint32 word, then 8 bytes: T dinv for rows. Offsets are byte offsets of 32-value live slots (slot 0 is always zero, slot 1 a sink),
 // `self` such an offset / 16; words are byte offsets of 32-value rows of the work or partial array.
 //   kLaneFwdRow0 + c (c = 0..4 entries), kLaneFwdRowN, kLaneFwdMore: a forward row at work offset
 //     `word`: read and zero acc at self, z = (b + acc) * dinv with b from its ring slot, z into the
@@ -157,9 +156,14 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
 //   kLaneBwdRow0 + c, kLaneBwdRowN, or kLaneBwdBegin, kLaneBwdMore..., kLaneBwdEnd: a backward row:
 //     acc = z from its ring slot minus val * x[offset] per entry, x = acc * dinv into the work row
 //     and into slot self.
-//   kLanePrefetch: copies `self` work rows (up to kLaneBatch), at the kLaneBatch uint32 offsets
-//     that fill its 16 bytes of entries, into the ring's lower (or, flag bit 1, upper) kLaneBatch
-//     slots, then waits for the batch before it.
+//   kLaneFwdPre1 + c - 1, kLaneBwdPre1 + c - 1 (c = 1..4 entries): the row of kind kLaneFwdRow0 + c
+//     (kLaneBwdRow0 + c) that opens a batch, its entries followed by a 16-byte prefetch block (the
+//     header's count is c + 16 / entry bytes): the prefetch block's copies run first, as a
+//     kLanePrefetch record's would.
+//   kLanePrefetch: its 16 bytes of entries are a prefetch block: kLaneBatch uint32 work-row
+//     offsets, the first with the row count (up to kLaneBatch) in bits 0-2 and the upper-half flag
+//     in bit 3; the rows are copied into the ring's lower (or upper) kLaneBatch slots, then the
+//     batch before them is waited for.
 //   kLanePhase: a new run of rows: earlier copies are finished and this lane's stores are visible
 //     to its copies.
 //   kLaneFlush: per entry, the partial row `word` takes slot `offset`, which is zeroed.
@@ -169,21 +173,23 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
 //   kLanePageEnd ends its page (every page has one).
 enum LaneKind : uint32_t {
   kLaneFwdRow0 = 0,  // .. kLaneFwdRow0 + 4
-  kLaneFwdRowN = 5,
-  kLaneFwdMore = 6,
-  kLaneBwdRow0 = 7,  // .. kLaneBwdRow0 + 4
-  kLaneBwdRowN = 12,
-  kLaneBwdBegin = 13,
-  kLaneBwdMore = 14,
-  kLaneBwdEnd = 15,
-  kLanePrefetch = 16,
-  kLanePhase = 17,
-  kLaneTopSum = 18,
-  kLaneFlush = 19,
-  kLaneImport = 20,
-  kLaneBarrier = 21,
-  kLaneEnd = 22,
-  kLanePageEnd = 23
+  kLaneFwdPre1 = 5,  // .. kLaneFwdPre1 + 3
+  kLaneBwdRow0 = 9,  // .. kLaneBwdRow0 + 4
+  kLaneBwdPre1 = 14,  // .. kLaneBwdPre1 + 3
+  kLaneFwdRowN = 18,
+  kLaneFwdMore = 19,
+  kLaneBwdRowN = 20,
+  kLaneBwdBegin = 21,
+  kLaneBwdMore = 22,
+  kLaneBwdEnd = 23,
+  kLanePrefetch = 24,
+  kLanePhase = 25,
+  kLaneTopSum = 26,
+  kLaneFlush = 27,
+  kLaneImport = 28,
+  kLaneBarrier = 29,
+  kLaneEnd = 30,
+  kLanePageEnd = 31
 };
 constexpr int kLaneBatch = 4;              // work rows per prefetch
 constexpr int kLaneRows = 2 * kLaneBatch;  // slots of a warp's prefetch ring
