@@ -147,9 +147,9 @@ def algorithmic_bytes(n: int, count: int, info: dict, mode: str, steps: float = 
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one lane_solve_kernel<double> launch on
-# the 10,000-bus block of 13,499 right-hand sides, from one ncu capture of this kernel (2.180 GB read,
-# 2.118 GB written); other kernels and workloads report none
-LANE_FP64_TRAFFIC = {(9999, 13499): 4.298141e9}
+# the 10,000-bus block of 13,499 right-hand sides, from one ncu capture of this kernel (2.176 GB read,
+# 2.115 GB written); other kernels and workloads report none
+LANE_FP64_TRAFFIC = {(9999, 13499): 4.290592e9}
 
 
 def traffic_of(result: dict, count: int, n: int):
