@@ -35,7 +35,7 @@ WORKLOAD = "10k-bus PTDF block: B' 9,999 x 9,999 AMD Cholesky, 13,499 branch RHS
 N_BUS, EXTRA = 10000, 3500
 FALLBACK_HBM_GBS = 6650.0
 IR_TOLERANCE, IR_MAX_STEPS = 1e-10, 3
-LANE_MIN_COUNT, LANE_AUTO_SLOTS = 4096, 64  # the library's automatic choice of the lane solve
+LANE_MIN_COUNT, LANE_AUTO_SLOTS = 3072, 64  # the library's automatic choice of the lane solve
 
 
 def parse():

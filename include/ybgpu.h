@@ -167,7 +167,7 @@ int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t *info);
  * which three blocks fit an SM). */
 int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32_t page_bytes);
 /* No ybus counterpart: the number of right-hand sides from which the automatic choice takes the
- * lane solve (default 4096). */
+ * lane solve (default 3072). */
 int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t min_count);
 /* No ybus counterpart: with on = 1, every lane-solve launch from now on records CUDA events around
  * its three kernels (gather, solve, scatter) on the caller's stream, for up to 4096 launches;

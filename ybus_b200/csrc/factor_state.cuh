@@ -109,7 +109,7 @@ struct TileConfig {
   int domain_warps = 16, domain_ring = 2, domain_page = 2048, domain_cut = -1;
   // the automatic choice takes the lane solve from this many right-hand sides on (one warp per 32:
   // fewer leave SMs idle, where the domain solve's tiles spread over all of them)
-  int64_t lane_min_count = 4096;
+  int64_t lane_min_count = 3072;
   int lane_warps = 8, lane_page = 0;  // the lane solve's warps per block (one group of 32 right-hand sides), page bytes
 };
 
