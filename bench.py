@@ -388,9 +388,10 @@ def main():
         replicas.barrier()
         return replicas.max_over_ranks(elapsed_ms), launch_ms, kernels
 
-    # which solve each mode runs: the plain FP64 solve takes the lane solve from the lane threshold
-    # on (three launches: gather, solve, scatter), else the domain solve; the refined solve is the
-    # domain solve with its refinement fused (one launch)
+    # which solve each mode runs: from the lane threshold on, the plain FP64 solve takes the lane
+    # solve (three launches: gather, solve, scatter) and the refined solve its FP32 lane passes with
+    # an FP64 update and residual between them; below it, the domain solve (the refined one with its
+    # refinement fused into one launch)
     lane = None
     try:
         lane = factor.lane_info(FP64)
@@ -398,10 +399,22 @@ def main():
         pass
     use_lane = lane is not None and count >= LANE_MIN_COUNT and lane["slots"] <= LANE_AUTO_SLOTS
 
+    lane32 = None
+    try:
+        lane32 = factor.lane_info(FP32)
+    except Exception:
+        pass
+    use_lane32 = lane32 is not None and count >= LANE_MIN_COUNT and lane32["slots"] <= LANE_AUTO_SLOTS
+
     def solver_of(mode):
         if mode == "fp64" and use_lane:
             return {"solver": "lane", "kernel": "lane_solve_kernel<double>", "launches_per_step": 3,
                     "lane": {k: lane[k] for k in ("warps", "slots", "domains", "top", "pages", "smem")}}
+        if mode == "fp32_ir" and use_lane32:
+            # an initialisation and two gathers, per pass a solve, an update, a residual and a
+            # decision (passes after every group has stopped return at once), then the scatter
+            return {"solver": "lane", "kernel": "lane_solve_kernel<float>", "launches_per_step": 4 + 4 * (IR_MAX_STEPS + 1),
+                    "lane": {k: lane32[k] for k in ("warps", "slots", "domains", "top", "pages", "smem")}}
         prec = FP64 if mode == "fp64" else FP32
         return {"solver": "domain", "kernel": "domain_tile_kernel", "launches_per_step": 1,
                 "tile": factor.domain_info(prec)["tile"]}

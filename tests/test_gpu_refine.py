@@ -2,13 +2,15 @@
 oracle: the relative residual ||b - A x||inf / ||b||inf of every column (accuracy.rs:58-79) reaches
 the tolerance, the device's own ratios agree with the oracle's, the corrections stop early when the
 tolerance is met, and the solutions agree with the FP64 oracle to what the residual allows. Runs
-on the reference's fixture matrix and the synthetic 2,000- and 10,000-bus grids."""
+on the reference's fixture matrix and the synthetic 2,000- and 10,000-bus grids, by the domain
+solve (the automatic choice for these counts) and by the lane solve (forced; its refinement passes
+take groups of 32 columns)."""
 import numpy as np
 import pytest
 
 import oracle.oracle as orc
 from fixtures import random_spd, right_hand_sides, worst_relative_difference
-from ybus_b200 import CudaError, GpuFactor, grids, host
+from ybus_b200 import FP32, CudaError, GpuFactor, grids, host
 
 pytestmark = pytest.mark.gpu
 
@@ -22,11 +24,16 @@ def bprime(n_bus, extra, seed):
     return host.Matrix.from_triplets(n_bus, n_bus, r, c, v).select(keep, keep)
 
 
-def refined(gpu, a, rhs, max_steps=4, tol=TOL):
+LANE = 5
+
+
+def refined(gpu, a, rhs, max_steps=4, tol=TOL, lane=False):
     import torch
     chol = host.cholesky(a)
     factor = GpuFactor.from_cholesky(gpu, chol)
     factor.attach_matrix(a)
+    if lane:
+        factor.set_tile_kind(FP32, LANE)
     b = torch.from_numpy(rhs).cuda()
     x = torch.empty_like(b)
     ratio = torch.empty(rhs.shape[0], dtype=torch.float64, device="cuda")
@@ -38,8 +45,9 @@ def refined(gpu, a, rhs, max_steps=4, tol=TOL):
     return chol, x.cpu().numpy(), ratio.cpu().numpy(), steps.cpu().numpy()
 
 
+@pytest.mark.parametrize("lane", [False, True], ids=["domain", "lane"])
 @pytest.mark.parametrize("case", ["fixture", "grid2k", "grid10k"])
-def test_refinement_reaches_the_tolerance(gpu, case):
+def test_refinement_reaches_the_tolerance(gpu, case, lane):
     if case == "fixture":
         a = random_spd(300, 3, 7)
         rhs = right_hand_sides(300, 37, 11)
@@ -49,7 +57,7 @@ def test_refinement_reaches_the_tolerance(gpu, case):
     else:
         a = bprime(10000, 3500, grids.SEED_BASE + 2)
         rhs = np.random.default_rng(2).standard_normal((600, 9999))
-    chol, x, ratio, steps = refined(gpu, a, rhs)
+    chol, x, ratio, steps = refined(gpu, a, rhs, lane=lane)
     p, i, v = a.to_csr().arrays()
     oracle_ratio = np.array([orc.relative_residual(p, i, v, x[k], rhs[k]) for k in range(rhs.shape[0])])
     assert oracle_ratio.max() <= TOL, oracle_ratio.max()
@@ -62,10 +70,11 @@ def test_refinement_reaches_the_tolerance(gpu, case):
     assert worst_relative_difference(x, cpu) < 1e-8
 
 
-def test_zero_steps_is_the_fp32_solve_and_reports_its_residual(gpu):
+@pytest.mark.parametrize("lane", [False, True], ids=["domain", "lane"])
+def test_zero_steps_is_the_fp32_solve_and_reports_its_residual(gpu, lane):
     a = random_spd(300, 3, 7)
     rhs = right_hand_sides(300, 9, 3)
-    _, x, ratio, steps = refined(gpu, a, rhs, max_steps=0)
+    _, x, ratio, steps = refined(gpu, a, rhs, max_steps=0, lane=lane)
     assert (steps == 0).all()
     assert 1e-12 < ratio.max() < 1e-4
 
@@ -77,3 +86,16 @@ def test_refinement_needs_an_attached_matrix(gpu):
     b = torch.ones((2, 50), dtype=torch.float64, device="cuda")
     with pytest.raises(CudaError):
         factor.solve_many_refined_device(b.data_ptr(), b.data_ptr(), 2)
+
+
+def test_lane_refinement_stops_each_group_on_its_own(gpu):
+    # two groups of 32: the first's columns are zero (ratio 0 after the first solve, no correction),
+    # the second's are not (at least one correction); a third, partial group of 5 columns
+    a = bprime(2000, 700, grids.SEED_BASE + 1)
+    rhs = np.random.default_rng(4).standard_normal((69, 1999))
+    rhs[:32] = 0.0
+    chol, x, ratio, steps = refined(gpu, a, rhs, lane=True)
+    assert (steps[:32] == 0).all() and (ratio[:32] == 0).all() and (x[:32] == 0).all()
+    assert (steps[32:] >= 1).all() and ratio[32:].max() <= TOL
+    p, i, v = a.to_csr().arrays()
+    assert max(orc.relative_residual(p, i, v, x[k], rhs[k]) for k in range(32, 69)) <= TOL

@@ -11,6 +11,7 @@
 #include "factor_state.cuh"
 #include "domain_solve.cuh"
 #include "lane_solve.cuh"
+#include "lane_refine.cuh"
 #include "smem_solve.cuh"
 #include "stream_solve.cuh"
 #include "solve.cuh"
@@ -756,7 +757,8 @@ void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, doub
     const unsigned io_grid = (unsigned)lane_io_blocks(groups, n);
     cudaEvent_t *ev = lane_timing_slot(f);
     if (ev) cuda_check(cudaEventRecord(ev[0], stream), "cudaEventRecord");
-    lane_in_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(b + g0 * 32 * ldb, ldb, cols, (int32_t)n, groups, d->in_pos.get(), work);
+    lane_in_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(b + g0 * 32 * ldb, ldb, cols, (int32_t)n, groups, d->in_pos.get(), work,
+                                                                  nullptr);
     cuda_check(cudaGetLastError(), "lane_in_kernel launch");
     if (ev) cuda_check(cudaEventRecord(ev[1], stream), "cudaEventRecord");
     lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
@@ -1228,11 +1230,92 @@ extern "C" int32_t yb_factor_attach_matrix(yb_factor *f, const int64_t *a_ptr, c
     f->a_ptr.upload(p, s);
     f->a_idx.upload(idx.empty() ? std::vector<int32_t>{0} : idx, s);
     f->a_val.upload(val.empty() ? std::vector<double>{0.0} : val, s);
+    // and A as given (CSR, natural order), for the lane refinement's residual
+    std::vector<int32_t> csr_ptr(n + 1), csr_idx(nnz ? nnz : 1, 0);
+    std::vector<double> csr_val(nnz ? nnz : 1, 0.0);
+    for (int64_t i = 0; i <= n; ++i) csr_ptr[i] = (int32_t)a_ptr[i];
+    for (int64_t k = 0; k < nnz; ++k) csr_idx[k] = (int32_t)a_idx[k], csr_val[k] = a_val[k];
+    f->a_csr_ptr.upload(csr_ptr, s);
+    f->a_csr_idx.upload(csr_idx, s);
+    f->a_csr_val.upload(csr_val, s);
     cuda_check(cudaStreamSynchronize(s), "matrix upload");
     f->a_rows = n;
     return YB_OK;
   });
 }
+
+namespace yb {
+// The refined solve through the lane solve: per launch's groups, pass 0 solves b, each later pass
+// the residual; after each solve the update x += d and the residual in FP64, then each group's
+// decision; the kernels of a pass skip the groups that have stopped (lane_refine.cuh).
+void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
+                         int32_t max_steps, double tolerance, double *ratio_out, int32_t *steps_out, cudaStream_t stream) {
+  using T = float;
+  const int64_t n = f->n;
+  const size_t group_bytes = (size_t)n * 32 * sizeof(T);
+  const int64_t groups_all = (count + 31) / 32;
+  // per launch as many groups as the plain solve takes (the FP32 work array's bound); b and x in
+  // FP64 in the lane layout take four times the work array's bytes beside it
+  const int64_t per_launch = std::max<int64_t>(1, std::min<int64_t>(groups_all, (int64_t)(kLaneWorkBytes / group_bytes)));
+  const int64_t cols_most = per_launch * 32;
+  f->lane_work.reserve((size_t)per_launch * group_bytes);
+  f->lane_partial.reserve((size_t)per_launch * std::max(d->partials, 1) * 32 * sizeof(T));
+  f->refine_scratch.reserve((size_t)(2 * cols_most * n));
+  f->refine_state.reserve((size_t)cols_most * 3 * sizeof(double) + (size_t)per_launch);
+  T *work = reinterpret_cast<T *>(f->lane_work.get());
+  T *partial = reinterpret_cast<T *>(f->lane_partial.get());
+  double *bl = f->refine_scratch.get(), *xl = bl + cols_most * n;
+  auto *rmax = reinterpret_cast<unsigned long long *>(f->refine_state.get());
+  unsigned long long *bmax = rmax + cols_most;
+  double *prev = reinterpret_cast<double *>(bmax + cols_most);
+  uint8_t *active = reinterpret_cast<uint8_t *>(prev + cols_most);
+  const size_t smem = lane_smem<T>(d);
+  if (smem > (size_t)f->gpu->smem_optin) throw host::Error(host::kInvalidArgument, "the lane solve's block does not fit in shared memory");
+  cuda_check(cudaFuncSetAttribute(lane_solve_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  LaneArgs a{};
+  a.n = (int32_t)n;
+  a.slots = d->slots, a.page_bytes = d->page_bytes, a.partials = d->partials;
+  a.blob = d->blob.get();
+  a.warp_page = d->warp_page.get();
+  a.error = f->error.get();
+  a.group_active = active;
+  // b's row i sits in work row in_pos[i] = i (the work array follows b's own order), so in_pos also
+  // maps the lane layout's natural rows
+  const int32_t *natural = d->in_pos.get();
+  for (int64_t g0 = 0; g0 < groups_all; g0 += per_launch) {
+    const int64_t groups = std::min(per_launch, groups_all - g0);
+    const int64_t cols = std::min(count - g0 * 32, groups * 32);
+    const double *bg = b + g0 * 32 * ldb;
+    const unsigned io_grid = (unsigned)lane_io_blocks(groups, n);
+    const int64_t init_n = std::max(cols, groups);
+    lane_refine_init_kernel<<<(unsigned)((init_n + 255) / 256), 256, 0, stream>>>(groups, cols, rmax, bmax, prev, active);
+    cuda_check(cudaGetLastError(), "lane_refine_init_kernel launch");
+    lane_in_kernel<double><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(bg, ldb, cols, (int32_t)n, groups, natural, bl, nullptr);
+    cuda_check(cudaGetLastError(), "lane_in_kernel launch");
+    lane_in_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(bg, ldb, cols, (int32_t)n, groups, d->in_pos.get(), work,
+                                                                  nullptr);
+    cuda_check(cudaGetLastError(), "lane_in_kernel launch");
+    for (int32_t pass = 0; pass <= max_steps; ++pass) {
+      lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
+      cuda_check(cudaGetLastError(), "lane_solve_kernel launch");
+      lane_update_kernel<T><<<io_grid, 256, 0, stream>>>(work, d->out_pos.get(), xl, (int32_t)n, groups, active, pass == 0);
+      cuda_check(cudaGetLastError(), "lane_update_kernel launch");
+      lane_residual_kernel<<<io_grid, 256, 0, stream>>>(bl, xl, work, d->in_pos.get(), (int32_t)n, groups, cols,
+                                                        f->a_csr_ptr.get(), f->a_csr_idx.get(), f->a_csr_val.get(), active,
+                                                        rmax, pass == 0 ? bmax : nullptr);
+      cuda_check(cudaGetLastError(), "lane_residual_kernel launch");
+      lane_refine_decide_kernel<<<(unsigned)((groups + 127) / 128), 128, 0, stream>>>(
+          groups, cols, pass, max_steps, tolerance, rmax, bmax, prev, active, ratio_out ? ratio_out + g0 * 32 : nullptr,
+          steps_out ? steps_out + g0 * 32 : nullptr);
+      cuda_check(cudaGetLastError(), "lane_refine_decide_kernel launch");
+    }
+    lane_out_kernel<double><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(xl, cols, (int32_t)n, groups, natural,
+                                                                      x + g0 * 32 * ldx, ldx);
+    cuda_check(cudaGetLastError(), "lane_out_kernel launch");
+  }
+}
+}  // namespace yb
 
 extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out,
                                                 int64_t ldx, int64_t count, int32_t max_steps, double tolerance,
@@ -1250,6 +1333,15 @@ extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rh
     if (count == 0 || f->n == 0) return YB_OK;
     require(!f->single, "a single-row factor needs no refinement: use yb_solve_many_device");
     cudaStream_t s = stream ? (cudaStream_t)stream : f->gpu->stream;
+    const TileConfig &t32 = f->tile32;
+    if (t32.kind == kTileLane || (t32.kind == kTileAuto && count >= t32.lane_min_count)) {
+      DeviceLane *d = lane_pick<float>(f, t32, s);
+      if (d && (t32.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
+        launch_lane_refined(f, d, d_rhs, ldb, d_out, ldx, count, max_steps, tolerance, d_ratio, d_steps, s);
+        return YB_OK;
+      }
+      if (t32.kind == kTileLane) throw host::Error(host::kInvalidArgument, "the factor admits no lane layout");
+    }
     TileConfig cfg = resolve<float>(f, f->tile32);
     if (cfg.kind != kTileDomain)
       throw host::Error(host::kInvalidArgument, "the refined solve needs the domain solve, which this factor does not admit");

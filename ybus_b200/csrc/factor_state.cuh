@@ -182,6 +182,9 @@ struct yb_factor {
   // the solution slots, FP64
   int64_t a_rows = -1;
   yb::DeviceArray<int32_t> a_ptr, a_idx;
+  yb::DeviceArray<int32_t> a_csr_ptr, a_csr_idx;  // A as attached (CSR, natural order)
+  yb::DeviceArray<double> a_csr_val;
+  yb::DeviceArray<uint8_t> refine_state;  // the lane refinement's per-column maxima and per-group flags
   yb::DeviceArray<double> a_val;
   yb::DeviceArray<double> refine_scratch;  // per block n * W residuals
   // a complex LU factor (yb_factor_from_lu_complex): its plan, its sweeps in complex128 and

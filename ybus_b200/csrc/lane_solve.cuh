@@ -37,6 +37,7 @@ struct LaneArgs {
   const uint8_t *__restrict__ blob;       // every warp's pages
   const int32_t *__restrict__ warp_page;  // [warps + 1]
   int32_t *error;                         // set to 1 if a wait ran out or a stream is malformed
+  const uint8_t *group_active;            // [groups] 0: the group is skipped; null: every group runs
 };
 
 // A warp's shared memory: live slots, the prefetch ring, the page ring and its barriers.
@@ -131,6 +132,7 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
   // The warp index through a shuffle from lane 0: the compiler then knows it (and the shared
   // offsets, record fields and branches derived from it) to be the same across the warp, and keeps
   // the records' decoding on the uniform datapath instead of every lane's registers.
+  if (a.group_active && !a.group_active[blockIdx.x]) return;  // the whole block, before any barrier
   const int lane = threadIdx.x & 31, warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
   constexpr int S = kLaneRing;  // known here, so the ring's slot and phase are a mask and a shift
   const int PB = a.page_bytes;
@@ -399,11 +401,12 @@ template <class T>
 __global__ void __launch_bounds__(kLaneIoWarps * 32) lane_in_kernel(const double *__restrict__ b, int64_t ldb, int64_t count,
                                                                    int32_t n, int64_t groups,
                                                                    const int32_t *__restrict__ in_pos,
-                                                                   T *__restrict__ work) {
+                                                                   T *__restrict__ work,
+                                                                   const uint8_t *__restrict__ group_active) {
   const int lane = threadIdx.x & 31;
   const int64_t w = (int64_t)blockIdx.x * kLaneIoWarps + (threadIdx.x >> 5);
   const int64_t chunks = (n + 31) / 32, g = w / chunks;
-  if (g >= groups) return;
+  if (g >= groups || (group_active && !group_active[g])) return;
   const int i = (int)(w % chunks) * 32 + lane;
   if (i >= n) return;
   double v[32];
