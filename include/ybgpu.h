@@ -377,11 +377,15 @@ int32_t yb_solve_batch_complex(int64_t networks, yb_factor *const *factors, cons
  * columns mapped to the factor's solution order is kept on the device. */
 int32_t yb_factor_attach_matrix(yb_factor *f, const int64_t *a_ptr, const int64_t *a_idx, const double *a_val);
 /* No ybus counterpart on the GPU; the CPU's is `solve_refined_normwise` (accuracy.rs:83-122):
- * the substitutions in FP32, the residual and the update x += d in FP64 against the attached A (the
- * residual kept as r -= A d in FP64, the residual of x to rounding), up to max_steps corrections
- * per tile, until every column's ||r||inf / ||b||inf <= tolerance or the residual stops halving. Device arrays as yb_solve_many_device; d_ratio (double,
- * count) and d_steps (int32, count) receive each column's final relative residual and corrections
- * (either may be NULL). Needs the domain solve (YB_ERROR_INVALID_ARGUMENT otherwise). */
+ * the substitutions in FP32, the residual and the update x += d in FP64 against the attached A, up
+ * to max_steps corrections per tile, until every column's ||r||inf / ||b||inf <= tolerance or the
+ * residual stops halving. From the FP32 lane threshold on (yb_factor_set_lane_min_count) the passes
+ * run on the lane solve, a tile being a group of 32 columns, with b and x held in FP64 beside the
+ * work array (r = b - A x each pass); below it, or when the factor admits no lane layout, on the
+ * domain solve with the refinement fused into its launch (r kept as r -= A d, the residual of x to
+ * rounding). Device arrays as yb_solve_many_device; d_ratio (double, count) and d_steps (int32,
+ * count) receive each column's final relative residual and corrections (either may be NULL).
+ * YB_ERROR_INVALID_ARGUMENT when the factor admits neither solve. */
 int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
                                      int64_t count, int32_t max_steps, double tolerance, double *d_ratio,
                                      int32_t *d_steps, void *stream);
