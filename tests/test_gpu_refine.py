@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle.oracle as orc
-from fixtures import random_spd, right_hand_sides, worst_relative_difference
+from fixtures import random_spd, random_square, right_hand_sides, worst_relative_difference
 from ybus_b200 import FP32, CudaError, GpuFactor, grids, host
 
 pytestmark = pytest.mark.gpu
@@ -99,3 +99,30 @@ def test_lane_refinement_stops_each_group_on_its_own(gpu):
     assert (steps[32:] >= 1).all() and ratio[32:].max() <= TOL
     p, i, v = a.to_csr().arrays()
     assert max(orc.relative_residual(p, i, v, x[k], rhs[k]) for k in range(32, 69)) <= TOL
+
+
+def test_lane_refinement_of_an_lu_factor_or_its_refusal(gpu):
+    # an LU factor with pivoting: x's rows come from other work rows than b's, which the update
+    # follows; a factor that admits no lane layout is refused when the lane solve is forced
+    import torch
+    a = random_square(250, 4, 3)
+    factor = GpuFactor.from_lu(gpu, host.lu(a))
+    factor.attach_matrix(a)
+    factor.set_tile_kind(FP32, LANE)
+    rhs = right_hand_sides(250, 40, 5)
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    ratio = torch.empty(40, dtype=torch.float64, device="cuda")
+    try:
+        factor.lane_info(FP32)
+    except CudaError:
+        with pytest.raises(CudaError):
+            factor.solve_many_refined_device(b.data_ptr(), x.data_ptr(), 40, 4, TOL, ratio.data_ptr())
+        return
+    factor.solve_many_refined_device(b.data_ptr(), x.data_ptr(), 40, 4, TOL, ratio.data_ptr())
+    gpu.synchronize()
+    factor.check_error()
+    p, i, v = a.to_csr().arrays()
+    xs = x.cpu().numpy()
+    assert max(orc.relative_residual(p, i, v, xs[k], rhs[k]) for k in range(40)) <= TOL
+    assert ratio.cpu().numpy().max() <= TOL
