@@ -35,7 +35,8 @@ WORKLOAD = "10k-bus PTDF block: B' 9,999 x 9,999 AMD Cholesky, 13,499 branch RHS
 N_BUS, EXTRA = 10000, 3500
 FALLBACK_HBM_GBS = 6650.0
 IR_TOLERANCE, IR_MAX_STEPS = 1e-10, 3
-LANE_MIN_COUNT, LANE_AUTO_SLOTS = 3072, 64  # the library's automatic choice of the lane solve
+LANE_MIN_COUNT, LANE_AUTO_SLOTS = 3072, 64
+LANE_REFINE_MIN_COUNT = 5120  # the refined solve's own threshold for the lane solve  # the library's automatic choice of the lane solve
 
 
 def parse():
@@ -389,9 +390,9 @@ def main():
         return replicas.max_over_ranks(elapsed_ms), launch_ms, kernels
 
     # which solve each mode runs: from the lane threshold on, the plain FP64 solve takes the lane
-    # solve (three launches: gather, solve, scatter) and the refined solve its FP32 lane passes with
-    # an FP64 update and residual between them; below it, the domain solve (the refined one with its
-    # refinement fused into one launch)
+    # solve (three launches: gather, solve, scatter), and from its own higher threshold the refined
+    # solve takes FP32 lane passes with an FP64 update and residual between them; below them, the
+    # domain solve (the refined one with its refinement fused into one launch)
     lane = None
     try:
         lane = factor.lane_info(FP64)
@@ -404,7 +405,7 @@ def main():
         lane32 = factor.lane_info(FP32)
     except Exception:
         pass
-    use_lane32 = lane32 is not None and count >= LANE_MIN_COUNT and lane32["slots"] <= LANE_AUTO_SLOTS
+    use_lane32 = lane32 is not None and count >= LANE_REFINE_MIN_COUNT and lane32["slots"] <= LANE_AUTO_SLOTS
 
     def solver_of(mode):
         if mode == "fp64" and use_lane:

@@ -379,8 +379,9 @@ int32_t yb_factor_attach_matrix(yb_factor *f, const int64_t *a_ptr, const int64_
 /* No ybus counterpart on the GPU; the CPU's is `solve_refined_normwise` (accuracy.rs:83-122):
  * the substitutions in FP32, the residual and the update x += d in FP64 against the attached A, up
  * to max_steps corrections per tile, until every column's ||r||inf / ||b||inf <= tolerance or the
- * residual stops halving. From the FP32 lane threshold on (yb_factor_set_lane_min_count) the passes
- * run on the lane solve, a tile being a group of 32 columns, with b and x held in FP64 beside the
+ * residual stops halving. From 5,120 right-hand sides on (or the FP32 lane threshold of
+ * yb_factor_set_lane_min_count, if higher) the passes run on the lane solve, a tile being a group of
+ * 32 columns, with b and x held in FP64 beside the
  * work array (r = b - A x each pass); below it, or when the factor admits no lane layout, on the
  * domain solve with the refinement fused into its launch (r kept as r -= A d, the residual of x to
  * rounding). Device arrays as yb_solve_many_device; d_ratio (double, count) and d_steps (int32,

@@ -1334,7 +1334,11 @@ extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rh
     require(!f->single, "a single-row factor needs no refinement: use yb_solve_many_device");
     cudaStream_t s = stream ? (cudaStream_t)stream : f->gpu->stream;
     const TileConfig &t32 = f->tile32;
-    if (t32.kind == kTileLane || (t32.kind == kTileAuto && count >= t32.lane_min_count)) {
+    // the refinement's passes cost more than the plain solve's launches, so its crossover with the
+    // domain refinement lies higher (10k-bus block: 2.15 against 2.33 ms at 4,096 right-hand sides,
+    // 3.36 against 3.02 ms at 6,144)
+    constexpr int64_t kLaneRefineMinCount = 5120;
+    if (t32.kind == kTileLane || (t32.kind == kTileAuto && count >= std::max(t32.lane_min_count, kLaneRefineMinCount))) {
       DeviceLane *d = lane_pick<float>(f, t32, s);
       if (d && (t32.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane_refined(f, d, d_rhs, ldb, d_out, ldx, count, max_steps, tolerance, d_ratio, d_steps, s);
