@@ -1,16 +1,20 @@
 #!/usr/bin/env python
-"""Benchmark: the full PTDF block of the 10,000-bus synthetic grid, solved on the GPU.
+"""Benchmark of the factor-once / solve-many path on the synthetic 10,000-bus grid.
 
-Workload (synthetic, seeded): 10,000 buses uniform in the unit square, a random spanning tree of
-the k=4 nearest-neighbour graph plus 3,500 further neighbour edges (13,499 branches), reactance
-log-uniform in [0.005, 0.5]; B' (9,999 x 9,999) factored once by AMD-ordered Cholesky on the host.
-A step solves all 13,499 branch right-hand sides A'diag(1/x)e_k (restricted to the non-slack buses)
-with that factor. The right-hand sides (1.08 GB) are larger than L2, so no flush is needed.
+Headline workload (seeded; ybus_b200/configs.py): 10,000 buses uniform in the unit square, a random
+spanning tree of the k=4 nearest-neighbour graph plus 3,500 further neighbour edges (13,499
+branches), reactance log-uniform in [0.005, 0.5]; B' (9,999 x 9,999) factored once by AMD-ordered
+Cholesky on the host. A step solves all 13,499 branch right-hand sides A'diag(1/x)e_k (restricted
+to the non-slack buses) with that factor; on N GPUs the columns are split over the ranks. The
+right-hand sides (1.08 GB) are larger than L2, so no flush is needed.
 
 Our arm times, on the device with CUDA events, K steps of the solve with inputs resident in HBM
-(`value`), and separately the same solve through the host-array C ABI call with pinned host
-buffers, copies included (`e2e`). `--impl reference` times the reference's CPU solve path (the
-oracle's restatement of ybus_sparse's `par_solve_many`) on all host cores.
+(`value`: FP64, and FP32 substitution with FP64 refinement to 1e-10, the faster passing mode as the
+headline), the same block in blocks of 64, 256 and 1,024 columns (`modes_by_width`), the solve
+through the host-array C ABI call with pinned host buffers, copies included (`e2e`), and the
+other configurations of the path (`workloads`: the N-1 screening batch, the flow-loss adjoint, the
+complex multi-network batch). `--impl reference` times the reference's CPU solve path (the
+oracle's restatement of ybus_sparse's `par_solve_many`) on all host cores, loading no GPU library.
 """
 from __future__ import annotations
 
@@ -32,11 +36,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = "RHS solved/s @1e-10 resid, 10k buses: batched FP32+IR vs FP64 GPU; HBM GB/s"
 UNIT = "RHS/s"
 WORKLOAD = "10k-bus PTDF block: B' 9,999 x 9,999 AMD Cholesky, 13,499 branch RHS"
-N_BUS, EXTRA = 10000, 3500
 FALLBACK_HBM_GBS = 6650.0
 IR_TOLERANCE, IR_MAX_STEPS = 1e-10, 3
-LANE_MIN_COUNT, LANE_AUTO_SLOTS = 3072, 64
-LANE_REFINE_MIN_COUNT = 5120  # the refined solve's own threshold for the lane solve  # the library's automatic choice of the lane solve
+WIDTHS = (64, 256, 1024)
 
 
 def parse():
@@ -48,26 +50,27 @@ def parse():
     p.add_argument("--mode", default="auto", choices=["auto", "fp64", "fp32_ir"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="time the headline modes only (no block widths, workloads or comparison): for profiling")
     p.add_argument("--rhs", type=int, default=0, help="solve only the first RHS (a smaller case for profiling)")
     p.add_argument("--workload", default="ptdf", choices=["ptdf", "n1", "adjoint", "complex"],
-                   help="ptdf: the headline PTDF block; n1, adjoint, complex: the N-1 screening batch, the flow-loss "
-                        "adjoint and the complex multi-network batch, each timed on its own (one GPU)")
+                   help="ptdf: the headline PTDF block with the other workloads as extra keys; n1, adjoint, complex: "
+                        "one of the other workloads alone, one JSON line")
     return p.parse_args()
 
 
+def headline_config(count: int, n: int, world: int) -> dict:
+    """The workload's description, the same for both arms."""
+    return {"workload": WORKLOAD, "rhs_per_step": count, "n": n, "flush": "inputs (1.08 GB) > L2",
+            "parallelism": f"RHS columns split over {world} GPU(s)"}
+
+
 def workload():
-    from ybus_b200 import grids, host
-    g = grids.make_grid(N_BUS, EXTRA, grids.SEED_BASE + 2)
-    r, c, v = grids.bbus_triplets(g)
-    keep = np.arange(1, N_BUS)
-    bp = host.Matrix.from_triplets(N_BUS, N_BUS, r, c, v).select(keep, keep)
+    from ybus_b200 import configs, host
+    g = configs.grid_10k()
+    bp = configs.bprime(g)
     chol = host.cholesky(bp)
-    rhs = np.zeros((g.n_branch, N_BUS))
-    k = np.arange(g.n_branch)
-    rhs[k, g.frm] += g.susceptance
-    rhs[k, g.to] -= g.susceptance
-    rhs = np.ascontiguousarray(rhs[:, 1:])
-    return g, bp, chol, rhs
+    return g, bp, chol, configs.branch_rhs(g)
 
 
 def measured_peak():
@@ -159,160 +162,226 @@ def traffic_of(result: dict, count: int, n: int):
     return None
 
 
-def cpu_baseline(chol, rhs, seconds_target: float = 10.0) -> dict:
+def _time_oracle(chol, rhs, threads: int, passes: int, seconds: float) -> tuple[float, int]:
+    """Median seconds of `passes` oracle solves of `rhs` on `threads` threads (fewer if the time
+    budget runs out), after one warm-up on a slice."""
     from oracle import oracle as orc
-    cores = os.cpu_count() or 1
-    # bounded sample: enough RHS for ~1-3 s per pass on all cores
-    sample = rhs[: min(rhs.shape[0], 13499)]
-    orc.solve_many(chol, sample[:256], threads=cores)  # warm-up
-    times = []
-    t_total = 0.0
-    while len(times) < 5 and t_total < seconds_target:
+    orc.solve_many(chol, rhs[: min(64, rhs.shape[0])], threads=threads)
+    times, total = [], 0.0
+    while len(times) < passes and total < seconds:
         t0 = time.perf_counter()
-        orc.solve_many(chol, sample, threads=cores)
-        dt = time.perf_counter() - t0
-        times.append(dt)
-        t_total += dt
-    med = statistics.median(times)
-    return {"value": sample.shape[0] / med, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{sample.shape[0]} PTDF RHS of the 10k-bus B' factor, median of {len(times)} passes, "
-                      f"oracle par_solve_many on {cores} threads"}
+        orc.solve_many(chol, rhs, threads=threads)
+        times.append(time.perf_counter() - t0)
+        total += times[-1]
+    return statistics.median(times), len(times)
+
+
+def cpu_baseline(chol, rhs) -> dict:
+    """The oracle's par_solve_many on every host core (13,499 RHS, median of up to 5 passes) and on
+    one thread (a 1,000-RHS sample, median of up to 3 passes)."""
+    cores = os.cpu_count() or 1
+    med, passes = _time_oracle(chol, rhs, cores, 5, 10.0)
+    one = rhs[:1000]
+    med1, passes1 = _time_oracle(chol, one, 1, 3, 10.0)
+    return {"value": rhs.shape[0] / med, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{rhs.shape[0]} PTDF RHS of the 10k-bus B' factor, median of {passes} passes, oracle "
+                      f"par_solve_many on {cores} threads",
+            "value_1thread": one.shape[0] / med1,
+            "sample_1thread": f"the first {one.shape[0]} of those RHS, median of {passes1} passes on 1 thread"}
 
 
 def run_reference(a):
+    """The reference's CPU path: the oracle's restatement of ybus_sparse's par_solve_many on every
+    host core, on the factor the host producer (libybhost.so alone) makes. Rank 0 only."""
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return 0
     g, bp, chol, rhs = workload()
     from oracle import oracle as orc
     cores = os.cpu_count() or 1
-    for _ in range(a.warmup):
+    if a.rhs > 0:
+        rhs = np.ascontiguousarray(rhs[: a.rhs])
+    for _ in range(max(a.warmup, 1)):
         orc.solve_many(chol, rhs[:512], threads=cores)
-    per_step = min(rhs.shape[0], 13499)
     t0 = time.perf_counter()
     for _ in range(a.steps):
-        orc.solve_many(chol, rhs[:per_step], threads=cores)
+        orc.solve_many(chol, rhs, threads=cores)
     dt = time.perf_counter() - t0
-    value = per_step * a.steps / dt
+    value = rhs.shape[0] * a.steps / dt
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": dt / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": dt / a.steps * 1e3, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "rhs_per_step": per_step, "n": chol.n, "flush": "inputs > L2"},
+            "config": headline_config(rhs.shape[0], chol.n, a.gpus),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{per_step} PTDF RHS per step, oracle par_solve_many (restating "
+                             "sample": f"{rhs.shape[0]} PTDF RHS per step, oracle par_solve_many (restating "
                                        f"ybus_sparse factorization.rs:71-92) on {cores} threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    maps = Path("/proc/self/maps")
+    if maps.exists():
+        text = maps.read_text()
+        line["native_libraries"] = sorted({n for n in ("libybhost.so", "libybgpu.so", "liboracle.so") if n in text})
     print(json.dumps(line), flush=True)
     return 0
+
+
+# ---- the other workloads of the path ------------------------------------------------------------
+
+def _timed_wall(fn, steps: int, warm: int, device: int):
+    """Wall time per step of `fn` (it synchronises before returning: its API takes host arrays),
+    the max over ranks, with the clocks sampled meanwhile."""
+    import torch
+
+    from ybus_b200 import replicas
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    replicas.barrier()
+    clocks = ClockSampler(device).start()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        out = fn()
+    torch.cuda.synchronize()
+    dt = replicas.max_over_ranks((time.perf_counter() - t0) / steps)
+    return dt, out, clocks.stop()
+
+
+def workload_n1(gpu, steps: int, warm: int, rank: int, world: int, device: int) -> dict:
+    """Configuration 3: 2,000 non-bridge outages of the 10,000-bus grid with U[1, 64] injection
+    scenarios each, screened for their largest loading in one captured launch per rank (cases split
+    over the ranks by LPT on their scenario counts), pinned host arrays in and out."""
+    import torch
+
+    from ybus_b200 import FP32, FP64, configs, replicas
+    from ybus_b200.dc import DcNetwork
+    g = configs.grid_10k()
+    net = DcNetwork.from_grid(gpu, g)
+    cases = configs.n1_cases(g, net.bridges())
+    counts = np.diff(cases.scenario_ptr)
+    mine = replicas.lpt(counts + 1, world)[rank]
+    sp = np.concatenate([[0], np.cumsum(counts[mine])]).astype(np.int64)
+    cols = np.concatenate([np.arange(cases.scenario_ptr[c], cases.scenario_ptr[c + 1]) for c in mine])
+    inj = torch.from_numpy(np.ascontiguousarray(cases.injections[cols])).pin_memory().numpy()
+    outaged = cases.outaged[mine]
+    modes = {}
+    for name, prec in (("fp64", FP64), ("fp32_ir", FP32)):
+        dt, (rows, vals, bad, sing), ck = _timed_wall(
+            lambda: net.outage_loadings_batch(outaged, sp, inj, cases.weights, prec), steps, warm, device)
+        modes[name] = {"scenarios_s": int(cases.scenario_ptr[-1]) / dt, "ms_per_step": dt * 1e3,
+                       "not_finite": int(bad.sum()), "singular": int(sing.sum()), "clocks": ck}
+    best = max(modes, key=lambda m: modes[m]["scenarios_s"])
+    return {"metric": "N-1 scenarios screened/s (largest loading per scenario), pinned host arrays in and out",
+            "value": modes[best]["scenarios_s"], "unit": "scenarios/s", "higher_is_better": True,
+            "config": {"n_bus": configs.N_BUS, "outages": int(cases.outaged.size),
+                       "scenarios": int(cases.scenario_ptr[-1]), "h2d_bytes_per_step": int(inj.nbytes),
+                       "mode": best, "split": f"cases by LPT over {world} GPU(s)"}, "modes": modes}
+
+
+def workload_adjoint(gpu, steps: int, warm: int, rank: int, world: int, device: int) -> dict:
+    """Configuration 4: the flow-loss forward and backward over 1,024 scenarios of the 10,000-bus
+    grid (dL/dp and dL/db), pinned host arrays in and out; on N GPUs the scenarios are split and
+    dL/db and the loss are summed over the ranks in rank order."""
+    import torch
+
+    from ybus_b200 import configs, replicas
+    from ybus_b200.dc import DcNetwork, FlowLoss
+    g = configs.grid_10k()
+    net = DcNetwork.from_grid(gpu, g)
+    p, limits = configs.adjoint_scenarios(g)
+    share = replicas.shard(p.shape[0], rank, world)
+    pm = torch.from_numpy(np.ascontiguousarray(p[share.start:share.stop])).pin_memory().numpy()
+    gp_out = torch.zeros(pm.shape, dtype=torch.float64).pin_memory().numpy()
+    gb_out = np.zeros(g.n_branch)
+    loss_fn = FlowLoss(net, pm.shape[0])
+
+    def step():
+        loss = loss_fn.forward(pm, limits)
+        gp, gb = loss_fn.backward(gp_out, gb_out)
+        total = replicas.sum_in_rank_order(np.append(gb, loss))
+        return total[-1], gp, total[:-1]
+
+    dt, (loss, gp, gb), ck = _timed_wall(step, steps, warm, device)
+    return {"metric": "flow-loss forward + backward scenarios/s (dL/dp and dL/db), pinned host arrays in and out",
+            "value": p.shape[0] / dt, "unit": "scenarios/s", "higher_is_better": True, "ms_per_step": dt * 1e3,
+            "config": {"n_bus": configs.N_BUS, "scenarios": int(p.shape[0]), "loss": float(loss),
+                       "finite": bool(np.isfinite(gp).all() and np.isfinite(gb).all()),
+                       "split": f"scenarios over {world} GPU(s), dL/db summed in rank order"}, "clocks": ck}
+
+
+def workload_complex(gpu, steps: int, warm: int, rank: int, world: int, device: int) -> dict:
+    """Configuration 5: 16 complex Ybus networks of 500 to 70,000 buses, 128 right-hand sides each,
+    in one launch per rank (networks split over the ranks by LPT on factor entries x right-hand
+    sides), device arrays, complex128 and complex64 with complex128 refinement."""
+    import torch
+
+    from ybus_b200 import FP32, FP64, GpuFactor, configs, replicas, solve_batch_complex
+    sizes = configs.complex_sizes()
+    nets = [configs.complex_network(int(n), i) for i, n in enumerate(sizes)]
+    work = [(net.lu.l.idx.size + net.lu.u.idx.size) * net.rhs.shape[0] for net in nets]
+    mine = replicas.lpt(work, world)[rank]
+    factors, bs, xs, rs = [], [], [], []
+    for i in mine:
+        net = nets[i]
+        f = GpuFactor.from_lu_complex(gpu, net.lu)
+        f.attach_matrix_complex(net.ybus)
+        factors.append(f)
+        bs.append(torch.from_numpy(net.rhs.view(np.float64).copy()).cuda())
+        xs.append(torch.empty_like(bs[-1]))
+        rs.append(torch.empty(net.rhs.shape[0], dtype=torch.float64, device="cuda"))
+    total = sum(net.rhs.shape[0] for net in nets)
+    modes = {}
+    for name, prec in (("c128", FP64), ("c64_ir", FP32)):
+        def run():
+            st = solve_batch_complex(factors, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs],
+                                     [nets[i].rhs.shape[0] for i in mine], prec, 3, 1e-10, [r.data_ptr() for r in rs])
+            torch.cuda.synchronize()
+            return st
+        dt, st, ck = _timed_wall(run, steps, warm, device)
+        worst = replicas.max_over_ranks(max((float(r.max()) for r in rs), default=0.0))
+        modes[name] = {"rhs_s": total / dt, "ms_per_step": dt * 1e3, "corrections": st, "max_rel_residual": worst,
+                       "clocks": ck}
+    passing = [m for m in modes if modes[m]["max_rel_residual"] <= 1e-10]
+    best = max(passing or list(modes), key=lambda m: modes[m]["rhs_s"])
+    return {"metric": "complex RHS solved/s over a 16-network Ybus batch, one launch",
+            "value": modes[best]["rhs_s"], "unit": "RHS/s", "higher_is_better": True,
+            "config": {"networks": [int(v) for v in sizes], "rhs_per_network": configs.COMPLEX_RHS, "mode": best,
+                       "split": f"networks by LPT over {world} GPU(s)"}, "modes": modes}
+
+
+WORKLOADS = {"n1": workload_n1, "adjoint": workload_adjoint, "complex": workload_complex}
+
+
+def init_ranks():
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from ybus_b200 import replicas
+    rank, world, local = replicas.rank_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
 
 
 def run_workload(a) -> int:
-    """The other workloads of the solve path, one GPU, one JSON line each: the N-1 screening batch
-    (10,000-bus grid, 2,000 non-bridge outages with U[1, 64] injection scenarios each), the
-    flow-loss adjoint (1,024 scenarios, forward and backward), and the complex multi-network batch
-    (16 Ybus networks of 500 to 70,000 buses, 128 right-hand sides each, complex128 and complex64
-    with complex128 refinement). Pinned host arrays in and out for the first two (their API takes
-    host arrays, so the copies are inside the time); device arrays for the third."""
-    import torch
-
-    from ybus_b200 import FP32, FP64, Gpu, GpuFactor, grids, host, solve_batch_complex
-    from ybus_b200.dc import DcNetwork, FlowLoss
-
-    if int(os.environ.get("WORLD_SIZE", 1)) > 1:
-        if int(os.environ.get("RANK", 0)) == 0:
-            print(json.dumps({"workload": a.workload, "unavailable": "the extra workloads run on one GPU"}))
-        return 0
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    gpu = Gpu.new(int(os.environ.get("LOCAL_RANK", 0)))
-    steps, warm = max(a.steps, 1), max(a.warmup, 1)
-    line = {"workload": a.workload, "n_gpus": 1, "steps": steps, "warmup": warm, "data": "synthetic"}
-
-    def wall(fn):
-        for _ in range(warm):
-            fn()
-        torch.cuda.synchronize()
-        clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", 0))).start()
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            out = fn()
-        torch.cuda.synchronize()
-        dt = (time.perf_counter() - t0) / steps
-        return dt, out, clocks.stop()
-
-    if a.workload == "n1":
-        g = grids.make_grid(N_BUS, EXTRA, grids.SEED_BASE + 2)
-        net = DcNetwork.from_grid(gpu, g)
-        rng = np.random.default_rng(grids.SEED_BASE + 3)
-        outaged = rng.choice(np.flatnonzero(~net.bridges()), 2000, replace=False)
-        counts = rng.integers(1, 65, outaged.size)
-        sp = np.concatenate([[0], np.cumsum(counts)])
-        inj = rng.normal(0.0, 0.1, (int(sp[-1]), g.n_bus))
-        inj[:, 0] = -inj[:, 1:].sum(axis=1)
-        inj = torch.from_numpy(inj).pin_memory().numpy()  # pinned, as the headline's e2e
-        weights = 1.0 / rng.uniform(0.5, 2.0, g.n_branch)
-        modes = {}
-        for name, prec in (("fp64", FP64), ("fp32_ir", FP32)):
-            dt, (rows, vals, bad, sing), ck = wall(lambda: net.outage_loadings_batch(outaged, sp, inj, weights, prec))
-            modes[name] = {"scenarios_s": sp[-1] / dt, "ms_per_step": dt * 1e3, "not_finite": int(bad.sum()),
-                           "singular": int(sing.sum()), "clocks": ck}
-        best = max(modes, key=lambda m: modes[m]["scenarios_s"])
-        line.update({"metric": "N-1 scenarios screened/s (largest loading per scenario), pinned host arrays in and out",
-                     "value": modes[best]["scenarios_s"], "unit": "scenarios/s", "higher_is_better": True,
-                     "config": {"n_bus": N_BUS, "outages": int(outaged.size), "scenarios": int(sp[-1]),
-                                "h2d_bytes_per_step": int(inj.nbytes), "mode": best}, "modes": modes})
-    elif a.workload == "adjoint":
-        g = grids.make_grid(N_BUS, EXTRA, grids.SEED_BASE + 2)
-        net = DcNetwork.from_grid(gpu, g)
-        rng = np.random.default_rng(grids.SEED_BASE + 4)
-        count = 1024
-        p = rng.normal(0.0, 0.1, (count, g.n_bus))
-        p[:, 0] = -p[:, 1:].sum(axis=1)
-        p = torch.from_numpy(p).pin_memory().numpy()  # pinned host arrays in and out
-        gp_out = torch.zeros((count, g.n_bus), dtype=torch.float64).pin_memory().numpy()
-        limits = rng.uniform(0.5, 2.0, g.n_branch)
-        loss_fn = FlowLoss(net, count)
-
-        def step():
-            loss = loss_fn.forward(p, limits)
-            return loss, loss_fn.backward(gp_out)
-        dt, (loss, (gp, gb)), ck = wall(step)
-        line.update({"metric": "flow-loss forward + backward scenarios/s (dL/dp and dL/db), pinned host arrays in and out",
-                     "value": count / dt, "unit": "scenarios/s", "higher_is_better": True, "ms_per_step": dt * 1e3,
-                     "config": {"n_bus": N_BUS, "scenarios": count, "loss": loss,
-                                "finite": bool(np.isfinite(gp).all() and np.isfinite(gb).all())}, "clocks": ck})
-    else:
-        rng = np.random.default_rng(grids.SEED_BASE + 5)
-        sizes = np.sort(np.exp(rng.uniform(np.log(500), np.log(70000), 16)).astype(int))[::-1]
-        factors, bs, xs, rs = [], [], [], []
-        for i, n_bus in enumerate(sizes):
-            gc = grids.make_complex_grid(int(n_bus), grids.SEED_BASE + 60 + i)
-            r, c, v = grids.ybus_triplets(gc)
-            m = host.Matrix.from_triplets(int(n_bus), int(n_bus), r, c, v, by_rows=False)
-            f = GpuFactor.from_lu_complex(gpu, host.lu(m, host.COLAMD))
-            f.attach_matrix_complex(m)
-            factors.append(f)
-            b = rng.standard_normal((128, int(n_bus))) + 1j * rng.standard_normal((128, int(n_bus)))
-            bs.append(torch.from_numpy(b.view(np.float64).copy()).cuda())
-            xs.append(torch.empty_like(bs[-1]))
-            rs.append(torch.empty(128, dtype=torch.float64, device="cuda"))
-        total = 128 * len(sizes)
-        modes = {}
-        for name, prec in (("c128", FP64), ("c64_ir", FP32)):
-            dt, st, ck = wall(lambda: solve_batch_complex(factors, [b.data_ptr() for b in bs],
-                                                          [x.data_ptr() for x in xs], [128] * len(sizes), prec,
-                                                          3, 1e-10, [r.data_ptr() for r in rs]))
-            worst = max(float(r.max()) for r in rs) if prec == FP32 else None
-            modes[name] = {"rhs_s": total / dt, "ms_per_step": dt * 1e3, "corrections": st,
-                           "max_rel_residual": worst, "clocks": ck}
-        passing = [m for m in modes if m == "c128" or (modes[m]["max_rel_residual"] or 1) <= 1e-10]
-        best = max(passing, key=lambda m: modes[m]["rhs_s"])
-        line.update({"metric": "complex RHS solved/s over a 16-network Ybus batch, one launch",
-                     "value": modes[best]["rhs_s"], "unit": "RHS/s", "higher_is_better": True,
-                     "config": {"networks": [int(v) for v in sizes], "rhs_per_network": 128, "mode": best},
-                     "modes": modes})
-    print(json.dumps(line), flush=True)
+    """One of the other workloads alone: one JSON line (rank 0)."""
+    from ybus_b200 import Gpu
+    rank, world, local = init_ranks()
+    gpu = Gpu.new(local)
+    line = {"workload": a.workload, "n_gpus": world, "steps": max(a.steps, 1), "warmup": max(a.warmup, 1),
+            "data": "synthetic"}
+    line.update(WORKLOADS[a.workload](gpu, max(a.steps, 1), max(a.warmup, 1), rank, world, local))
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
     return 0
 
+
+# ---- the headline ---------------------------------------------------------------------------------
 
 def main():
     a = parse()
@@ -325,16 +394,13 @@ def main():
 
     from ybus_b200 import FP32, FP64, Gpu, GpuFactor, replicas
 
-    rank, world, local = replicas.rank_info()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-
-    g, bp, chol, rhs = workload()
+    rank, world, local = init_ranks()
+    g, bp, chol, rhs_all = workload()
     if a.rhs > 0:
-        rhs = np.ascontiguousarray(rhs[: a.rhs])
+        rhs_all = np.ascontiguousarray(rhs_all[: a.rhs])
+    total = rhs_all.shape[0]
+    mine = replicas.shard(total, rank, world)
+    rhs = np.ascontiguousarray(rhs_all[mine.start:mine.stop])
     n, count = chol.n, rhs.shape[0]
     gpu = Gpu.new(local)
     factor = GpuFactor.from_cholesky(gpu, chol)
@@ -351,24 +417,31 @@ def main():
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
 
-    # each mode: one launch per step over the whole block
-    runs = {
-        "fp64": lambda: factor.solve_many_device(d_b.data_ptr(), d_x.data_ptr(), count, FP64, sh),
-        "fp32_ir": lambda: factor.solve_many_refined_device(d_b.data_ptr(), d_x.data_ptr(), count, IR_MAX_STEPS,
-                                                            IR_TOLERANCE, d_ratio.data_ptr(), d_steps.data_ptr(), sh),
-    }
+    def solve(mode, cols=None, off=0):
+        c = count if cols is None else cols
+        b, x = d_b.data_ptr() + off * n * 8, d_x.data_ptr() + off * n * 8
+        if mode == "fp64":
+            factor.solve_many_device(b, x, c, FP64, sh)
+        else:
+            factor.solve_many_refined_device(b, x, c, IR_MAX_STEPS, IR_TOLERANCE, d_ratio.data_ptr() + off * 8,
+                                             d_steps.data_ptr() + off * 4, sh)
+
+    def blocks(mode, width):  # the block solved in blocks of `width` columns, one launch each
+        for k0 in range(0, count, width):
+            solve(mode, min(width, count - k0), k0)
+
     modes = ["fp64", "fp32_ir"] if a.mode == "auto" else [a.mode]
 
-    def timed(run, lane_timing=False):
+    def timed(run, lane_timing=False, steps=None):
+        steps = a.steps if steps is None else steps
         for _ in range(max(a.warmup, 3)):
             run()
         torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         if lane_timing:  # events around each launch's gather, solve and scatter kernels
             factor.time_lane(True)
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
         for e0, e1 in evs:
@@ -389,32 +462,30 @@ def main():
         replicas.barrier()
         return replicas.max_over_ranks(elapsed_ms), launch_ms, kernels
 
-    # which solve each mode runs: from the lane threshold on, the plain FP64 solve takes the lane
-    # solve (three launches: gather, solve, scatter), and from its own higher threshold the refined
-    # solve takes FP32 lane passes with an FP64 update and residual between them; below them, the
-    # domain solve (the refined one with its refinement fused into one launch)
-    lane = None
+    # which solve each mode runs (the library's automatic choice, read back from its settings)
+    lane = lane32 = None
     try:
         lane = factor.lane_info(FP64)
     except Exception:
         pass
-    use_lane = lane is not None and count >= LANE_MIN_COUNT and lane["slots"] <= LANE_AUTO_SLOTS
-
-    lane32 = None
     try:
         lane32 = factor.lane_info(FP32)
     except Exception:
         pass
-    use_lane32 = lane32 is not None and count >= LANE_REFINE_MIN_COUNT and lane32["slots"] <= LANE_AUTO_SLOTS
+    lane_min, refine_min = factor.lane_min_count(FP64), factor.refine_lane_min_count()
+    use_lane = lane is not None and count >= lane_min and lane["slots"] <= 64
+    use_lane32 = lane32 is not None and count >= max(refine_min, factor.lane_min_count(FP32)) and lane32["slots"] <= 64
 
     def solver_of(mode):
         if mode == "fp64" and use_lane:
             return {"solver": "lane", "kernel": "lane_solve_kernel<double>", "launches_per_step": 3,
                     "lane": {k: lane[k] for k in ("warps", "slots", "domains", "top", "pages", "smem")}}
         if mode == "fp32_ir" and use_lane32:
-            # an initialisation and two gathers, per pass a solve, an update, a residual and a
-            # decision (passes after every group has stopped return at once), then the scatter
-            return {"solver": "lane", "kernel": "lane_solve_kernel<float>", "launches_per_step": 4 + 4 * (IR_MAX_STEPS + 1),
+            # an initialisation and the gather, per pass a solve, a residual (the update folded
+            # in), a decision and the restore of columns a pass made no better, and between passes
+            # the FP64 carry of x (kernels of groups that have stopped return at once)
+            return {"solver": "lane", "kernel": "lane_solve_kernel<float>",
+                    "launches_per_step": 2 + 4 * (IR_MAX_STEPS + 1) + max(0, IR_MAX_STEPS - 1),
                     "lane": {k: lane32[k] for k in ("warps", "slots", "domains", "top", "pages", "smem")}}
         prec = FP64 if mode == "fp64" else FP32
         return {"solver": "domain", "kernel": "domain_tile_kernel", "launches_per_step": 1,
@@ -425,28 +496,30 @@ def main():
     sample = np.arange(0, count, max(1, count // 64))
     cpu = orc.solve_many(chol, rhs[sample], threads=os.cpu_count() or 1)
     peak, peak_kind = measured_peak()
+
+    def check(mode, r):
+        xs = d_x.cpu().numpy()
+        r["max_rel_residual"] = max(orc.relative_residual(p, i, v, xs[k], rhs[k]) for k in range(0, count, 13))
+        r["max_rel_err_vs_oracle"] = float(max(np.abs(xs[k] - c).max() / np.abs(c).max() for k, c in zip(sample, cpu)))
+        if mode == "fp32_ir":
+            ratios, steps = d_ratio.cpu().numpy(), d_steps.cpu().numpy()
+            r.update({"device_max_ratio": float(ratios.max()), "mean_corrections": float(steps.mean()),
+                      "max_corrections": int(steps.max()), "tolerance": IR_TOLERANCE, "max_steps": IR_MAX_STEPS})
+        return r
+
     clocks = ClockSampler(local).start()
     time.sleep(0.3)
     results = {}
     for mode in modes:
         on_lane = mode == "fp64" and use_lane
-        elapsed_ms, launch_ms, kernels = timed(runs[mode], lane_timing=on_lane)
-        # check the timed results: relative residual of every 13th column, the oracle on a sample
-        xs = d_x.cpu().numpy()
-        resid = max(orc.relative_residual(p, i, v, xs[k], rhs[k]) for k in range(0, count, 13))
-        err = float(max(np.abs(xs[k] - c).max() / np.abs(c).max() for k, c in zip(sample, cpu)))
-        r = {"rhs_s": world * count * a.steps / (elapsed_ms / 1e3), "ms_per_step": elapsed_ms / a.steps,
-             "launch_ms": launch_ms, "max_rel_residual": resid, "max_rel_err_vs_oracle": err}
-        if mode == "fp32_ir":
-            ratios, steps = d_ratio.cpu().numpy(), d_steps.cpu().numpy()
-            r.update({"device_max_ratio": float(ratios.max()), "mean_corrections": float(steps.mean()),
-                      "max_corrections": int(steps.max()), "tolerance": IR_TOLERANCE, "max_steps": IR_MAX_STEPS})
-            r["algorithmic_bytes_per_launch"] = algorithmic_bytes(n, count, info, "fp32_ir", float(steps.mean()), len(i))
-        else:
-            r["algorithmic_bytes_per_launch"] = algorithmic_bytes(n, count, info, "fp64")
+        elapsed_ms, launch_ms, kernels = timed(lambda: solve(mode), lane_timing=on_lane)
+        r = check(mode, {"rhs_s": total * a.steps / (elapsed_ms / 1e3), "ms_per_step": elapsed_ms / a.steps,
+                         "launch_ms": launch_ms})
+        steps_mean = r.get("mean_corrections", 0.0)
+        r["algorithmic_bytes_per_launch"] = algorithmic_bytes(n, count, info, mode, steps_mean, len(i))
         r.update(solver_of(mode))
-        # the dominant kernel's own launch time: the lane solve kernel (events around it in every
-        # launch), else the one launch of the step
+        # the dominant kernel's own launch time where the library records it (the lane solve), else
+        # the step's launches
         r["kernel_ms"] = launch_ms
         if kernels:
             r["kernels"] = kernels
@@ -454,7 +527,27 @@ def main():
             io_bytes = count * 16 * n  # each of the gather and the scatter reads and writes 8 n per RHS
             r["kernels"]["gather_gbs"] = io_bytes / (kernels["gather_ms"] / 1e3) / 1e9
             r["kernels"]["scatter_gbs"] = io_bytes / (kernels["scatter_ms"] / 1e3) / 1e9
+        # the mode's roofline over its whole step (every launch of it): SURVEY's byte model over the
+        # step's time, against the measured copy bandwidth
+        step_gbs = r["algorithmic_bytes_per_launch"] / (launch_ms / 1e3) / 1e9
+        r["step_roofline"] = {"achieved": step_gbs, "peak": peak, "unit": "GB/s", "frac": step_gbs / peak}
         results[mode] = r
+    if "fp64" in results and "fp32_ir" in results:
+        results["fp32_ir_over_fp64"] = results["fp32_ir"]["rhs_s"] / results["fp64"]["rhs_s"]
+
+    # the same block in blocks of 64, 256 and 1,024 columns (configuration 2's block widths)
+    by_width = {}
+    if not a.no_extras:
+        for width in WIDTHS:
+            by_width[str(width)] = {}
+            for mode in modes:
+                steps_w = max(3, min(a.steps, 10))
+                elapsed_ms, launch_ms, _ = timed(lambda: blocks(mode, width), steps=steps_w)
+                r = check(mode, {"rhs_s": total * steps_w / (elapsed_ms / 1e3), "ms_per_step": elapsed_ms / steps_w,
+                                 "launches_per_step": -(-count // width)})
+                r["solver"] = solver_of(mode)["solver"] if width >= (lane_min if mode == "fp64" else refine_min) \
+                    else "domain"
+                by_width[str(width)][mode] = r
     clock_info = clocks.stop()
 
     # the headline: the fastest mode whose every checked column meets the 1e-10 relative residual
@@ -463,24 +556,23 @@ def main():
     best = results[mode]
     achieved = best["algorithmic_bytes_per_launch"] / (best["kernel_ms"] / 1e3) / 1e9
     compulsory = count * 16 * n / (best["launch_ms"] / 1e3) / 1e9
-    if "fp64" in results and "fp32_ir" in results:
-        results["fp32_ir_over_fp64"] = results["fp32_ir"]["rhs_s"] / results["fp64"]["rhs_s"]
+    launches = a.steps * sum(results[m]["launches_per_step"] for m in modes)
+    launches += sum(max(3, min(a.steps, 10)) * r["launches_per_step"] for w in by_width.values() for r in w.values())
 
     line = {"metric": METRIC, "value": best["rhs_s"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": best["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": best["ms_per_step"], "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64" if mode == "fp64" else "f32 substitution, f64 refinement",
-            "data": "synthetic",
-            "config": {"workload": WORKLOAD, "rhs_per_step": count, "n": n, "mode": mode,
-                       "nnz_factor_per_sweep": info["fwd_entries"] + n, "levels": [info["fwd_levels"], info["bwd_levels"]],
-                       "solver": best["solver"], "flush": "inputs (1.08 GB) > L2", "parallelism": f"replicas x{world}"},
+            "data": "synthetic", "config": headline_config(total, n, world),
+            "mode": mode, "solver": best["solver"], "nnz_factor_per_sweep": info["fwd_entries"] + n,
+            "levels": [info["fwd_levels"], info["bwd_levels"]],
             "accuracy": {"max_rel_residual": best["max_rel_residual"], "max_rel_err_vs_oracle": best["max_rel_err_vs_oracle"]},
-            "modes": results,
+            "modes": results, "modes_by_width": by_width,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic_of(best, count, n), "peak_source": peak_kind, "kernel": best["kernel"],
                          "algorithmic_bytes_per_launch": best["algorithmic_bytes_per_launch"],
                          "kernel_ms": best["kernel_ms"], "launch_ms": best["launch_ms"], "compulsory_gbs": compulsory,
                          "compulsory_frac": compulsory / peak},
-            "clocks": clock_info, "gpu_launches": a.steps * sum(results[m]["launches_per_step"] for m in modes)}
+            "clocks": clock_info, "gpu_launches": launches}
 
     if not a.no_e2e:
         # every rank through the host-array call on its own GPU; the step time is the max over ranks
@@ -492,31 +584,34 @@ def main():
             factor.solve_many_into(bn, xn)
         reps = max(3, min(a.steps, 10))
         factor.reset_timings()
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
         t0 = time.perf_counter()
         for _ in range(reps):
             factor.solve_many_into(bn, xn)
         dt = replicas.max_over_ranks(time.perf_counter() - t0)
         t = factor.timings()
         e2e_err = float(max(np.abs(xn[k] - c).max() / np.abs(c).max() for k, c in zip(sample, cpu)))
-        line["e2e"] = {"value": world * count * reps / dt, "unit": UNIT, "h2d_bytes_per_step": int(rhs.nbytes),
+        line["e2e"] = {"value": total * reps / dt, "unit": UNIT, "h2d_bytes_per_step": int(rhs.nbytes),
                        "d2h_bytes_per_step": int(rhs.nbytes), "ms_per_step": dt / reps * 1e3,
                        "api": "yb_solve_many (pinned host arrays, chunks overlapped over both copy engines)",
                        "max_rel_err_vs_oracle": e2e_err, "chunks_per_step": t.blocks // reps,
                        "stage_ms_per_step": {"upload": t.upload / reps * 1e3, "solve": t.solve / reps * 1e3,
                                              "download": t.download / reps * 1e3}}
-    if world == 1 and not a.no_e2e:
+    if world == 1 and not a.no_extras:
         # for comparison: ybus_cuda's own route to the solve (cuSPARSE SpSM, lower then upper, in
-        # blocks), on the same factor and device arrays; its best block width of 64, 256 and 1024
+        # blocks; libybcompare.so), on the same factor and device arrays; its best block width
+        from ybus_b200 import compare
         spsm = {}
-        for width in (64, 256, 1024):
-            factor.reference_spsm_solve_device(d_b.data_ptr(), d_x.data_ptr(), count, width)
-            spsm[width] = factor.reference_spsm_solve_device(d_b.data_ptr(), d_x.data_ptr(), count, width)
+        for width in WIDTHS:
+            compare.spsm_solve(chol, d_b.data_ptr(), d_x.data_ptr(), count, width)
+            spsm[width] = compare.spsm_solve(chol, d_b.data_ptr(), d_x.data_ptr(), count, width)
         width = min(spsm, key=spsm.get)
         line["reference_gpu_spsm"] = {"value": count / (spsm[width] / 1e3), "unit": UNIT, "ms_per_step": spsm[width],
                                       "width": width, "ms_by_width": spsm,
                                       "route": "cuSPARSE SpSM lower + upper on CSR triangles (ybus_cuda's Block::solve)"}
+    if not a.no_extras:
+        steps_w, warm_w = max(3, min(a.steps, 5)), max(1, min(a.warmup, 2))
+        line["workloads"] = {name: fn(gpu, steps_w, warm_w, rank, world, local) for name, fn in WORKLOADS.items()}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(chol, rhs)
     if rank == 0:

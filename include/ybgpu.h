@@ -14,6 +14,10 @@
  * at element k*n. Indices are int64 at the boundary and must fit 32 bits on the device
  * (YB_ERROR_TOO_LARGE otherwise, as ybus_cuda's `CudaError::TooLarge`, ybus_cuda/src/lib.rs:98).
  * A row index of -1 means "none" wherever ybus_cuda takes an `Option<usize>`.
+ *
+ * The status codes, the last-error message and the host factor producer are declared in
+ * ybhost.h and live in libybhost.so, which libybgpu.so loads (a caller that only factors on the
+ * host needs that library alone).
  */
 #ifndef YBGPU_H
 #define YBGPU_H
@@ -21,71 +25,11 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "ybhost.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
-
-/* ---- status codes (ybus_cuda's `CudaError` variants, ybus_cuda/src/lib.rs:89-124) ---------- */
-#define YB_OK 0
-#define YB_ERROR_INVALID_ARGUMENT 1 /* a contract violation (ybus_cuda panics) */
-#define YB_ERROR_SHAPE_MISMATCH 2   /* CudaError::ShapeMismatch */
-#define YB_ERROR_TOO_LARGE 3        /* CudaError::TooLarge */
-#define YB_ERROR_NOT_POSITIVE_DEFINITE 4
-#define YB_ERROR_SINGULAR 5
-#define YB_NO_DEVICE 6              /* Gpu::new() -> Ok(None) */
-#define YB_ERROR_CUDA 7             /* CudaError::Driver */
-#define YB_ERROR_NOT_SYMMETRIC 8
-#define YB_ERROR_DEVICE_TIMEOUT 9   /* a bounded device wait gave up */
-#define YB_ERROR_INTERNAL 10
-
-#define YB_CHOLESKY 1
-#define YB_LU 2
-
-#define YB_ORDER_NATURAL 0
-#define YB_ORDER_AMD 1
-#define YB_ORDER_COLAMD 3
-
-/* The message of the calling thread's last failure, NUL-terminated and truncated to `length`;
- * returns the length needed including the NUL. */
-int32_t yb_last_error_message(char *buffer, size_t length);
-
-/* ---- host factor producer (the ybus_sparse calls whose results ybus_cuda uploads) --------- */
-typedef struct yb_matrix yb_matrix;
-typedef struct yb_host_factor yb_host_factor;
-
-/* A compressed matrix from triplets, duplicates summed in input order
- * (ybus_sparse/src/compressed_matrix.rs:254-330). `by_rows` = 1 for CSR, 0 for CSC. Complex
- * values are interleaved (re, im), 2*count doubles. */
-int32_t yb_matrix_from_triplets(int64_t rows, int64_t cols, int64_t count, const int64_t *row_idx,
-                                const int64_t *col_idx, const double *values, int32_t by_rows,
-                                int32_t is_complex, yb_matrix **out);
-/* Rows and columns in the given orders (ybus_sparse/src/compressed_matrix/access.rs:175-216). */
-int32_t yb_matrix_select(const yb_matrix *m, int64_t n_rows, const int64_t *rows, int64_t n_cols,
-                         const int64_t *cols, yb_matrix **out);
-/* The other orientation of the same matrix (to_csc / to_csr). */
-int32_t yb_matrix_reorient(const yb_matrix *m, yb_matrix **out);
-int32_t yb_matrix_info(const yb_matrix *m, int64_t *rows, int64_t *cols, int64_t *stored,
-                       int32_t *by_rows, int32_t *is_complex);
-int32_t yb_matrix_export(const yb_matrix *m, int64_t *ptr, int64_t *idx, double *values);
-void yb_matrix_free(yb_matrix *m);
-/* A fill-reducing ordering (ybus_sparse/src/compressed_matrix/ordering.rs:46-64). */
-int32_t yb_ordering(const yb_matrix *m, int32_t ordering, int64_t *perm);
-
-/* `CsrMatrix::analyze_cholesky(ordering)` then `factor` (cholesky.rs:50-311): P A Pᵀ = L Lᵀ. */
-int32_t yb_host_cholesky(const yb_matrix *csr, int32_t ordering, yb_host_factor **out);
-/* `CscMatrix::analyze_lu(ordering)` then `factor` with the pivot threshold (lu.rs:142-247). */
-int32_t yb_host_lu(const yb_matrix *csc, int32_t ordering, double pivot_threshold, yb_host_factor **out);
-int32_t yb_host_factor_info(const yb_host_factor *f, int32_t *kind, int32_t *is_complex, int64_t *n,
-                            int64_t *lower_stored, int64_t *upper_stored);
-/* Cholesky: lower = L (CSR, diagonal last), upper = Lᵀ (CSR, diagonal first), both perms = P.
- * LU: lower = L (CSC, unit diagonal first), upper = U (CSC, diagonal last), row_perm = P,
- * col_perm = Q. Any output may be NULL. */
-int32_t yb_host_factor_export(const yb_host_factor *f, int64_t *lower_ptr, int64_t *lower_idx,
-                              double *lower_val, int64_t *upper_ptr, int64_t *upper_idx,
-                              double *upper_val, int64_t *row_perm, int64_t *col_perm);
-int32_t yb_host_etree(const yb_host_factor *f, int64_t *parent);
-void yb_host_factor_free(yb_host_factor *f);
-
 
 /* ---- the GPU (ybus_cuda `Gpu`, ybus_cuda/src/lib.rs:168-219) ----------------------------- */
 typedef struct yb_gpu yb_gpu;
@@ -169,6 +113,15 @@ int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32
 /* No ybus counterpart: the number of right-hand sides from which the automatic choice takes the
  * lane solve (default 3072). */
 int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t min_count);
+/* No ybus counterpart: the number of right-hand sides from which yb_solve_many_refined_device takes
+ * the FP32 lane solve (default 5120, the measured crossover with the refinement fused into the
+ * domain solve on the 10,000-bus B'; the FP32 lane threshold of yb_factor_set_lane_min_count applies
+ * too, whichever is higher). */
+int32_t yb_factor_set_refine_lane_min_count(yb_factor *f, int64_t min_count);
+/* No ybus counterpart: the thresholds the automatic choice applies for a precision: the plain
+ * solve's lane threshold and the refined solve's (either output may be NULL). */
+int32_t yb_factor_lane_min_counts(const yb_factor *f, int32_t precision, int64_t *lane_min_count,
+                                  int64_t *refine_lane_min_count);
 /* No ybus counterpart: with on = 1, every lane-solve launch from now on records CUDA events around
  * its three kernels (gather, solve, scatter) on the caller's stream, for up to 4096 launches;
  * on = 0 stops. Either way the record so far is cleared. */
@@ -379,26 +332,21 @@ int32_t yb_factor_attach_matrix(yb_factor *f, const int64_t *a_ptr, const int64_
 /* No ybus counterpart on the GPU; the CPU's is `solve_refined_normwise` (accuracy.rs:83-122):
  * the substitutions in FP32, the residual and the update x += d in FP64 against the attached A, up
  * to max_steps corrections per tile, until every column's ||r||inf / ||b||inf <= tolerance or the
- * residual stops halving. From 5,120 right-hand sides on (or the FP32 lane threshold of
- * yb_factor_set_lane_min_count, if higher) the passes run on the lane solve, a tile being a group of
- * 32 columns, with b and x held in FP64 beside the
- * work array (r = b - A x each pass); below it, or when the factor admits no lane layout, on the
- * domain solve with the refinement fused into its launch (r kept as r -= A d, the residual of x to
- * rounding). Device arrays as yb_solve_many_device; d_ratio (double, count) and d_steps (int32,
- * count) receive each column's final relative residual and corrections (either may be NULL).
+ * residual stops halving. Each column keeps, as refine_normwise does, its best iterate: x, d_ratio
+ * and d_steps are those of the iterate with the smallest relative residual. From 5,120 right-hand
+ * sides on (yb_factor_set_refine_lane_min_count; or the FP32 lane threshold of
+ * yb_factor_set_lane_min_count, if higher) the passes run on the lane solve, the stop rule applied
+ * per column and the solve skipping groups of 32 columns that have all stopped, with each pass's
+ * FP32 correction kept beside the work array (two work arrays of FP32, plus an FP64 one when
+ * max_steps >= 2) and r = b - A x formed from them each pass; below it, or when the factor admits no
+ * lane layout, on the domain solve with the refinement fused into its launch (r kept as r -= A d,
+ * the residual of x to rounding). Device arrays as yb_solve_many_device; d_ratio (double, count) and
+ * d_steps (int32, count) receive each column's relative residual and corrections (either may be
+ * NULL).
  * YB_ERROR_INVALID_ARGUMENT when the factor admits neither solve. */
 int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
                                      int64_t count, int32_t max_steps, double tolerance, double *d_ratio,
                                      int32_t *d_steps, void *stream);
-
-/* For comparison only, not a solve path of this library: ybus_cuda's own route to the solve
- * (`Block::solve`, ybus_cuda/src/sparse.rs:371-420: cuSPARSE SpSM on the lower, then the upper
- * triangle as CSR, blocks of `width` right-hand sides, the last block padded with zeros), on a
- * Cholesky factor and device arrays as yb_solve_many_device takes them, the permutations applied on
- * the device. cuSPARSE is opened at the first call (YB_ERROR_INVALID_ARGUMENT without it). solve_ms
- * (may be NULL) receives the time of the solves, their analysis excluded. */
-int32_t yb_reference_spsm_solve(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
-                                int64_t count, int64_t width, double *solve_ms);
 
 /* No counterpart in ybus. The device-array solve for callers that must not have the library
  * allocate device memory: programs whose own pool allocator has reserved the GPU's memory (so a
@@ -408,8 +356,10 @@ int32_t yb_reference_spsm_solve(yb_factor *f, const double *d_rhs, int64_t ldb, 
  * holds until exit, and calls no cudaMalloc or cudaFree. Arguments as yb_solve_many_device; the
  * factor's upload (yb_factor_from_*) still allocates, once. The tile width is the one
  * yb_factor_set_tile gives the precision; YB_ERROR_TOO_LARGE if one block's working vectors
- * (order x tile width x value size) exceed the array. The first call on a device looks up the
- * array's address and should come before any stream capture. Every call shares the array and
+ * (order x tile width x value size) exceed the array. yb_gpu_new places the array on its device
+ * and looks up its address (so the module that holds it is loaded then, not at this entry point's
+ * first call under lazy module loading), and yb_gpu_new fails if that fails; this entry point
+ * itself then loads and allocates nothing. Every call shares the array and
  * leaves its contents behind (no part needs to start at zero); calls that overlap on the GPU race
  * on it and must be serialised by the caller. */
 int32_t yb_solve_many_device_noalloc(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,

@@ -145,6 +145,45 @@ def relative_residual(ptr, idx, val, x, b) -> float:
     return lib().or_relative_residual(ptr.size - 1, _p(ptr), _p(idx), _p(val), _p(x), _p(b))
 
 
+def refine_normwise(ptr, idx, val, b, max_steps, tolerance, solve):
+    """`refine_normwise` (ybus_sparse/src/compressed_matrix/accuracy.rs:93-118): x = solve(b), then
+    while the relative residual ||b - A x||inf / ||b||inf (accuracy.rs:58-79) is above the tolerance,
+    at most max_steps corrections x += solve(b - A x), keeping the iterate with the smallest ratio,
+    stopping on a NaN ratio or one above half the ratio before. A is CSR (ptr, idx, val). Returns
+    (best x, its correction count, its ratio, every ratio in order, the smallest relative margin of
+    the comparisons the decisions took)."""
+    b = _c(b, np.float64)
+
+    def residual(x):
+        r = b - csr_mul_vec(ptr, idx, val, x)
+        rn, bn = np.abs(r).max(initial=0.0), np.abs(b).max(initial=0.0)
+        ratio = rn / bn if bn > 0 else (np.inf if rn > 0 else 0.0)
+        return ratio, r
+
+    def margin(lhs, rhs):
+        return abs(lhs - rhs) / max(abs(rhs), 1e-300) if np.isfinite(lhs) and np.isfinite(rhs) else np.inf
+
+    x = solve(b)
+    ratio, r = residual(x)
+    best = (x.copy(), 0, ratio)
+    ratios, margins = [ratio], []
+    for step in range(1, max_steps + 1):
+        margins.append(margin(ratio, tolerance))
+        if ratio <= tolerance:
+            break
+        x = x + solve(r)
+        previous = ratio
+        ratio, r = residual(x)
+        ratios.append(ratio)
+        margins.append(margin(ratio, best[2]))
+        if ratio < best[2]:
+            best = (x.copy(), step, ratio)
+        margins.append(margin(ratio, 0.5 * previous))
+        if np.isnan(ratio) or ratio > 0.5 * previous:
+            break
+    return best[0], best[1], best[2], ratios, min(margins, default=np.inf)
+
+
 # ---- factor checks (independent of how the factor was made) -------------------------------
 
 def dense_from_csr(n_rows, n_cols, ptr, idx, val, by_rows=True):

@@ -288,16 +288,17 @@ def test_full_ptdf_block_on_the_10k_grid(gpu):
 
 
 def test_the_cusparse_comparison_solves_the_same(gpu):
-    # ybus_cuda's own route (cuSPARSE SpSM), kept for the bench's side-by-side timing: the same
-    # solutions as the oracle, every block width, a last block padded
+    # ybus_cuda's own route (cuSPARSE SpSM, libybcompare.so), kept for the bench's side-by-side
+    # timing: the same solutions as the oracle, every block width, a last block padded
     import torch
+
+    from ybus_b200 import compare
     chol = host.cholesky(random_spd(300, 3, 7))
     rhs = right_hand_sides(300, 70, 11)
     cpu = orc.solve_many(chol, rhs)
-    factor = upload(gpu, chol)
     b = torch.from_numpy(rhs).cuda()
     for width in (1, 16, 64, 256):
         x = torch.zeros_like(b)
-        ms = factor.reference_spsm_solve_device(b.data_ptr(), x.data_ptr(), 70, width)
+        ms = compare.spsm_solve(chol, b.data_ptr(), x.data_ptr(), 70, width)
         assert ms > 0
         assert worst_relative_difference(x.cpu().numpy(), cpu) < BAR, f"width {width}"

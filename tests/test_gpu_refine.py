@@ -126,3 +126,45 @@ def test_lane_refinement_of_an_lu_factor_or_its_refusal(gpu):
     xs = x.cpu().numpy()
     assert max(orc.relative_residual(p, i, v, xs[k], rhs[k]) for k in range(40)) <= TOL
     assert ratio.cpu().numpy().max() <= TOL
+
+
+@pytest.mark.parametrize("lane", [False, True], ids=["domain", "lane"])
+def test_each_column_returns_its_best_iterate(gpu, lane):
+    # A nearby matrix attached in place of the factored one (A' = 1.1 A + 8e-6 diag(A)), as
+    # refine_normwise allows (a solve with a nearby matrix's factors): some columns improve and
+    # stop, some stop on a pass that made them worse and must return the iterate before it. Against
+    # the CPU's refine_normwise with the FP64 solve, column by column: the corrections of the best
+    # iterate, its ratio and its x, to what the FP32 substitutions change; only columns whose every
+    # decision holds with a relative margin above 1e-3 (the FP32 solves move a ratio by ~1e-5).
+    import torch
+    a = bprime(2000, 700, grids.SEED_BASE + 1)
+    p, i, v = a.to_csr().arrays()
+    rows = np.repeat(np.arange(p.size - 1), np.diff(p))
+    near = v * 1.1
+    near[rows == i] += 8e-6 * v[rows == i]
+    rhs = np.random.default_rng(4).standard_normal((64, 1999))
+    chol = host.cholesky(a)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.attach_matrix((p, i, near))
+    if lane:
+        factor.set_tile_kind(FP32, LANE)
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    ratio = torch.empty(64, dtype=torch.float64, device="cuda")
+    steps = torch.empty(64, dtype=torch.int32, device="cuda")
+    factor.solve_many_refined_device(b.data_ptr(), x.data_ptr(), 64, 4, TOL, ratio.data_ptr(), steps.data_ptr())
+    gpu.synchronize()
+    factor.check_error()
+    xs, ratio, steps = x.cpu().numpy(), ratio.cpu().numpy(), steps.cpu().numpy()
+    solve = lambda r: orc.solve_many(chol, r[None, :])[0]
+    checked, worse = 0, 0
+    for k in range(64):
+        bx, bs, br, ratios, margin = orc.refine_normwise(p, i, near, rhs[k], 4, TOL, solve)
+        if margin < 1e-3:
+            continue
+        checked += 1
+        worse += bs < len(ratios) - 1  # its last pass made it no better
+        assert steps[k] == bs, (k, steps[k], bs, ratios)
+        assert abs(ratio[k] - br) <= 1e-3 * br, (k, ratio[k], br)
+        assert np.abs(xs[k] - bx).max() <= 1e-4 * np.abs(bx).max(), k
+    assert checked >= 40 and worse >= 5, (checked, worse)

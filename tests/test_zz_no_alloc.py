@@ -44,13 +44,19 @@ def test_noalloc_solve_matches_the_device_entry_point_twice(gpu, case):
     gpu.synchronize()
     expected = ref.cpu().numpy()
     assert worst_relative_difference(expected, orc.solve_many(chol, rhs, threads=8)) < BAR
-    for call in range(2):
-        x = torch.full_like(b, float("nan"))
-        torch.cuda.synchronize()
+    xs = [torch.full_like(b, float("nan")) for _ in range(2)]
+    torch.cuda.synchronize()
+    free = []
+    for call, x in enumerate(xs):
+        free.append(torch.cuda.mem_get_info()[0])
         assert _noalloc(factor, b, x, rhs.shape[0], FP64) == _lib.YB_OK, _lib.last_error()
         gpu.synchronize()
         d = worst_relative_difference(x.cpu().numpy(), expected)
         assert d < BAR, f"call {call}: {d:e}"
+    # the entry point's whole contract: the device's free memory is what it was before either call
+    # (the fixed array and the kernels were placed when the GPU was opened)
+    free.append(torch.cuda.mem_get_info()[0])
+    assert free[0] == free[1] == free[2], free
 
 
 def test_noalloc_solve_in_fp32_and_narrow_tiles(gpu):

@@ -1,7 +1,9 @@
-"""ctypes binding of libybgpu.so (the C ABI declared in include/ybgpu.h).
+"""ctypes bindings of libybhost.so (the host factor producer, include/ybhost.h) and libybgpu.so
+(the GPU path, include/ybgpu.h).
 
-The library is loaded from this package's directory. There is no fallback: if it is missing or
-fails to load, every call raises, so nothing silently runs on the CPU instead.
+Both are loaded from this package's directory; libybgpu.so is loaded only at the first call that
+needs it, so host-only work never maps it. There is no fallback: if a library is missing or fails
+to load, every call raises, so nothing silently runs on the CPU instead.
 """
 from __future__ import annotations
 
@@ -11,6 +13,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libybgpu.so"
+HOST_LIB_PATH = HERE / "libybhost.so"
 
 i32, i64, u64, dbl, vp = C.c_int32, C.c_int64, C.c_uint64, C.c_double, C.c_void_p
 P_i64 = C.POINTER(C.c_int64)
@@ -36,8 +39,8 @@ YB_ORDER_COLAMD = 3
 YB_FP64 = 0
 YB_FP32 = 1
 
-# name -> (restype, argtypes)
-SIGNATURES: dict[str, tuple] = {
+# name -> (restype, argtypes), libybhost.so
+HOST_SIGNATURES: dict[str, tuple] = {
     "yb_last_error_message": (i32, [C.c_char_p, C.c_size_t]),
     "yb_matrix_from_triplets": (i32, [i64, i64, i64, vp, vp, vp, i32, i32, C.POINTER(vp)]),
     "yb_matrix_select": (i32, [vp, i64, vp, i64, vp, C.POINTER(vp)]),
@@ -52,6 +55,10 @@ SIGNATURES: dict[str, tuple] = {
     "yb_host_factor_export": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "yb_host_etree": (i32, [vp, vp]),
     "yb_host_factor_free": (None, [vp]),
+}
+
+# name -> (restype, argtypes), libybgpu.so
+SIGNATURES: dict[str, tuple] = {
     "yb_gpu_new": (i32, [i32, C.POINTER(vp)]),
     "yb_gpu_free": (None, [vp]),
     "yb_gpu_name": (i32, [vp, C.c_char_p, C.c_size_t]),
@@ -79,9 +86,10 @@ SIGNATURES: dict[str, tuple] = {
     "yb_factor_set_tail_level": (i32, [vp, i32, i32]),
     "yb_factor_set_domain": (i32, [vp, i32, i32, i32, i32, i32]),
     "yb_factor_autotune": (i32, [vp, i32, i64, vp, P_dbl]),
-    "yb_reference_spsm_solve": (i32, [vp, vp, i64, vp, i64, i64, i64, P_dbl]),
     "yb_factor_lane_info": (i32, [vp, i32, vp]),
     "yb_factor_set_lane_min_count": (i32, [vp, i32, i64]),
+    "yb_factor_set_refine_lane_min_count": (i32, [vp, i64]),
+    "yb_factor_lane_min_counts": (i32, [vp, i32, P_i64, P_i64]),
     "yb_factor_time_lane": (i32, [vp, i32]),
     "yb_factor_lane_times": (i32, [vp, P_dbl, P_dbl, P_dbl, P_i64]),
     "yb_factor_set_lane": (i32, [vp, i32, i32, i32]),
@@ -125,6 +133,7 @@ SIGNATURES: dict[str, tuple] = {
 }
 
 _lib: C.CDLL | None = None
+_host_lib: C.CDLL | None = None
 
 
 class YbError(RuntimeError):
@@ -136,23 +145,37 @@ class YbError(RuntimeError):
         self.message = message
 
 
+def _open(path: Path, signatures: dict) -> C.CDLL:
+    if not path.exists():
+        raise RuntimeError(f"{path} is not built: run `python -c 'import __graft_entry__ as g; g.build()'`")
+    handle = C.CDLL(str(path), mode=os.RTLD_LOCAL)
+    for name, (res, args) in signatures.items():
+        fn = getattr(handle, name)
+        fn.restype = res
+        fn.argtypes = args
+    return handle
+
+
+def host_lib() -> C.CDLL:
+    """libybhost.so: the host factor producer and the last-error store."""
+    global _host_lib
+    if _host_lib is None:
+        _host_lib = _open(HOST_LIB_PATH, HOST_SIGNATURES)
+    return _host_lib
+
+
 def lib() -> C.CDLL:
+    """libybgpu.so: the GPU path (it loads libybhost.so beside it)."""
     global _lib
     if _lib is None:
-        if LIB_PATH is None or not LIB_PATH.exists():
-            raise RuntimeError(f"{LIB_PATH} is not built: run `python -c 'import __graft_entry__ as g; g.build()'`")
-        handle = C.CDLL(str(LIB_PATH), mode=os.RTLD_LOCAL)
-        for name, (res, args) in SIGNATURES.items():
-            fn = getattr(handle, name)
-            fn.restype = res
-            fn.argtypes = args
-        _lib = handle
+        host_lib()
+        _lib = _open(LIB_PATH, SIGNATURES)
     return _lib
 
 
 def last_error() -> str:
     buf = C.create_string_buffer(1024)
-    lib().yb_last_error_message(buf, len(buf))
+    host_lib().yb_last_error_message(buf, len(buf))
     return buf.value.decode(errors="replace")
 
 

@@ -1,8 +1,14 @@
-"""Builds libybgpu.so in-tree with nvcc for sm_100a (B200).
+"""Builds the package's native libraries in-tree with g++ and nvcc (sm_100a, B200):
 
-The library holds the host factor producer (C++), the plan builder (C++) and the CUDA kernels
-with their C ABI. It is built in place (``ybus_b200/libybgpu.so``) so it travels with the
-source tree; nothing is cached outside the repository.
+- ``libybhost.so``: the host factor producer and the last-error store (C++, no CUDA), the only
+  library a host-only caller (the CPU reference arm, the host tests) loads;
+- ``libybgpu.so``: the plan and layout builders (C++), the CUDA kernels and the C ABI of the GPU
+  path; it depends on ``libybhost.so`` (found beside it through its run path);
+- ``libybcompare.so``: for comparison only, ybus_cuda's cuSPARSE route re-created on the same
+  arrays; no solve of ``libybgpu.so`` loads it.
+
+They are built in place (``ybus_b200/*.so``) so they travel with the source tree; nothing is
+cached outside the repository.
 """
 from __future__ import annotations
 
@@ -14,24 +20,43 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
+INCLUDE = HERE.parent / "include"
+HOST_LIB = HERE / "libybhost.so"
 LIB = HERE / "libybgpu.so"
+COMPARE_LIB = HERE / "libybcompare.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+HOST_SOURCES = ["host/factor.cpp", "host/colamd.cpp", "capi_host.cpp"]
+
+
+def host_sources() -> list[Path]:
+    return [CSRC / s for s in HOST_SOURCES]
 
 
 def sources() -> list[Path]:
-    files = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp")) + sorted((CSRC / "host").glob("*.cpp"))
-    return files
+    """The sources of libybgpu.so."""
+    host = set(host_sources())
+    files = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+    return [f for f in files if f not in host]
 
 
-def _inputs() -> list[Path]:
-    return sources() + sorted(CSRC.rglob("*.hpp")) + sorted(CSRC.rglob("*.cuh")) + [HERE.parent / "include" / "ybgpu.h"]
+def compare_sources() -> list[Path]:
+    return sorted((CSRC / "compare").glob("*.cu"))
+
+
+def _headers() -> list[Path]:
+    return sorted(CSRC.rglob("*.hpp")) + sorted(CSRC.rglob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _fresh(lib: Path, inputs: list[Path]) -> bool:
+    if not lib.exists():
+        return False
+    built = lib.stat().st_mtime
+    return all(p.stat().st_mtime <= built for p in inputs)
 
 
 def up_to_date() -> bool:
-    if not LIB.exists():
-        return False
-    built = LIB.stat().st_mtime
-    return all(p.stat().st_mtime <= built for p in _inputs())
+    return (_fresh(HOST_LIB, host_sources() + _headers()) and _fresh(LIB, sources() + _headers() + [HOST_LIB])
+            and _fresh(COMPARE_LIB, compare_sources()))
 
 
 def nvcc() -> str:
@@ -45,21 +70,18 @@ def nvcc() -> str:
     return found
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and up_to_date():
-        return LIB
-    objdir = HERE / "_build"
-    objdir.mkdir(exist_ok=True)
-    common = ["-std=c++17", "-O3", "-Xcompiler", "-fPIC", "-I", str(CSRC), "-I", str(HERE.parent / "include")]
-    objs = []
-    procs = []
-    for src in sources():
-        obj = objdir / (src.stem + (".cu.o" if src.suffix == ".cu" else ".o"))
+def _compile(srcs: list[Path], objdir: Path, verbose: bool) -> list[Path]:
+    common = ["-std=c++17", "-O3", "-I", str(CSRC), "-I", str(INCLUDE)]
+    objs, procs = [], []
+    for src in srcs:
+        rel = src.relative_to(CSRC).with_suffix("")
+        obj = objdir / (str(rel).replace("/", "_") + (".cu.o" if src.suffix == ".cu" else ".o"))
         if src.suffix == ".cu":
-            cmd = [nvcc(), *ARCH, "-lineinfo", "--expt-relaxed-constexpr", *common, "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc(), *ARCH, "-lineinfo", "--expt-relaxed-constexpr", *common, "-Xcompiler", "-fPIC", "-c",
+                   str(src), "-o", str(obj)]
         else:
-            cmd = ["g++", "-std=c++17", "-O3", "-fPIC", "-Wall", "-I", str(CSRC), "-I", str(HERE.parent / "include"),
-                   "-I", str(Path(nvcc()).parent.parent / "include"), "-c", str(src), "-o", str(obj)]
+            cmd = ["g++", *common, "-fPIC", "-Wall", "-I", str(Path(nvcc()).parent.parent / "include"), "-c", str(src),
+                   "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         procs.append((subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT), src))
@@ -73,12 +95,29 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             print(out.decode(errors="replace"), file=sys.stderr)
     if failed:
         raise RuntimeError("build failed:\n" + "\n".join(failed))
-    tmp = LIB.with_suffix(".so.tmp")
-    link = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lpthread"]
-    res = subprocess.run(link, capture_output=True, text=True)
+    return objs
+
+
+def _link(cmd: list[str], target: Path) -> None:
+    tmp = target.with_suffix(".so.tmp")
+    res = subprocess.run([*cmd, "-o", str(tmp)], capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("link failed:\n" + res.stdout + res.stderr)
-    os.replace(tmp, LIB)
+        raise RuntimeError(f"link of {target.name} failed:\n" + res.stdout + res.stderr)
+    os.replace(tmp, target)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and up_to_date():
+        return LIB
+    objdir = HERE / "_build"
+    objdir.mkdir(exist_ok=True)
+    host_objs = _compile(host_sources(), objdir, verbose)
+    _link(["g++", "-shared", "-Wl,-soname,libybhost.so", *map(str, host_objs), "-lpthread"], HOST_LIB)
+    gpu_objs = _compile(sources(), objdir, verbose)
+    _link([nvcc(), *ARCH, "-shared", *map(str, gpu_objs), "-L", str(HERE), "-lybhost", "-Xlinker", "-rpath=$ORIGIN",
+           "-lpthread"], LIB)
+    cmp_objs = _compile(compare_sources(), objdir, verbose)
+    _link([nvcc(), *ARCH, "-shared", *map(str, cmp_objs), "-ldl"], COMPARE_LIB)
     return LIB
 
 

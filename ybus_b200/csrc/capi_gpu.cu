@@ -18,6 +18,10 @@
 
 using namespace yb;
 
+namespace yb {
+void noalloc_prepare(int device);  // noalloc.cu
+}
+
 // ---------------------------------------------------------------------------------------------
 // Gpu
 // ---------------------------------------------------------------------------------------------
@@ -48,6 +52,7 @@ extern "C" int32_t yb_gpu_new(int32_t device, yb_gpu **out) {
     g->smem_optin = prop.sharedMemPerBlockOptin;
     g->smem_per_sm = prop.sharedMemPerMultiprocessor;
     cuda_check(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    noalloc_prepare(device);  // the allocation-free solve's fixed array, placed now rather than at its first call
     *out = g.release();
     return YB_OK;
   });
@@ -703,6 +708,7 @@ template <class T> DeviceLane *lane_for(yb_factor *f, int warps, int page_bytes,
     d->warp_page.upload(lay.warp_page, stream);
     d->in_pos.upload(lay.in_pos, stream);
     d->out_pos.upload(lay.out_pos, stream);
+    d->host_out_pos = lay.out_pos;
     cuda_check(cudaStreamSynchronize(stream), "lane layout upload");
   } catch (const host::Error &e) {
     if (e.status != host::kInvalidArgument && e.status != host::kTooLarge) throw;
@@ -1193,6 +1199,27 @@ extern "C" int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision,
   });
 }
 
+extern "C" int32_t yb_factor_set_refine_lane_min_count(yb_factor *f, int64_t min_count) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(min_count >= 0, "negative count");
+    f->tile32.refine_lane_min_count = min_count;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_lane_min_counts(const yb_factor *f, int32_t precision, int64_t *lane_min_count,
+                                             int64_t *refine_lane_min_count) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    const TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
+    if (lane_min_count) *lane_min_count = t.lane_min_count;
+    if (refine_lane_min_count) *refine_lane_min_count = f->tile32.refine_lane_min_count;
+    return YB_OK;
+  });
+}
+
 extern "C" int32_t yb_factor_attach_matrix(yb_factor *f, const int64_t *a_ptr, const int64_t *a_idx,
                                            const double *a_val) {
   return guard([&] {
@@ -1239,36 +1266,93 @@ extern "C" int32_t yb_factor_attach_matrix(yb_factor *f, const int64_t *a_ptr, c
     f->a_csr_idx.upload(csr_idx, s);
     f->a_csr_val.upload(csr_val, s);
     cuda_check(cudaStreamSynchronize(s), "matrix upload");
+    f->a_host_ptr.assign(a_ptr, a_ptr + n + 1);
+    f->a_host_idx.assign(a_idx, a_idx + nnz);
+    f->a_host_val.assign(a_val, a_val + nnz);
+    f->a_attached += 1;
     f->a_rows = n;
     return YB_OK;
   });
 }
 
 namespace yb {
-// The refined solve through the lane solve: per launch's groups, pass 0 solves b, each later pass
-// the residual; after each solve the update x += d and the residual in FP64, then each group's
-// decision; the kernels of a pass skip the groups that have stopped (lane_refine.cuh).
+// The refined solve's copy of A for a lane layout (LaneRefineArgs' res_*): rows in natural order,
+// 32 to a slice, entry q of row 32 s + l at ptr[s] + 32 q + l, each column as the work row that
+// holds its unknown (out_pos).
+void lane_residual_matrix(yb_factor *f, DeviceLane *d, cudaStream_t stream) {
+  if (d->res_matrix == f->a_attached) return;
+  const int64_t n = f->n, slices = (n + 31) / 32;
+  std::vector<int32_t> ptr(slices + 1, 0), len(n), col;
+  std::vector<double> val;
+  for (int64_t s = 0; s < slices; ++s) {
+    int64_t width = 0;
+    for (int64_t r = 32 * s; r < std::min<int64_t>(n, 32 * s + 32); ++r)
+      width = std::max<int64_t>(width, f->a_host_ptr[r + 1] - f->a_host_ptr[r]);
+    const size_t o = col.size();
+    require(o + 32 * (size_t)width < (size_t)INT32_MAX, "the matrix is too large for 32-bit offsets", host::kTooLarge);
+    col.resize(o + 32 * width, 0);
+    val.resize(o + 32 * width, 0.0);
+    for (int64_t r = 32 * s; r < std::min<int64_t>(n, 32 * s + 32); ++r) {
+      len[r] = (int32_t)(f->a_host_ptr[r + 1] - f->a_host_ptr[r]);
+      for (int64_t k = f->a_host_ptr[r]; k < f->a_host_ptr[r + 1]; ++k) {
+        const size_t at = o + 32 * (size_t)(k - f->a_host_ptr[r]) + (size_t)(r - 32 * s);
+        col[at] = d->host_out_pos[f->a_host_idx[k]];
+        val[at] = f->a_host_val[k];
+      }
+    }
+    ptr[s + 1] = (int32_t)col.size();
+  }
+  d->res_ptr.upload(ptr, stream);
+  d->res_len.upload(len.empty() ? std::vector<int32_t>{0} : len, stream);
+  d->res_col.upload(col.empty() ? std::vector<int32_t>{0} : col, stream);
+  d->res_val.upload(val.empty() ? std::vector<double>{0.0} : val, stream);
+  cuda_check(cudaStreamSynchronize(stream), "residual matrix upload");
+  d->res_matrix = f->a_attached;
+}
+
+// The refined solve through the lane solve (lane_refine.cuh), per launch's run of groups: b
+// gathered once into the FP32 work array; per pass the FP32 lane solve (its correction into its
+// own array), the FP64 residual of the iterate it completes (which also writes that iterate into
+// the caller's x for the columns still refining), each column's decision, the restore of the best
+// iterate where a pass made it no better, and, while another pass may follow, the iterate carried
+// in FP64. Every kernel of a pass skips the groups that have stopped.
 void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
                          int32_t max_steps, double tolerance, double *ratio_out, int32_t *steps_out, cudaStream_t stream) {
   using T = float;
   const int64_t n = f->n;
-  const size_t group_bytes = (size_t)n * 32 * sizeof(T);
+  const size_t group_vals = (size_t)n * 32;
   const int64_t groups_all = (count + 31) / 32;
-  // per launch as many groups as the plain solve takes (the FP32 work array's bound); b and x in
-  // FP64 in the lane layout take four times the work array's bytes beside it
-  const int64_t per_launch = std::max<int64_t>(1, std::min<int64_t>(groups_all, (int64_t)(kLaneWorkBytes / group_bytes)));
+  const int64_t per_launch = std::max<int64_t>(1, std::min<int64_t>(groups_all, (int64_t)(kLaneWorkBytes / (group_vals * sizeof(T)))));
   const int64_t cols_most = per_launch * 32;
-  f->lane_work.reserve((size_t)per_launch * group_bytes);
+  lane_residual_matrix(f, d, stream);
+  f->lane_work.reserve((size_t)per_launch * group_vals * sizeof(T));
   f->lane_partial.reserve((size_t)per_launch * std::max(d->partials, 1) * 32 * sizeof(T));
-  f->refine_scratch.reserve((size_t)(2 * cols_most * n));
-  f->refine_state.reserve((size_t)cols_most * 3 * sizeof(double) + (size_t)per_launch);
+  f->refine_parts.reserve(2 * (size_t)per_launch * group_vals);
+  if (max_steps >= 2) f->refine_scratch.reserve((size_t)per_launch * group_vals);
+  // per column: rmax, bmax, cur, best (8 bytes each), best_steps (4); per group: col_active,
+  // write_mask, restore_mask (4 each), active (1)
+  const size_t state_bytes = (size_t)cols_most * 36 + (size_t)per_launch * 13 + 64;
+  f->refine_state.reserve(state_bytes);
   T *work = reinterpret_cast<T *>(f->lane_work.get());
   T *partial = reinterpret_cast<T *>(f->lane_partial.get());
-  double *bl = f->refine_scratch.get(), *xl = bl + cols_most * n;
-  auto *rmax = reinterpret_cast<unsigned long long *>(f->refine_state.get());
-  unsigned long long *bmax = rmax + cols_most;
-  double *prev = reinterpret_cast<double *>(bmax + cols_most);
-  uint8_t *active = reinterpret_cast<uint8_t *>(prev + cols_most);
+  T *dA = f->refine_parts.get(), *dB = dA + (size_t)per_launch * group_vals;
+  double *X = f->refine_scratch.get();
+  uint8_t *st = f->refine_state.get();
+  LaneRefineArgs r{};
+  r.n = (int32_t)n;
+  r.rmax = reinterpret_cast<unsigned long long *>(st);
+  r.bmax = r.rmax + cols_most;
+  r.cur = reinterpret_cast<double *>(r.bmax + cols_most);
+  r.best = r.cur + cols_most;
+  r.best_steps = reinterpret_cast<int32_t *>(r.best + cols_most);
+  r.col_active = reinterpret_cast<uint32_t *>(r.best_steps + cols_most);
+  r.write_mask = r.col_active + per_launch;
+  r.restore_mask = r.write_mask + per_launch;
+  r.active = reinterpret_cast<uint8_t *>(r.restore_mask + per_launch);
+  r.in_pos = d->in_pos.get(), r.out_pos = d->out_pos.get();
+  r.res_ptr = d->res_ptr.get(), r.res_len = d->res_len.get(), r.res_col = d->res_col.get(), r.res_val = d->res_val.get();
+  r.work = work;
+  r.ldb = ldb, r.ldx = ldx;
   const size_t smem = lane_smem<T>(d);
   if (smem > (size_t)f->gpu->smem_optin) throw host::Error(host::kInvalidArgument, "the lane solve's block does not fit in shared memory");
   cuda_check(cudaFuncSetAttribute(lane_solve_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -1279,40 +1363,54 @@ void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t l
   a.blob = d->blob.get();
   a.warp_page = d->warp_page.get();
   a.error = f->error.get();
-  a.group_active = active;
-  // b's row i sits in work row in_pos[i] = i (the work array follows b's own order), so in_pos also
-  // maps the lane layout's natural rows
-  const int32_t *natural = d->in_pos.get();
+  a.group_active = r.active;
+  auto check = [](const char *what) { cuda_check(cudaGetLastError(), what); };
   for (int64_t g0 = 0; g0 < groups_all; g0 += per_launch) {
     const int64_t groups = std::min(per_launch, groups_all - g0);
-    const int64_t cols = std::min(count - g0 * 32, groups * 32);
-    const double *bg = b + g0 * 32 * ldb;
-    const unsigned io_grid = (unsigned)lane_io_blocks(groups, n);
-    const int64_t init_n = std::max(cols, groups);
-    lane_refine_init_kernel<<<(unsigned)((init_n + 255) / 256), 256, 0, stream>>>(groups, cols, rmax, bmax, prev, active);
-    cuda_check(cudaGetLastError(), "lane_refine_init_kernel launch");
-    lane_in_kernel<double><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(bg, ldb, cols, (int32_t)n, groups, natural, bl, nullptr);
-    cuda_check(cudaGetLastError(), "lane_in_kernel launch");
-    lane_in_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(bg, ldb, cols, (int32_t)n, groups, d->in_pos.get(), work,
-                                                                  nullptr);
-    cuda_check(cudaGetLastError(), "lane_in_kernel launch");
+    r.groups = groups;
+    r.count = std::min(count - g0 * 32, groups * 32);
+    r.b = b + g0 * 32 * ldb, r.x = x + g0 * 32 * ldx;
+    r.ratio_out = ratio_out ? ratio_out + g0 * 32 : nullptr;
+    r.steps_out = steps_out ? steps_out + g0 * 32 : nullptr;
+    const unsigned rows_grid = (unsigned)((groups * ((n + 15) / 16) + 7) / 8);  // warps of 16 rows, 8 per block
+    const unsigned group_grid = (unsigned)((groups + 127) / 128);
+    const int64_t init_n = std::max(r.count, groups);
+    lane_refine_init_kernel<<<(unsigned)((init_n + 255) / 256), 256, 0, stream>>>(r);
+    check("lane_refine_init_kernel launch");
+    lane_in_kernel<T><<<(unsigned)lane_io_blocks(groups, n), kLaneIoWarps * 32, 0, stream>>>(r.b, ldb, r.count, (int32_t)n,
+                                                                                           groups, d->in_pos.get(), work,
+                                                                                           nullptr);
+    check("lane_in_kernel launch");
+    const size_t vals = (size_t)groups * group_vals;
+    const unsigned carry_grid = (unsigned)((vals + 255) / 256);
     for (int32_t pass = 0; pass <= max_steps; ++pass) {
+      T *dk = pass == 1 ? dB : dA;  // this pass's correction
+      a.xout = dk;
       lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
-      cuda_check(cudaGetLastError(), "lane_solve_kernel launch");
-      lane_update_kernel<T><<<io_grid, 256, 0, stream>>>(work, d->out_pos.get(), xl, (int32_t)n, groups, active, pass == 0);
-      cuda_check(cudaGetLastError(), "lane_update_kernel launch");
-      lane_residual_kernel<<<io_grid, 256, 0, stream>>>(bl, xl, work, d->in_pos.get(), (int32_t)n, groups, cols,
-                                                        f->a_csr_ptr.get(), f->a_csr_idx.get(), f->a_csr_val.get(), active,
-                                                        rmax, pass == 0 ? bmax : nullptr);
-      cuda_check(cudaGetLastError(), "lane_residual_kernel launch");
-      lane_refine_decide_kernel<<<(unsigned)((groups + 127) / 128), 128, 0, stream>>>(
-          groups, cols, pass, max_steps, tolerance, rmax, bmax, prev, active, ratio_out ? ratio_out + g0 * 32 : nullptr,
-          steps_out ? steps_out + g0 * 32 : nullptr);
-      cuda_check(cudaGetLastError(), "lane_refine_decide_kernel launch");
+      check("lane_solve_kernel launch");
+      if (pass == 0)
+        lane_residual_kernel<0><<<rows_grid, 256, 0, stream>>>(r, dk, nullptr, nullptr, true);
+      else if (pass == 1)
+        lane_residual_kernel<1><<<rows_grid, 256, 0, stream>>>(r, dk, dA, nullptr, false);
+      else
+        lane_residual_kernel<2><<<rows_grid, 256, 0, stream>>>(r, dk, nullptr, X, false);
+      check("lane_residual_kernel launch");
+      lane_refine_decide_kernel<<<group_grid, 128, 0, stream>>>(r, pass, max_steps, tolerance);
+      check("lane_refine_decide_kernel launch");
+      // the best iterate back where this pass made no better (x_{pass-1}), or x0 where pass 0 ends
+      if (pass <= 1)
+        lane_restore_kernel<T><<<rows_grid, 256, 0, stream>>>(r, dA);
+      else
+        lane_restore_kernel<double><<<rows_grid, 256, 0, stream>>>(r, X);
+      check("lane_restore_kernel launch");
+      if (pass >= 1 && pass < max_steps) {  // x_pass in FP64 for the next pass's residual
+        if (pass == 1)
+          lane_carry_kernel<T><<<carry_grid, 256, 0, stream>>>(r, dA, dB, X);
+        else
+          lane_carry_kernel<double><<<carry_grid, 256, 0, stream>>>(r, X, dA, X);
+        check("lane_carry_kernel launch");
+      }
     }
-    lane_out_kernel<double><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(xl, cols, (int32_t)n, groups, natural,
-                                                                      x + g0 * 32 * ldx, ldx);
-    cuda_check(cudaGetLastError(), "lane_out_kernel launch");
   }
 }
 }  // namespace yb
@@ -1334,11 +1432,8 @@ extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rh
     require(!f->single, "a single-row factor needs no refinement: use yb_solve_many_device");
     cudaStream_t s = stream ? (cudaStream_t)stream : f->gpu->stream;
     const TileConfig &t32 = f->tile32;
-    // the refinement's passes cost more than the plain solve's launches, so its crossover with the
-    // domain refinement lies higher (10k-bus block: 2.15 against 2.33 ms at 4,096 right-hand sides,
-    // 3.36 against 3.02 ms at 6,144)
-    constexpr int64_t kLaneRefineMinCount = 5120;
-    if (t32.kind == kTileLane || (t32.kind == kTileAuto && count >= std::max(t32.lane_min_count, kLaneRefineMinCount))) {
+    if (t32.kind == kTileLane ||
+        (t32.kind == kTileAuto && count >= std::max(t32.lane_min_count, t32.refine_lane_min_count))) {
       DeviceLane *d = lane_pick<float>(f, t32, s);
       if (d && (t32.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane_refined(f, d, d_rhs, ldb, d_out, ldx, count, max_steps, tolerance, d_ratio, d_steps, s);
@@ -1351,7 +1446,7 @@ extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rh
       throw host::Error(host::kInvalidArgument, "the refined solve needs the domain solve, which this factor does not admit");
     const int64_t tiles = (count + cfg.width - 1) / cfg.width;
     const int64_t grid = std::min<int64_t>(tiles, (int64_t)f->gpu->sm_count);
-    f->refine_scratch.reserve((size_t)(grid * f->n * cfg.width));
+    f->refine_scratch.reserve((size_t)(2 * grid * f->n * cfg.width));  // each block's R and previous x
     RefineIO io{};
     io.scratch = f->refine_scratch.get();
     io.b = d_rhs, io.ldb = ldb, io.x = d_out, io.ldx = ldx;

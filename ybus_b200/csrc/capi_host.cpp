@@ -1,13 +1,14 @@
-// C ABI of the host-side factor producer: assemble a matrix from triplets, select rows and
-// columns, factor by AMD-ordered Cholesky or by LU (AMD or COLAMD column order), and copy the
-// factors out. These stand in for the ybus_sparse calls whose results ybus_cuda uploads
+// C ABI of the host-side factor producer (libybhost.so, no GPU code): assemble a matrix from
+// triplets, select rows and columns, factor by AMD-ordered Cholesky or by LU (AMD or COLAMD
+// column order), and copy the factors out; and the thread-local last error every entry point of
+// libybhost.so and libybgpu.so reports through. These stand in for the ybus_sparse calls whose results ybus_cuda uploads
 // (ybus_cuda/src/factor.rs:103-133 takes a `Cholesky<f64>` or `Lu<f64>` made by ybus_sparse).
 #include <memory>
 #include <vector>
 
-#include "../../include/ybgpu.h"
+#include "../../include/ybhost.h"
 #include "capi_common.hpp"
-#include "plan.hpp"
+#include "host/sparse.hpp"
 
 using namespace yb;
 using host::c128;
@@ -325,71 +326,5 @@ int32_t yb_host_etree(const yb_host_factor *f, int64_t *parent) {
 }
 
 void yb_host_factor_free(yb_host_factor *f) { delete f; }
-
-int32_t yb_domain_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
-                                  const int64_t *perm, int32_t value_bytes, int32_t warps, int32_t page_bytes,
-                                  int32_t cut, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *top_slot,
-                                  double *top_condition) {
-  return guard([&] {
-    require(n >= 0 && l_ptr && perm && info, "null argument");
-    host::Compressed<double> lower;
-    lower.rows = lower.cols = n;
-    lower.by_rows = true;
-    lower.ptr.assign(l_ptr, l_ptr + n + 1);
-    require(lower.ptr[0] == 0, "pointers must start at 0");
-    for (int64_t i = 0; i < n; ++i) require(lower.ptr[i + 1] >= lower.ptr[i], "pointers must not decrease");
-    const int64_t nnz = lower.ptr[n];
-    require(nnz == 0 || (l_idx && l_val), "null index or value array");
-    lower.idx.assign(l_idx, l_idx + nnz);
-    lower.val.assign(l_val, l_val + nnz);
-    for (int64_t v : lower.idx) require(v >= 0 && v < n, "an index is out of range");
-    host::Compressed<double> upper = host::reorient(lower);
-    upper.by_rows = true;
-    std::vector<int64_t> p(perm, perm + n);
-    const Plan<double> plan = build_plan<double>(n, lower, false, upper, p, p);
-    const DomainLayout lay = domain_layout(plan, value_bytes, warps, page_bytes, cut);
-    const int64_t pages = lay.warp_page.back();
-    const int64_t v[8] = {lay.K, lay.tail, lay.stages, lay.warps, pages, lay.records, lay.entries, lay.page_bytes};
-    std::copy(v, v + 8, info);
-    if (blob) std::copy(lay.blob.begin(), lay.blob.end(), blob);
-    if (warp_page) std::copy(lay.warp_page.begin(), lay.warp_page.end(), warp_page);
-    if (top_slot) std::copy(lay.tail_slot.begin(), lay.tail_slot.end(), top_slot);
-    if (top_condition) *top_condition = lay.top_condition;
-    return YB_OK;
-  });
-}
-
-int32_t yb_lane_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
-                                const int64_t *perm, int32_t value_bytes, int32_t page_bytes, int32_t max_slots,
-                                int32_t warps, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *in_pos,
-                                int32_t *out_pos) {
-  return guard([&] {
-    require(n >= 0 && l_ptr && perm && info, "null argument");
-    host::Compressed<double> lower;
-    lower.rows = lower.cols = n;
-    lower.by_rows = true;
-    lower.ptr.assign(l_ptr, l_ptr + n + 1);
-    require(lower.ptr[0] == 0, "pointers must start at 0");
-    for (int64_t i = 0; i < n; ++i) require(lower.ptr[i + 1] >= lower.ptr[i], "pointers must not decrease");
-    const int64_t nnz = lower.ptr[n];
-    require(nnz == 0 || (l_idx && l_val), "null index or value array");
-    lower.idx.assign(l_idx, l_idx + nnz);
-    lower.val.assign(l_val, l_val + nnz);
-    for (int64_t v : lower.idx) require(v >= 0 && v < n, "an index is out of range");
-    host::Compressed<double> upper = host::reorient(lower);
-    upper.by_rows = true;
-    std::vector<int64_t> p(perm, perm + n);
-    const Plan<double> plan = build_plan<double>(n, lower, false, upper, p, p);
-    const LaneLayout lay = lane_layout(plan, value_bytes, page_bytes, max_slots, warps);
-    const int64_t v[12] = {lay.slots, lay.warp_page.back(), lay.page_bytes, lay.fwd_live, lay.bwd_live, lay.fwd_entries,
-                           lay.bwd_entries, lay.warps, lay.domains, lay.top, lay.partials, 0};
-    std::copy(v, v + 12, info);
-    if (blob) std::copy(lay.blob.begin(), lay.blob.end(), blob);
-    if (warp_page) std::copy(lay.warp_page.begin(), lay.warp_page.end(), warp_page);
-    if (in_pos) std::copy(lay.in_pos.begin(), lay.in_pos.end(), in_pos);
-    if (out_pos) std::copy(lay.out_pos.begin(), lay.out_pos.end(), out_pos);
-    return YB_OK;
-  });
-}
 
 }  // extern "C"

@@ -402,9 +402,12 @@ struct AdjointIO {
 // for the next solve. R is updated rather than recomputed from x, so it is the residual of x up to
 // rounding of the order of eps ||A|| ||x||. The tile is done when every column's relative residual
 // ||r||inf / ||b||inf is at most the tolerance, after `max_steps` corrections, or when no column
-// above the tolerance at least halved its residual in the last step (stagnation). Unlike the CPU's
-// routine, which keeps each column's best iterate, the last iterate is kept; the final ratio and
-// the corrections taken are reported per column.
+// above the tolerance at least halved its residual in the last step (stagnation). Each column follows
+// the CPU's refine_normwise (accuracy.rs:93-118) on its own: it stops within the tolerance, on a NaN
+// ratio, when its ratio did not halve, or after max_steps; a column that has stopped is no longer
+// updated; and a column that stops on a correction that made it no better gets its previous iterate
+// back (kept for every column while it refines), so the x returned, the ratio and the corrections
+// reported are the best iterate's. The tile is done when its last column stops.
 struct RefineIO {
   static constexpr bool kRefine = true;
   const double *__restrict__ b;
@@ -419,7 +422,7 @@ struct RefineIO {
   const int32_t *__restrict__ a_ptr;  // [slices + 1]
   const int32_t *__restrict__ a_idx;
   const double *__restrict__ a_val;
-  double *scratch;  // gridDim.x blocks of n * W doubles
+  double *scratch;  // 2 gridDim.x blocks of n * W doubles: each block's R, then each block's previous x
   int32_t max_steps;
   double tolerance;
   double *__restrict__ ratio_out;  // [count] or null
@@ -427,6 +430,19 @@ struct RefineIO {
 
   template <int W> __device__ __forceinline__ double *residual(int n) const {
     return scratch + (size_t)blockIdx.x * n * W;
+  }
+  template <int W> __device__ __forceinline__ double *previous(int n) const {
+    return scratch + ((size_t)gridDim.x + blockIdx.x) * n * W;
+  }
+
+  // x of the columns in `mask` back to the previous iterate (the columns a last correction made no
+  // better), every thread of the block over the rows
+  template <int W> __device__ __forceinline__ void restore(uint32_t mask, int64_t col0, int n) const {
+    const double *P = previous<W>(n);
+    for (int r = threadIdx.x; r < n; r += blockDim.x)
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc)
+        if ((mask >> cc) & 1u) x[(col0 + cc) * ldx + r] = P[(size_t)r * W + cc];
   }
 
   // b into the slots and into R, and ||b||inf of each column into bnorm (for all threads)
@@ -464,13 +480,15 @@ struct RefineIO {
     block_max<W>(local, red, bnorm);
   }
 
-  // x (first) or x += d from the slots; R -= A d; ||R||inf per column into rnorm; R into the slots
+  // x (first) or x += d from the slots for the columns still refining (`active`), the x before
+  // kept; R -= A d; ||R||inf per column into rnorm; R into the slots
   template <class T, int W>
-  __device__ __forceinline__ void update(bool first, int64_t col0, int64_t count, int n, T *Ys,
+  __device__ __forceinline__ void update(bool first, uint32_t active, int64_t col0, int64_t count, int n, T *Ys,
                                          double (&rnorm)[W]) const {
     constexpr int U = W >= 8 ? 1 : 4;  // rows in flight per thread
     __shared__ double red[32][W];
     double *R = residual<W>(n);
+    double *P = previous<W>(n);
     double local[W];
 #pragma unroll
     for (int cc = 0; cc < W; ++cc) local[cc] = 0.0;
@@ -498,7 +516,10 @@ struct RefineIO {
         load_w<T, W>(Ys + (size_t)__ldg(out_slot + r) * W, d);
 #pragma unroll
         for (int cc = 0; cc < W; ++cc)
-          if (col0 + cc < count) x[(col0 + cc) * ldx + r] = xo[u][cc] + (double)d[cc];
+          if (col0 + cc < count && ((active >> cc) & 1u)) {
+            if (!first) P[(size_t)r * W + cc] = xo[u][cc];
+            x[(col0 + cc) * ldx + r] = xo[u][cc] + (double)d[cc];
+          }
         int p = p0[u];
 #pragma unroll 1
         for (; p + 96 < p1[u]; p += 128) {  // four entries of the row at a time, their loads together
@@ -640,9 +661,16 @@ __global__ void __launch_bounds__(512, 1) domain_tile_kernel(DomainArgs a, IO io
   for (int64_t tile = blockIdx.x; tile < a.tiles; tile += gridDim.x) {
     const int64_t col0 = tile * W;
     const int64_t it = (tile - blockIdx.x) / gridDim.x;
-    double bnorm[W], prev[W];
+    // per column (the same in every thread): ||b||inf, the current and the best relative residual,
+    // the best's corrections, and which columns still refine
+    double bnorm[W], cur[W], best[W];
+    int best_steps[W];
+    uint32_t active = 0;
 #pragma unroll
-    for (int cc = 0; cc < W; ++cc) bnorm[cc] = 0.0, prev[cc] = __longlong_as_double(0x7ff0000000000000LL);
+    for (int cc = 0; cc < W; ++cc) {
+      bnorm[cc] = 0.0, cur[cc] = best[cc] = __longlong_as_double(0x7ff0000000000000LL), best_steps[cc] = 0;
+      if (col0 + cc < a.count) active |= 1u << cc;
+    }
     for (int pass = 0;; ++pass) {
     // diagnostics rows: the first 4 tiles, or for a refined solve the first 4 passes of tile 0
     const int64_t mark = IO::kRefine ? (it == 0 ? pass : 4) : it;
@@ -828,30 +856,39 @@ __global__ void __launch_bounds__(512, 1) domain_tile_kernel(DomainArgs a, IO io
     }
     if constexpr (IO::kRefine) {
       double rnorm[W];
-      io.template update<T, W>(pass == 0, col0, a.count, n, Ys, rnorm);
+      io.template update<T, W>(pass == 0, active, col0, a.count, n, Ys, rnorm);
       if (pc) pc[3] = clock64();
-      // the relative residual of each column after `pass` corrections (accuracy.rs:58-79), and
-      // whether another correction is worth it
-      bool open = false, progress = false, bad = false;
+      // each refining column's relative residual after `pass` corrections (accuracy.rs:58-79) and
+      // refine_normwise's decision for it (accuracy.rs:93-118)
+      uint32_t restore = 0;
 #pragma unroll
       for (int cc = 0; cc < W; ++cc) {
-        if (col0 + cc >= a.count) continue;
+        if (!((active >> cc) & 1u)) continue;
         const double ratio = bnorm[cc] > 0.0 ? rnorm[cc] / bnorm[cc]
                                              : (rnorm[cc] > 0.0 ? __longlong_as_double(0x7ff0000000000000LL) : 0.0);
-        bad = bad || (ratio != ratio);
-        if (ratio > io.tolerance) {
-          open = true;
-          progress = progress || (ratio <= 0.5 * prev[cc]);
+        bool stop;
+        if (pass == 0) {
+          best[cc] = cur[cc] = ratio;
+          stop = ratio <= io.tolerance || io.max_steps < 1;
+        } else {
+          const double previous = cur[cc];
+          cur[cc] = ratio;
+          const bool improved = ratio < best[cc];
+          if (improved) best[cc] = ratio, best_steps[cc] = pass;
+          stop = ratio != ratio || ratio > 0.5 * previous || ratio <= io.tolerance || pass >= io.max_steps;
+          if (stop && !improved && best_steps[cc] == pass - 1) restore |= 1u << cc;
         }
-        prev[cc] = ratio;
-      }
-      if (!open || !progress || bad || pass >= io.max_steps) {
-#pragma unroll
-        for (int cc = 0; cc < W; ++cc)
-          if (threadIdx.x == cc && col0 + cc < a.count) {
-            if (io.ratio_out) io.ratio_out[col0 + cc] = prev[cc];
-            if (io.steps_out) io.steps_out[col0 + cc] = pass;
+        if (stop) {
+          active &= ~(1u << cc);
+          if (threadIdx.x == cc) {
+            if (io.ratio_out) io.ratio_out[col0 + cc] = best[cc];
+            if (io.steps_out) io.steps_out[col0 + cc] = best_steps[cc];
           }
+        }
+      }
+      if (restore) io.template restore<W>(restore, col0, n);
+      if (!active) {
+        __syncthreads();  // the restore's reads of the previous iterate, before the next tile
         break;
       }
     } else {

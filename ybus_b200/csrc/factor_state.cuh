@@ -111,6 +111,9 @@ struct TileConfig {
   // fewer leave SMs idle, where the domain solve's tiles spread over all of them)
   int64_t lane_min_count = 3072;
   int lane_warps = 8, lane_page = 0;  // the lane solve's warps per block (one group of 32 right-hand sides), page bytes
+  // the refined solve takes the lane solve from this many right-hand sides on (its passes cost more
+  // launches than the plain solve's, so its crossover with the fused domain refinement lies higher)
+  int64_t refine_lane_min_count = 5120;
 };
 
 // A lane layout on the device (LaneLayout in plan.hpp).
@@ -119,6 +122,12 @@ struct DeviceLane {
   int64_t entries = 0, pages = 0;
   DeviceArray<uint8_t> blob;
   DeviceArray<int32_t> warp_page, in_pos, out_pos;
+  std::vector<int32_t> host_out_pos;
+  // the refined solve's copy of the attached A (LaneRefineArgs' res_*): natural rows in slices of
+  // 32, columns as work rows; built at its first use, for the matrix attached then
+  int64_t res_matrix = -1;  // the attach count it was built for
+  DeviceArray<int32_t> res_ptr, res_len, res_col;
+  DeviceArray<double> res_val;
 };
 
 // A domain layout on the device (DomainLayout in plan.hpp).
@@ -184,9 +193,13 @@ struct yb_factor {
   yb::DeviceArray<int32_t> a_ptr, a_idx;
   yb::DeviceArray<int32_t> a_csr_ptr, a_csr_idx;  // A as attached (CSR, natural order)
   yb::DeviceArray<double> a_csr_val;
-  yb::DeviceArray<uint8_t> refine_state;  // the lane refinement's per-column maxima and per-group flags
+  yb::DeviceArray<uint8_t> refine_state;  // the lane refinement's per-column and per-group state
   yb::DeviceArray<double> a_val;
-  yb::DeviceArray<double> refine_scratch;  // per block n * W residuals
+  yb::DeviceArray<double> refine_scratch;  // per block n * W residuals; the lane refinement's FP64 iterate
+  yb::DeviceArray<float> refine_parts;     // the lane refinement's FP32 corrections (two work arrays)
+  std::vector<int64_t> a_host_ptr, a_host_idx;  // A as attached (CSR, natural order), on the host
+  std::vector<double> a_host_val;
+  int64_t a_attached = 0;                  // how many times a matrix was attached
   // a complex LU factor (yb_factor_from_lu_complex): its plan, its sweeps in complex128 and
   // complex64, and the complex matrix attached for refinement (CSR, natural order)
   bool is_complex = false;

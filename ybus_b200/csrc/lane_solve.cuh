@@ -38,6 +38,8 @@ struct LaneArgs {
   const int32_t *__restrict__ warp_page;  // [warps + 1]
   int32_t *error;                         // set to 1 if a wait ran out or a stream is malformed
   const uint8_t *group_active;            // [groups] 0: the group is skipped; null: every group runs
+  void *xout;  // null: the solutions overwrite the work array; else an array of the work array's layout
+               // that receives them (the backward rows' results and the top solutions the domains read)
 };
 
 // A warp's shared memory: live slots, the prefetch ring, the page ring and its barriers.
@@ -143,6 +145,8 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
   uint64_t *full = &lane_at<uint64_t>(ring + (uint32_t)S * PB);
   const uint32_t smem_s = smem_u32(lane_shared);  // the shared window address of offset 0
   uint8_t *w_lane = reinterpret_cast<uint8_t *>(work + (size_t)blockIdx.x * a.n * 32 + lane);
+  uint8_t *x_lane = a.xout ? reinterpret_cast<uint8_t *>(static_cast<T *>(a.xout) + (size_t)blockIdx.x * a.n * 32 + lane)
+                           : w_lane;
   uint8_t *part_lane = reinterpret_cast<uint8_t *>(partial + (size_t)blockIdx.x * a.partials * 32 + lane);
   const int p0 = __ldg(a.warp_page + warp), np = __ldg(a.warp_page + warp + 1) - p0;
   const uint8_t *stream = a.blob + (size_t)p0 * PB;
@@ -189,11 +193,11 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
       z = b * dinv;
       *reinterpret_cast<T *>(w_lane + h.y) = z;
     };
-    // the end of a backward row: x into its slot and the work row
+    // the end of a backward row: x into its slot and its row of the output
     auto backward = [&]() {
       const T x = z * dinv;
       lane_at<T>(self) = x;
-      *reinterpret_cast<T *>(w_lane + h.y) = x;
+      *reinterpret_cast<T *>(x_lane + h.y) = x;
     };
     // a prefetch block: the batch's rows into their half of the ring, then the batch before waited for
     auto prefetch = [&](uint32_t at) {
@@ -302,7 +306,7 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
             T v;
             uint32_t w;
             lane_entry(e + min(c + q, count - 1) * E, v, w, o[q]);
-            x[q] = *reinterpret_cast<const T *>(w_lane + w);
+            x[q] = *reinterpret_cast<const T *>(x_lane + w);
           }
 #pragma unroll
           for (int q = 0; q < 4; ++q)

@@ -9,9 +9,11 @@
 // instead of the scratch buffer the ordinary entry points grow on demand.
 //
 // The array is kNoAllocScratchBytes (16 MiB) of device memory that every GPU which loads the
-// library holds until the process exits. The first call on a device looks the array's device
-// address up (cudaGetSymbolAddress, with that device current) and keeps it; make that first call
-// before any stream capture. All calls share the one array and it keeps whatever the last call
+// library holds until the process exits. yb_gpu_new looks the array's device address up
+// (cudaGetSymbolAddress, with that device current) and keeps it, which also makes the driver load
+// this file's module and place the array then: with lazy module loading (the default since CUDA
+// 12.2) that would otherwise happen at the first solve of this entry point, which would then
+// allocate after all. All calls share the one array and it keeps whatever the last call
 // left there: nothing in it needs to start at zero (each tile's load overwrites every slot it
 // uses), but calls whose kernels overlap on the GPU, on two streams or two host threads, race on
 // it and must be serialised by the caller.
@@ -84,7 +86,30 @@ void dispatch(yb_factor *f, const yb::DeviceSweep<T> &fwd, const yb::DeviceSweep
   }
 }
 
+// Loads every kernel the entry point may launch (a function's code is placed in device memory when
+// it is first used, under lazy loading)
+template <class T, int W> void load_kernel() {
+  cudaFuncAttributes attr{};
+  yb::cuda_check(cudaFuncGetAttributes(&attr, yb::tile_solve_kernel<T, W, yb::Load::Dense, yb::Store::Dense>),
+                 "loading the allocation-free solve's kernels");
+}
+template <class T> void load_kernels() {
+  load_kernel<T, 1>(), load_kernel<T, 2>(), load_kernel<T, 4>(), load_kernel<T, 8>(), load_kernel<T, 16>(),
+      load_kernel<T, 32>();
+}
+
 }  // namespace
+
+namespace yb {
+// Called by yb_gpu_new with `device` current: the fixed array is placed, its address kept and the
+// entry point's kernels loaded now, so that no later call of yb_solve_many_device_noalloc loads a
+// module or allocates.
+void noalloc_prepare(int device) {
+  scratch_address(device);
+  load_kernels<double>();
+  load_kernels<float>();
+}
+}  // namespace yb
 
 extern "C" int32_t yb_solve_many_device_noalloc(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out,
                                                 int64_t ldx, int64_t count, int32_t precision, void *stream) {

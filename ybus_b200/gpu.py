@@ -237,14 +237,6 @@ class GpuFactor:
         return {"tile": w.value, "cut": cut.value, "top": top.value, "records": rec.value, "bytes": by.value,
                 "smem": sm.value, "model_cycles": cyc.value}
 
-    def reference_spsm_solve_device(self, d_rhs: int, d_out: int, count: int, width: int = 1024) -> float:
-        """For comparison only: ybus_cuda's route (cuSPARSE SpSM, lower then upper, blocks of
-        `width`) on this factor's device arrays. Returns the solves' time in ms."""
-        n = self.dim()
-        ms = C.c_double()
-        _check(lib().yb_reference_spsm_solve(self._h, d_rhs, n, d_out, n, count, width, C.byref(ms)))
-        return ms.value
-
     def lane_info(self, precision: int = FP64) -> dict:
         """The lane solve's layout: slots, pages, peaks of live values, shared memory per block,
         warps per block, domains, top rows and partial values per block."""
@@ -261,6 +253,22 @@ class GpuFactor:
     def set_lane_min_count(self, precision: int, min_count: int) -> None:
         """The number of right-hand sides from which the automatic choice takes the lane solve."""
         _check(lib().yb_factor_set_lane_min_count(self._h, precision, min_count))
+
+    def set_refine_lane_min_count(self, min_count: int) -> None:
+        """The number of right-hand sides from which the refined solve takes the FP32 lane solve."""
+        _check(lib().yb_factor_set_refine_lane_min_count(self._h, min_count))
+
+    def lane_min_count(self, precision: int = FP64) -> int:
+        """The number of right-hand sides from which the automatic choice takes the lane solve."""
+        v = C.c_int64()
+        _check(lib().yb_factor_lane_min_counts(self._h, precision, C.byref(v), None))
+        return v.value
+
+    def refine_lane_min_count(self) -> int:
+        """The refined solve's own lane threshold."""
+        v = C.c_int64()
+        _check(lib().yb_factor_lane_min_counts(self._h, FP32, None, C.byref(v)))
+        return v.value
 
     def time_lane(self, on: bool = True) -> None:
         """Records CUDA events around the gather, solve and scatter of every lane-solve launch

@@ -2,7 +2,8 @@
 
 These are the ybus_sparse calls whose results ybus_cuda uploads (`CsrMatrix::cholesky`,
 `CscMatrix::analyze_lu(..).factor(..)`, ybus_sparse/src/compressed_matrix/{cholesky,lu}.rs),
-computed in FP64 (or complex128) by libybgpu's C++ host code.
+computed in FP64 (or complex128) by libybhost.so's C++ code; the layout diagnostics at the end
+call libybgpu.so's host-side layout builders.
 """
 from __future__ import annotations
 
@@ -12,7 +13,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import check, lib, ptr
+from ._lib import check, ptr
+from ._lib import host_lib as lib
 
 NATURAL = _lib.YB_ORDER_NATURAL
 AMD = _lib.YB_ORDER_AMD
@@ -186,13 +188,14 @@ def domain_layout(chol: HostCholesky, value_bytes: int = 8, warps: int = 16, pag
     l = chol.l
     val = np.ascontiguousarray(l.val, dtype=np.float64)
     args = (chol.n, ptr(l.ptr), ptr(l.idx), ptr(val), ptr(chol.perm), value_bytes, warps, page_bytes, cut)
-    check(lib().yb_domain_layout_cholesky(*args, ptr(info), None, None, None, None))
+    check(_lib.lib().yb_domain_layout_cholesky(*args, ptr(info), None, None, None, None))
     cut_, top, stages, w, pages, records, entries, pb = (int(v) for v in info)
     blob = np.zeros(pages * pb, np.uint8)
     warp_page = np.zeros(w + 1, np.int32)
     top_slot = np.zeros(max(top, 1), np.int32)
     cond = C.c_double()
-    check(lib().yb_domain_layout_cholesky(*args, ptr(info), ptr(blob), ptr(warp_page), ptr(top_slot), C.byref(cond)))
+    check(_lib.lib().yb_domain_layout_cholesky(*args, ptr(info), ptr(blob), ptr(warp_page), ptr(top_slot),
+                                               C.byref(cond)))
     return {"cut": cut_, "top": top, "stages": stages, "warps": w, "pages": pages, "records": records,
             "entries": entries, "page_bytes": pb, "blob": blob, "warp_page": warp_page, "top_slot": top_slot[:top],
             "value_bytes": value_bytes, "top_condition": cond.value}
@@ -206,13 +209,13 @@ def lane_layout(chol: HostCholesky, value_bytes: int = 8, page_bytes: int = 2048
     l = chol.l
     val = np.ascontiguousarray(l.val, dtype=np.float64)
     args = (chol.n, ptr(l.ptr), ptr(l.idx), ptr(val), ptr(chol.perm), value_bytes, page_bytes, max_slots, warps)
-    check(lib().yb_lane_layout_cholesky(*args, ptr(info), None, None, None, None))
+    check(_lib.lib().yb_lane_layout_cholesky(*args, ptr(info), None, None, None, None))
     slots, pages, pb, fwd_live, bwd_live, fwd_entries, bwd_entries, w, domains, top, partials, _ = (int(v) for v in info)
     blob = np.zeros(pages * pb, np.uint8)
     warp_page = np.zeros(w + 1, np.int32)
     in_pos = np.zeros(chol.n, np.int32)
     out_pos = np.zeros(chol.n, np.int32)
-    check(lib().yb_lane_layout_cholesky(*args, ptr(info), ptr(blob), ptr(warp_page), ptr(in_pos), ptr(out_pos)))
+    check(_lib.lib().yb_lane_layout_cholesky(*args, ptr(info), ptr(blob), ptr(warp_page), ptr(in_pos), ptr(out_pos)))
     return {"slots": slots, "pages": pages, "page_bytes": pb, "fwd_live": fwd_live, "bwd_live": bwd_live,
             "fwd_entries": fwd_entries, "bwd_entries": bwd_entries, "warps": w, "domains": domains, "top": top,
             "partials": partials, "blob": blob, "warp_page": warp_page, "in_pos": in_pos, "out_pos": out_pos,

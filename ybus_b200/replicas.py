@@ -1,8 +1,10 @@
 """One process per GPU for the solve path, which shards with no data-path exchange: right-hand
 sides, outage cases and networks are independent, so every rank solves its own share on its own GPU
-and the processes meet only to start timing together and to take the slowest rank's time. These
-helpers hold that logic apart from the GPU so that it runs (and is tested) on any torch.distributed
-backend, gloo on the CPU included."""
+and the processes meet only to start timing together and to take the slowest rank's time. The one
+exchange is the adjoint's: the gradient with respect to the branch susceptances is a sum over
+scenarios, so ranks that split the scenarios add their partial sums (in rank order, so the result
+does not depend on timing). These helpers hold that logic apart from the GPU so that it runs (and
+is tested) on any torch.distributed backend, gloo on the CPU included."""
 from __future__ import annotations
 
 import os
@@ -44,6 +46,41 @@ def shard(units: int, rank: int, world: int) -> range:
     base, extra = divmod(int(units), world)
     start = rank * base + min(rank, extra)
     return range(start, start + base + (1 if rank < extra else 0))
+
+
+def lpt(weights, world: int) -> list[list[int]]:
+    """Longest processing time first: units in decreasing weight (ties by index), each to the rank
+    with the least weight so far (ties to the lowest rank). Returns each rank's units in increasing
+    index order; every unit once. Used for outage cases (weighted by their right-hand sides) and
+    networks (weighted by factor entries times right-hand sides)."""
+    if world < 1:
+        raise ValueError("a world of at least one rank")
+    w = [float(x) for x in weights]
+    order = sorted(range(len(w)), key=lambda i: (-w[i], i))
+    load = [0.0] * world
+    share: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += w[i]
+        share[r].append(i)
+    return [sorted(s) for s in share]
+
+
+def sum_in_rank_order(values):
+    """The sum over ranks of every rank's float64 array `values` (its own for one process), added
+    in rank order on every rank, so all ranks get the same bits whatever the backend's reduction
+    order: an all-gather, then rank 0's + rank 1's + ..."""
+    import numpy as np
+    v = np.ascontiguousarray(values, np.float64)
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return v.copy()
+    t = torch.from_numpy(v).to(_device())
+    parts = [torch.empty_like(t) for _ in range(dist.get_world_size())]
+    dist.all_gather(parts, t)
+    total = parts[0].cpu().numpy().copy()
+    for q in parts[1:]:
+        total += q.cpu().numpy()
+    return total
 
 
 def whole_job_rate(units_per_rank: int, world: int, seconds: float) -> float:
