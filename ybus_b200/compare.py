@@ -22,7 +22,7 @@ def _open() -> C.CDLL:
             raise RuntimeError(f"{path} is not built")
         _lib = C.CDLL(str(path), mode=os.RTLD_LOCAL)
         _lib.ybc_spsm_solve.restype = C.c_int32
-        _lib.ybc_spsm_solve.argtypes = [C.c_int64] + [C.c_void_p] * 9 + [C.c_int64, C.c_void_p, C.c_int64, C.c_int64,
+        _lib.ybc_spsm_solve.argtypes = [C.c_int64] + [C.c_void_p] * 8 + [C.c_int64, C.c_void_p, C.c_int64, C.c_int64,
                                                                         C.c_int64, C.c_void_p, C.c_char_p, C.c_size_t]
     return _lib
 
