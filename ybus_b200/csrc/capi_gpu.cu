@@ -1372,8 +1372,8 @@ void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t l
     r.b = b + g0 * 32 * ldb, r.x = x + g0 * 32 * ldx;
     r.ratio_out = ratio_out ? ratio_out + g0 * 32 : nullptr;
     r.steps_out = steps_out ? steps_out + g0 * 32 : nullptr;
-    const unsigned rows_grid = (unsigned)((groups * ((n + 15) / 16) + 7) / 8);  // warps of 16 rows, 8 per block
-    const unsigned group_grid = (unsigned)((groups + 127) / 128);
+    const unsigned rows_grid = (unsigned)(groups * res_parts(n));  // blocks of kResRows rows of one group
+    const unsigned group_grid = (unsigned)((groups * 32 + 127) / 128);  // a warp per group
     const int64_t init_n = std::max(r.count, groups);
     lane_refine_init_kernel<<<(unsigned)((init_n + 255) / 256), 256, 0, stream>>>(r);
     check("lane_refine_init_kernel launch");
@@ -1381,33 +1381,33 @@ void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t l
                                                                                            groups, d->in_pos.get(), work,
                                                                                            nullptr);
     check("lane_in_kernel launch");
-    const size_t vals = (size_t)groups * group_vals;
-    const unsigned carry_grid = (unsigned)((vals + 255) / 256);
+    const int64_t carry_parts = std::max<int64_t>(1, (int64_t)((group_vals + 8191) / 8192));  // 8,192 values a block
+    const unsigned carry_grid = (unsigned)(groups * carry_parts);
     for (int32_t pass = 0; pass <= max_steps; ++pass) {
       T *dk = pass == 1 ? dB : dA;  // this pass's correction
       a.xout = dk;
       lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
       check("lane_solve_kernel launch");
       if (pass == 0)
-        lane_residual_kernel<0><<<rows_grid, 256, 0, stream>>>(r, dk, nullptr, nullptr, true);
+        lane_residual_kernel<0><<<rows_grid, kResWarps * 32, 0, stream>>>(r, dk, nullptr, nullptr, true);
       else if (pass == 1)
-        lane_residual_kernel<1><<<rows_grid, 256, 0, stream>>>(r, dk, dA, nullptr, false);
+        lane_residual_kernel<1><<<rows_grid, kResWarps * 32, 0, stream>>>(r, dk, dA, nullptr, false);
       else
-        lane_residual_kernel<2><<<rows_grid, 256, 0, stream>>>(r, dk, nullptr, X, false);
+        lane_residual_kernel<2><<<rows_grid, kResWarps * 32, 0, stream>>>(r, dk, nullptr, X, false);
       check("lane_residual_kernel launch");
       lane_refine_decide_kernel<<<group_grid, 128, 0, stream>>>(r, pass, max_steps, tolerance);
       check("lane_refine_decide_kernel launch");
       // the best iterate back where this pass made no better (x_{pass-1}), or x0 where pass 0 ends
       if (pass <= 1)
-        lane_restore_kernel<T><<<rows_grid, 256, 0, stream>>>(r, dA);
+        lane_restore_kernel<T><<<rows_grid, kResWarps * 32, 0, stream>>>(r, dA);
       else
-        lane_restore_kernel<double><<<rows_grid, 256, 0, stream>>>(r, X);
+        lane_restore_kernel<double><<<rows_grid, kResWarps * 32, 0, stream>>>(r, X);
       check("lane_restore_kernel launch");
       if (pass >= 1 && pass < max_steps) {  // x_pass in FP64 for the next pass's residual
         if (pass == 1)
-          lane_carry_kernel<T><<<carry_grid, 256, 0, stream>>>(r, dA, dB, X);
+          lane_carry_kernel<T><<<carry_grid, 256, 0, stream>>>(r, dA, dB, X, carry_parts);
         else
-          lane_carry_kernel<double><<<carry_grid, 256, 0, stream>>>(r, X, dA, X);
+          lane_carry_kernel<double><<<carry_grid, 256, 0, stream>>>(r, X, dA, X, carry_parts);
         check("lane_carry_kernel launch");
       }
     }

@@ -58,17 +58,25 @@ __device__ __forceinline__ unsigned long long abs_bits(double v) {
   return (unsigned long long)__double_as_longlong(fabs(v));
 }
 
-// Each lane holds 16 values, one per column of its half of the warp (lanes 0-15: columns 0-15,
-// lanes 16-31: columns 16-31), for its row. Reduces every column to its maximum over the half's 16
-// rows by a transposing butterfly: at each step a lane keeps half of its values and trades the
-// other half with its partner; after four steps lane l holds column l's maximum.
-__device__ __forceinline__ unsigned long long column_max16(unsigned long long (&v)[16]) {
+// The residual and restore kernels' lanes and blocks: a warp takes chunks of 8 consecutive rows of
+// one group, four lanes per row, each lane 8 of the group's 32 columns (lane = quarter * 8 + row, so
+// the 8 lanes of a quarter hold the chunk's 8 rows of the same 8 columns); a block of kResWarps
+// warps, each taking kResChunks chunks in turn, covers kResRows rows of one group and returns at
+// once, as a whole, when that group has stopped.
+constexpr int kResWarps = 8, kResChunks = 8, kResRows = kResWarps * kResChunks * 8;
+__host__ __device__ inline int64_t res_parts(int64_t n) { return (n + kResRows - 1) / kResRows; }
+
+// Each lane holds 8 values, one per column of its quarter, for its row. Reduces every column to its
+// maximum over the quarter's 8 rows by a transposing butterfly: at each step a lane keeps half of
+// its values and trades the other half with its partner; after three steps lane l holds column l's
+// maximum.
+__device__ __forceinline__ unsigned long long column_max8(unsigned long long (&v)[8]) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int s = 8, half = 8; s >= 1; s >>= 1, half >>= 1) {
+  for (int s = 4, half = 4; s >= 1; s >>= 1, half >>= 1) {
     const bool upper = (lane & s) != 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < 4; ++k) {
       if (k < half) {
         const unsigned long long send = upper ? v[k] : v[k + half];
         const unsigned long long keep = upper ? v[k + half] : v[k];
@@ -80,191 +88,239 @@ __device__ __forceinline__ unsigned long long column_max16(unsigned long long (&
   return v[0];
 }
 
-// 16 FP32 values of a work row (64 bytes, 32-byte aligned) as doubles
-__device__ __forceinline__ void load16(const float *p, double (&v)[16]) {
-#pragma unroll
-  for (int c = 0; c < 16; c += 8) {
-    float f[8];
-    asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]), "=f"(f[6]), "=f"(f[7])
-                 : "l"(p + c));
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v[c + k] = f[k];
-  }
+// 8 FP32 values (32 bytes, 32-byte aligned) in one load
+__device__ __forceinline__ void load8(const float *p, float (&v)[8]) {
+  asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+               : "l"(p));
 }
-// 16 FP64 values of a row (128 bytes, 32-byte aligned), added to v
-__device__ __forceinline__ void add16(const double *p, double (&v)[16]) {
+// 8 FP64 values (64 bytes, 32-byte aligned) in two loads
+__device__ __forceinline__ void load8(const double *p, double (&v)[8]) {
 #pragma unroll
-  for (int c = 0; c < 16; c += 4) {
-    double d[4];
-    asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(d[0]), "=d"(d[1]), "=d"(d[2]), "=d"(d[3]) : "l"(p + c));
-#pragma unroll
-    for (int k = 0; k < 4; ++k) v[c + k] = d[k] + v[c + k];
-  }
+  for (int c = 0; c < 8; c += 4)
+    asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v[c]), "=d"(v[c + 1]), "=d"(v[c + 2]), "=d"(v[c + 3])
+                 : "l"(p + c));
 }
 
-// The iterate's 16 values of this lane's half at work row `wr` of group g: d, plus the base
-// (x_{k-1}) when there is one (BASE 1: FP32 parts, BASE 2: FP64), added in FP64 as base + d.
-template <int BASE>
-__device__ __forceinline__ void iterate16(size_t at, const float *__restrict__ d, const float *__restrict__ base32,
-                                          const double *__restrict__ base64, double (&x)[16]) {
-  load16(d + at, x);
-  if constexpr (BASE == 1) {
-    double bv[16];
-    load16(base32 + at, bv);
-#pragma unroll
-    for (int c = 0; c < 16; ++c) x[c] = bv[c] + x[c];
-  } else if constexpr (BASE == 2) {
-    add16(base64 + at, x);
+// The iterate's 8 values of one lane's quarter at one work row, as loaded: the correction d and,
+// when there is one, the base x_{k-1} (BASE 1: FP32 parts, BASE 2: FP64); value(c) = base + d in
+// FP64. AT_ONCE: the neighbours whose loads the residual keeps in flight together.
+template <int BASE> struct Iterate8 {
+  static constexpr int AT_ONCE = 2;
+  float d[8];
+  __device__ __forceinline__ void load(size_t at, const float *dd, const float *, const double *) { load8(dd + at, d); }
+  __device__ __forceinline__ double value(int c) const { return (double)d[c]; }
+};
+template <> struct Iterate8<1> {
+  static constexpr int AT_ONCE = 2;
+  float d[8], b[8];
+  __device__ __forceinline__ void load(size_t at, const float *dd, const float *b32, const double *) {
+    load8(dd + at, d);
+    load8(b32 + at, b);
   }
-}
+  __device__ __forceinline__ double value(int c) const { return (double)b[c] + (double)d[c]; }
+};
+template <> struct Iterate8<2> {
+  static constexpr int AT_ONCE = 1;
+  float d[8];
+  double b[8];
+  __device__ __forceinline__ void load(size_t at, const float *dd, const float *, const double *b64) {
+    load8(dd + at, d);
+    load8(b64 + at, b);
+  }
+  __device__ __forceinline__ double value(int c) const { return b[c] + (double)d[c]; }
+};
 
 // The residual R = b - A x of the groups still refining, in FP64, with x = base + d formed at every
-// row read (BASE 0: x = d, pass 0). Two lanes per row, each the 16 columns of its half of the group;
-// a warp takes 16 consecutive rows of one group, so b's and x's columns are read and written 16
-// rows (128 bytes) at a time. R goes in FP32 to the work array (the next pass's right-hand side),
-// each column's ||R||inf (and on the first pass ||b||inf) by atomic maximum of its bit pattern, and
-// x_k to the caller's columns of write_mask.
+// row read (BASE 0: x = d, pass 0). Lanes as above: b's and x's columns are read and written 8 rows
+// (64 bytes) at a time, and each row of x a lane reads is one 32-byte load, the four lanes of a row
+// covering its 128-byte line, so an instruction touches 8 lines (against 16 with two lanes per row
+// and 32 with one column per lane: L1's request rate, not DRAM, bounds this kernel). A row's
+// neighbours are read AT_ONCE at a time. R goes in FP32 to the work array (the next pass's
+// right-hand side); each column's ||R||inf (and on the first pass ||b||inf) is reduced over the
+// block's rows in shared memory and then taken by one atomic maximum of its bit pattern per block;
+// x_k goes to the caller's columns of write_mask.
 template <int BASE>
-__global__ void __launch_bounds__(256) lane_residual_kernel(LaneRefineArgs a, const float *__restrict__ d,
-                                                            const float *__restrict__ base32,
-                                                            const double *__restrict__ base64, bool first) {
-  const int lane = threadIdx.x & 31, half = lane >> 4;
-  const int64_t w = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
-  const int64_t chunks = (a.n + 15) / 16, g = w / chunks;
-  if (g >= a.groups || !a.active[g]) return;  // the whole warp
-  const int i = (int)(w % chunks) * 16 + (lane & 15);
-  const bool row = i < a.n;
-  const int c0 = half * 16;                                   // this lane's first column in the group
+__global__ void __launch_bounds__(kResWarps * 32, 3) lane_residual_kernel(LaneRefineArgs a, const float *__restrict__ d,
+                                                                        const float *__restrict__ base32,
+                                                                        const double *__restrict__ base64, bool first) {
+  constexpr int AT = Iterate8<BASE>::AT_ONCE;
+  __shared__ unsigned long long red[2][kResWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t parts = res_parts(a.n), g = blockIdx.x / parts, part = blockIdx.x - g * parts;
+  if (g >= a.groups || !a.active[g]) return;  // the whole block
+  const int c0 = (lane >> 3) * 8;                             // this lane's first column in the group
   const int64_t col0 = g * 32 + c0;                           // ... in the launch
   const int64_t left = a.count - col0;
-  const int cols = left <= 0 ? 0 : (left >= 16 ? 16 : (int)left);
+  const int cols = left <= 0 ? 0 : (left >= 8 ? 8 : (int)left);
   const size_t gw = (size_t)g * a.n;                          // the group's first work row
-  double acc[16];
-  const double *bc = a.b + col0 * a.ldb + i;
+  uint32_t write = 0;
+  if constexpr (BASE != 0) write = (a.write_mask[g] >> c0) & 0xffu;
+  unsigned long long rmax = 0ull, bmax = 0ull;  // column `lane`'s maxima over this warp's rows
+  for (int k = 0; k < kResChunks; ++k) {
+    const int64_t i0 = ((part * kResWarps + warp) * kResChunks + k) * 8;
+    if (i0 >= a.n) break;  // the whole warp
+    const int i = (int)i0 + (lane & 7);
+    const bool row = i < a.n;
+    double acc[8];
+    const double *bc = a.b + col0 * a.ldb + i;
 #pragma unroll
-  for (int c = 0; c < 16; ++c) acc[c] = (row && c < cols) ? __ldg(bc + c * a.ldb) : 0.0;
-  if (first) {
-    unsigned long long bm[16];
+    for (int c = 0; c < 8; ++c) acc[c] = (row && c < cols) ? __ldg(bc + c * a.ldb) : 0.0;
+    if (first) {
+      unsigned long long bm[8];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) bm[c] = abs_bits(acc[c]);
-    const unsigned long long m = column_max16(bm);
-    if (g * 32 + lane < a.count) atomicMax(a.bmax + g * 32 + lane, m);
-  }
-  if (row) {
-    const int len = __ldg(a.res_len + i);
-    const int64_t e = __ldg(a.res_ptr + i / 32) + (i & 31);
-    for (int q = 0; q < len; ++q) {
-      const int32_t wj = __ldg(a.res_col + e + 32 * q);
-      const double v = __ldg(a.res_val + e + 32 * q);
-      double xj[16];
-      iterate16<BASE>((gw + wj) * 32 + c0, d, base32, base64, xj);
-#pragma unroll
-      for (int c = 0; c < 16; ++c) acc[c] = fma(-v, xj[c], acc[c]);
+      for (int c = 0; c < 8; ++c) bm[c] = abs_bits(acc[c]);
+      const unsigned long long m = column_max8(bm);
+      bmax = m > bmax ? m : bmax;
     }
-    // R into the work array, this half's 16 values in two 32-byte stores
-    float *r = a.work + (gw + __ldg(a.in_pos + i)) * 32 + c0;
+    if (row) {
+      const int len = __ldg(a.res_len + i);
+      const int64_t e = __ldg(a.res_ptr + i / 32) + (i & 31);
+      for (int q = 0; q < len; q += AT) {  // in stored order
+        int32_t w[AT];
+        double v[AT];
 #pragma unroll
-    for (int c = 0; c < 16; c += 8)
-      asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(r + c), "f"((float)acc[c]),
-                   "f"((float)acc[c + 1]), "f"((float)acc[c + 2]), "f"((float)acc[c + 3]), "f"((float)acc[c + 4]),
-                   "f"((float)acc[c + 5]), "f"((float)acc[c + 6]), "f"((float)acc[c + 7])
+        for (int t = 0; t < AT; ++t) {
+          const bool ok = q + t < len;
+          w[t] = ok ? __ldg(a.res_col + e + 32 * (q + t)) : 0;
+          v[t] = ok ? __ldg(a.res_val + e + 32 * (q + t)) : 0.0;
+        }
+        Iterate8<BASE> x[AT];
+#pragma unroll
+        for (int t = 0; t < AT; ++t) x[t].load((gw + w[t]) * 32 + c0, d, base32, base64);
+#pragma unroll
+        for (int t = 0; t < AT; ++t)
+          if (q + t < len) {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc[c] = fma(-v[t], x[t].value(c), acc[c]);
+          }
+      }
+      // R into the work array, this quarter's 8 values in one 32-byte store
+      float *r = a.work + (gw + __ldg(a.in_pos + i)) * 32 + c0;
+      asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(r), "f"((float)acc[0]),
+                   "f"((float)acc[1]), "f"((float)acc[2]), "f"((float)acc[3]), "f"((float)acc[4]), "f"((float)acc[5]),
+                   "f"((float)acc[6]), "f"((float)acc[7])
                    : "memory");
-  }
-  unsigned long long rm[16];
-#pragma unroll
-  for (int c = 0; c < 16; ++c) rm[c] = (row && c < cols) ? abs_bits(acc[c]) : 0ull;
-  const unsigned long long m = column_max16(rm);
-  if (g * 32 + lane < a.count) atomicMax(a.rmax + g * 32 + lane, m);
-  if constexpr (BASE != 0) {
-    const uint32_t mask = (a.write_mask[g] >> c0) & 0xffffu;
-    if (row && mask) {  // x_k of this row for the caller
-      double xi[16];
-      iterate16<BASE>((gw + __ldg(a.out_pos + i)) * 32 + c0, d, base32, base64, xi);
-      double *xc = a.x + col0 * a.ldx + i;
-#pragma unroll
-      for (int c = 0; c < 16; ++c)
-        if ((mask >> c) & 1u) xc[c * a.ldx] = xi[c];
     }
+    unsigned long long rm[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) rm[c] = (row && c < cols) ? abs_bits(acc[c]) : 0ull;
+    const unsigned long long m = column_max8(rm);
+    rmax = m > rmax ? m : rmax;
+    if constexpr (BASE != 0) {
+      if (row && write) {  // x_k of this row for the caller
+        Iterate8<BASE> xi;
+        xi.load((gw + __ldg(a.out_pos + i)) * 32 + c0, d, base32, base64);
+        double *xc = a.x + col0 * a.ldx + i;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if ((write >> c) & 1u) xc[c * a.ldx] = xi.value(c);
+      }
+    }
+  }
+  // the block's maxima, one atomic per column
+  red[0][warp][lane] = rmax;
+  red[1][warp][lane] = bmax;
+  __syncthreads();
+  if (warp == 0 && g * 32 + lane < a.count) {
+    unsigned long long mr = 0ull, mb = 0ull;
+#pragma unroll
+    for (int w = 0; w < kResWarps; ++w) {
+      mr = red[0][w][lane] > mr ? red[0][w][lane] : mr;
+      mb = red[1][w][lane] > mb ? red[1][w][lane] : mb;
+    }
+    if (mr) atomicMax(a.rmax + g * 32 + lane, mr);
+    if (first && mb) atomicMax(a.bmax + g * 32 + lane, mb);
   }
 }
 
-// One thread per group: each column's relative residual after `pass` corrections and the state of
-// refine_normwise (accuracy.rs:93-118): pass 0 takes x0 as the best; a later pass keeps x_k if its
-// ratio is below the best, else x_{k-1} is put back in the caller's x (restore_mask); a column stops
-// within the tolerance, on a NaN ratio, when the ratio did not halve, or after max_steps, and then
-// gets its best ratio and correction count. write_mask becomes the columns whose best is x_pass, the
-// ones the next pass may overwrite; a column that stops at pass 0 has its x0 written by the restore.
+// One warp per group, one lane per column: each column's relative residual after `pass`
+// corrections and the state of refine_normwise (accuracy.rs:93-118): pass 0 takes x0 as the best; a
+// later pass keeps x_k if its ratio is below the best, else x_{k-1} is put back in the caller's x
+// (restore_mask); a column stops within the tolerance, on a NaN ratio, when the ratio did not
+// halve, or after max_steps, and then gets its best ratio and correction count. write_mask becomes
+// the columns whose best is x_pass, the ones the next pass may overwrite; a column that stops at
+// pass 0 has its x0 written by the restore.
 __global__ void lane_refine_decide_kernel(LaneRefineArgs a, int32_t pass, int32_t max_steps, double tolerance) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= a.groups) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (g >= a.groups) return;  // the whole warp
   if (!a.active[g]) {
-    a.restore_mask[g] = 0;
+    if (lane == 0) a.restore_mask[g] = 0;
     return;
   }
-  uint32_t act = a.col_active[g], write = 0, restore = 0;
-  const uint32_t wrote = a.write_mask[g];
-  for (int c = 0; c < 32; ++c) {
-    if (!((act >> c) & 1u)) continue;
-    const int64_t col = g * 32 + c;
+  const uint32_t act = a.col_active[g], wrote = a.write_mask[g];
+  bool stop = false, write = false, restore = false;
+  if ((act >> lane) & 1u) {
+    const int64_t col = g * 32 + lane;
     const double rn = __longlong_as_double((long long)a.rmax[col]), bn = __longlong_as_double((long long)a.bmax[col]);
     const double ratio = bn > 0.0 ? rn / bn : (rn > 0.0 ? __longlong_as_double(0x7ff0000000000000LL) : 0.0);
     a.rmax[col] = 0ull;
-    bool stop;
     if (pass == 0) {
       a.best[col] = ratio, a.best_steps[col] = 0, a.cur[col] = ratio;
       stop = ratio <= tolerance || max_steps < 1;
-      if (stop) restore |= 1u << c;
+      restore = stop;
     } else {
       const double previous = a.cur[col];
       a.cur[col] = ratio;
       const bool improved = ratio < a.best[col];
       if (improved) a.best[col] = ratio, a.best_steps[col] = pass;
-      if (!improved && ((wrote >> c) & 1u)) restore |= 1u << c;
+      restore = !improved && ((wrote >> lane) & 1u);
       stop = ratio != ratio || ratio > 0.5 * previous || ratio <= tolerance || pass >= max_steps;
     }
     if (stop) {
-      act &= ~(1u << c);
       if (a.ratio_out) a.ratio_out[col] = a.best[col];
       if (a.steps_out) a.steps_out[col] = a.best_steps[col];
-    } else if (a.best_steps[col] == pass) {
-      write |= 1u << c;
+    } else {
+      write = a.best_steps[col] == pass;
     }
   }
-  a.col_active[g] = act, a.write_mask[g] = write, a.restore_mask[g] = restore;
-  if (!act) a.active[g] = 0;
+  const uint32_t stopped = __ballot_sync(0xffffffffu, stop), writes = __ballot_sync(0xffffffffu, write),
+                 restores = __ballot_sync(0xffffffffu, restore);
+  if (lane == 0) {
+    const uint32_t left = act & ~stopped;
+    a.col_active[g] = left, a.write_mask[g] = writes, a.restore_mask[g] = restores;
+    if (!left) a.active[g] = 0;
+  }
 }
 
 // The caller's x of the columns in restore_mask set to the iterate `base` holds (FP32 parts or
 // FP64, in the work array's layout): x_{pass-1} for the columns a pass made no better, x0 for the
-// columns that stopped at pass 0. Two lanes per row as in the residual; groups with nothing to
-// restore return at once.
+// columns that stopped at pass 0. Blocks and lanes as in the residual; a block whose group has
+// nothing to restore returns at once.
 template <class B>
-__global__ void __launch_bounds__(256) lane_restore_kernel(LaneRefineArgs a, const B *__restrict__ base) {
-  const int lane = threadIdx.x & 31, half = lane >> 4;
-  const int64_t w = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
-  const int64_t chunks = (a.n + 15) / 16, g = w / chunks;
+__global__ void __launch_bounds__(kResWarps * 32) lane_restore_kernel(LaneRefineArgs a, const B *__restrict__ base) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t parts = res_parts(a.n), g = blockIdx.x / parts, part = blockIdx.x - g * parts;
   if (g >= a.groups) return;
-  const int c0 = half * 16;
-  const uint32_t mask = (a.restore_mask[g] >> c0) & 0xffffu;
-  const int i = (int)(w % chunks) * 16 + (lane & 15);
-  if (!mask || i >= a.n) return;
-  const B *src = base + ((size_t)g * a.n + __ldg(a.out_pos + i)) * 32 + c0;
-  double *xc = a.x + (g * 32 + c0) * a.ldx + i;
+  const uint32_t all = a.restore_mask[g];
+  if (!all) return;  // the whole block
+  const int c0 = (lane >> 3) * 8;
+  const uint32_t mask = (all >> c0) & 0xffu;
+  if (!mask) return;
+  for (int k = 0; k < kResChunks; ++k) {
+    const int64_t i0 = ((part * kResWarps + warp) * kResChunks + k) * 8;
+    const int i = (int)i0 + (lane & 7);
+    if (i >= a.n) break;
+    const B *src = base + ((size_t)g * a.n + __ldg(a.out_pos + i)) * 32 + c0;
+    double *xc = a.x + (g * 32 + c0) * a.ldx + i;
 #pragma unroll
-  for (int c = 0; c < 16; ++c)
-    if ((mask >> c) & 1u) xc[c * a.ldx] = (double)src[c];
+    for (int c = 0; c < 8; ++c)
+      if ((mask >> c) & 1u) xc[c * a.ldx] = (double)src[c];
+  }
 }
 
-// X = base + d over every work row of the groups still refining: the iterate kept in FP64 for a
-// further pass (base FP32 parts on pass 1, X itself after).
+// X = base + d over the work rows of the groups still refining: the iterate kept in FP64 for a
+// further pass (base FP32 parts on pass 1, X itself after). A block takes one of `parts` slices of
+// one group's values and returns at once when the group has stopped.
 template <class B>
 __global__ void __launch_bounds__(256) lane_carry_kernel(LaneRefineArgs a, const B *base, const float *__restrict__ d,
-                                                        double *X) {  // base may be X itself
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // one value of the launch's groups
-  const int64_t g = k / ((int64_t)a.n * 32);
+                                                        double *X, int64_t parts) {  // base may be X itself
+  const int64_t g = blockIdx.x / parts, part = blockIdx.x - g * parts;
   if (g >= a.groups || !a.active[g]) return;
-  X[k] = (double)base[k] + (double)d[k];
+  const int64_t gv = (int64_t)a.n * 32, per = (gv + parts - 1) / parts;
+  const int64_t lo = g * gv + part * per, hi = g * gv + (gv < (part + 1) * per ? gv : (part + 1) * per);
+  for (int64_t k = lo + threadIdx.x; k < hi; k += blockDim.x) X[k] = (double)base[k] + (double)d[k];
 }
 
 // Every group refining with every column below `count`, no maxima yet.
