@@ -267,7 +267,8 @@ def workload_n1(gpu, steps: int, warm: int, rank: int, world: int, device: int) 
         dt, (rows, vals, bad, sing), ck = _timed_wall(
             lambda: net.outage_loadings_batch(outaged, sp, inj, cases.weights, prec), steps, warm, device)
         modes[name] = {"scenarios_s": int(cases.scenario_ptr[-1]) / dt, "ms_per_step": dt * 1e3,
-                       "not_finite": int(bad.sum()), "singular": int(sing.sum()), "clocks": ck}
+                       "not_finite": int(((bad & 1) != 0).sum()), "suspect_angles": int(((bad & 2) != 0).sum()),
+                       "singular": int(sing.sum()), "clocks": ck}
     best = max(modes, key=lambda m: modes[m]["scenarios_s"])
     return {"metric": "N-1 scenarios screened/s (largest loading per scenario), pinned host arrays in and out",
             "value": modes[best]["scenarios_s"], "unit": "scenarios/s", "higher_is_better": True,

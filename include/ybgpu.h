@@ -265,7 +265,8 @@ yb_factor *yb_dc_network_factor(yb_dc_network *net);
 /* One flag per branch: whether it is a bridge (its outage islands the network). */
 int32_t yb_dc_bridges(const yb_dc_network *net, uint8_t *bridge);
 /* `DcGpuSensitivity::ptdf_columns` (gpu.rs:506-528; sensitivity.rs:233): for an injection at each
- * of `count` buses, withdrawn at the slack, every branch's flow: n_branch x count, column-major. */
+ * of `count` buses, withdrawn at the slack, every branch's flow: n_branch x count, column-major;
+ * with slack weights set (yb_dc_set_slack_weights) each column less the shift H w. */
 int32_t yb_dc_ptdf_columns(yb_dc_network *net, int64_t count, const int64_t *buses, double *out);
 /* `DcGpuSensitivity::ptdf_transfers` (gpu.rs:532; sensitivity.rs:284): a transfer from each
  * from_bus to its to_bus. */
@@ -275,19 +276,48 @@ int32_t yb_dc_ptdf_transfers(yb_dc_network *net, int64_t count, const int64_t *f
  * every branch's change in flow as a fraction of its flow before, -1 for itself, a NaN column for a
  * bridge; n_branch x count. */
 int32_t yb_dc_lodf_columns(yb_dc_network *net, int64_t count, const int64_t *branches, double *out);
+/* `DcSensitivity`'s distributed slack (`PtdfSlack::Weights`, dc/sensitivity.rs:101-126, 256-263;
+ * on the GPU `DcGpuSensitivity::set_shifted`, gpu.rs:443-583): weights per bus (n_bus), normalized
+ * to sum to 1, or NULL for the single slack again. The shift H w, every branch's flow for the
+ * weighted injections, is computed here by one solve; yb_dc_ptdf_columns then subtracts it from
+ * every column (PTDF - (PTDF w) 1'), while transfers and LODF columns do not depend on the slack.
+ * YB_ERROR_INVALID_ARGUMENT when the weights' sum is zero or not finite. */
+int32_t yb_dc_set_slack_weights(yb_dc_network *net, const double *weights);
+/* `DcGpuStudy::solve_many` (gpu.rs:214-260) with the placement on the device: for each of `count`
+ * injection scenarios (n_bus x count, column-major, by bus; the slack's entry is ignored), the
+ * angles theta = B'^-1 p placed over the buses (the slack's angle 0; n_bus x count) and every
+ * branch's flow b (theta_f - theta_t) (n_branch x count), and per scenario flags: 1 a flow not
+ * finite, 2 an angle not finite or above 1e5 in magnitude (the check `DcStudy::place` makes before
+ * it accepts a solution, dc.rs:558-564). Any output may be NULL. */
+int32_t yb_dc_solve_many(yb_dc_network *net, int64_t count, const double *injections, double *theta, double *flows,
+                         int32_t *flags);
+/* `DcStudy::outage` for outages of several branches (dc/outage.rs:126-241: W = D^-1 - C'Y,
+ * theta' = x + Y W^-1 C'x) and `DcGpuStudy::solve_branch_outages` (gpu.rs:273-322, one branch a
+ * case) as whole solutions, on the device: case c takes out the branches branch_ptr[c] ..
+ * branch_ptr[c+1] - 1 of `branches` (up to 16, sorted and repeats dropped as `outaged_branches`
+ * does) and solves the scenario columns scenario_ptr[c] .. scenario_ptr[c+1] - 1 of `injections`
+ * (n_bus x total). Per scenario the angles over the buses and the flows, the outaged branches'
+ * zero, and the flags of yb_dc_solve_many; per case whether W is singular (the outage islands a
+ * bus: the scenarios keep the base angles and the caller decides, as the reference's CPU fallback
+ * would). Every output may be NULL. */
+int32_t yb_dc_outage_solutions(yb_dc_network *net, int64_t cases, const int64_t *branch_ptr, const int64_t *branches,
+                               const int64_t *scenario_ptr, const double *injections, double *theta, double *flows,
+                               int32_t *flags, int32_t *singular);
 /* No ybus counterpart as such (the reference screens one base per outage, `DcGpuStudy::
  * outage_loadings`, gpu.rs:334-430): N-1 screening of many injection scenarios per outage. Case c
  * takes out branch outaged[c] (a rank-one update of B', dc/outage.rs:126-241) and has the scenario
  * columns scenario_ptr[c] .. scenario_ptr[c+1] - 1 of `injections` (n_bus x total, column-major, by
  * bus; the slack's entry is ignored). For every scenario column: the branch with the largest
- * |flow| * weight (weights NULL: 1), the loading, whether any flow is not finite; per case whether
- * the update is singular (1/b - c'y = 0: a bridge). All cases run as one pair solve and one
+ * |flow| * weight (weights NULL: 1), the loading, and flags: 1 a flow not finite, 2 an angle not
+ * finite or above 1e5 in magnitude (with a singular case, the reference's reasons to distrust a
+ * screened outage and solve it again on the CPU, gpu.rs:406-410); per case whether the update is
+ * singular (1/b - c'y = 0: a bridge). All cases run as one pair solve and one
  * scenario solve with the update, flows and maxima fused (YB_FP64), captured in a CUDA graph that
  * later calls of the same sizes replay; or with FP32 substitution and FP64 refinement, then the
  * same epilogue (YB_FP32; the slack must be bus 0). */
 int32_t yb_dc_outage_loadings_batch(yb_dc_network *net, int64_t cases, const int64_t *outaged,
                                     const int64_t *scenario_ptr, const double *injections, const double *weights,
-                                    int32_t precision, int64_t *max_branch, double *max_loading, int32_t *not_finite,
+                                    int32_t precision, int64_t *max_branch, double *max_loading, int32_t *flags,
                                     int32_t *singular);
 
 /* No ybus counterpart: the adjoint of a flow loss over a DC network, a forward/backward pair (the

@@ -125,6 +125,9 @@ SIGNATURES: dict[str, tuple] = {
     "yb_dc_ptdf_transfers": (i32, [vp, i64, vp, vp, vp]),
     "yb_dc_lodf_columns": (i32, [vp, i64, vp, vp]),
     "yb_dc_outage_loadings_batch": (i32, [vp, i64, vp, vp, vp, vp, i32, vp, vp, vp, vp]),
+    "yb_dc_set_slack_weights": (i32, [vp, vp]),
+    "yb_dc_solve_many": (i32, [vp, i64, vp, vp, vp, vp]),
+    "yb_dc_outage_solutions": (i32, [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp]),
     "yb_dc_adjoint_new": (i32, [vp, i64, C.POINTER(vp)]),
     "yb_dc_adjoint_forward": (i32, [vp, vp, vp, dbl, vp, vp]),
     "yb_dc_adjoint_backward": (i32, [vp, vp, vp]),

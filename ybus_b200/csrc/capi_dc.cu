@@ -42,6 +42,13 @@ struct yb_dc_network {
   DeviceArray<int32_t> d_case_of, d_plus_u, d_minus_u, d_plus_slot, d_minus_slot, d_branch, d_bad, d_sing, d_steps;
   DeviceArray<int64_t> d_row;
   DeviceArray<double> d_value;
+  // the whole-solution calls' workspace (dc_solutions)
+  struct Solutions {
+    DeviceArray<int32_t> case_of, bus_of, unknown, out_ptr, out_branch, col_ptr, pu, mu, p0, p1, piv, singular, flags;
+    DeviceArray<double> inj, rhs, theta, theta_bus, flows, y, lu, s0, s1, invb;
+  } sol;
+  // the distributed slack's shift H w over the branches, negated (empty: the single slack)
+  std::vector<double> negated_shift;
   // a captured graph of the FP64 screening for the sizes it was made for
   cudaGraphExec_t graph = nullptr;
   int64_t graph_cases = -1, graph_columns = -1;
@@ -149,9 +156,10 @@ __global__ void outage_epilogue_kernel(const double *__restrict__ theta, int64_t
     const int uf = br_u_f[l], ut = br_u_t[l];
     const double tf = uf < 0 ? 0.0 : __dadd_rn(th[uf], __dmul_rn(z, y[uf]));
     const double tt = ut < 0 ? 0.0 : __dadd_rn(th[ut], __dmul_rn(z, y[ut]));
+    if ((uf >= 0 && !(fabs(tf) <= 1e5)) || (ut >= 0 && !(fabs(tt) <= 1e5))) bad |= 2;
     const double f = l == k ? 0.0 : __dadd_rn(__dmul_rn(br_b[l], tf), __dmul_rn(-br_b[l], tt));
     if (!isfinite(f)) {
-      bad = 1;
+      bad |= 1;
       continue;
     }
     const double load = fabs(f) * weight[l];
@@ -189,6 +197,304 @@ __global__ void case_cy_kernel(const double *__restrict__ Y, int64_t ldy, const 
   if (plus_u[c] >= 0) s = __dadd_rn(s, y[plus_u[c]]);
   if (minus_u[c] >= 0) s = __dsub_rn(s, y[minus_u[c]]);
   cy[c] = s;
+}
+
+// ---- whole solutions: solves with placement, multi-branch outages ------------------------------
+
+constexpr int kMaxOutageRank = 16;  // the branches one outage case may take out together
+
+// The right-hand sides over the unknowns from injections over the buses: rhs[s][u] = inj[s][bus_of[u]].
+__global__ void unknowns_of_buses_kernel(const double *__restrict__ inj, int64_t ldi, const int32_t *__restrict__ bus_of,
+                                         int64_t n, int64_t S, double *__restrict__ rhs) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n * S) return;
+  const int64_t s = k / n, u = k - s * n;
+  rhs[k] = inj[s * ldi + bus_of[u]];
+}
+
+// c'v for an outaged branch's c over the unknowns, summed as ybus_powerflow's outage update sums it
+// (dc/outage.rs:200-202): from 0, each entry sign * v[position] in position order.
+__device__ __forceinline__ double c_dot(int32_t p0, double s0, int32_t p1, double s1, const double *v) {
+  double d = __dadd_rn(0.0, s0 * v[p0]);
+  if (p1 >= 0) d = __dadd_rn(d, s1 * v[p1]);
+  return d;
+}
+
+// Per case (one thread): W = D^-1 - C'Y over its m outaged branches that touch an unknown
+// (dc/outage.rs:205-216: W_ij = -c_i'y_j, plus 1/b_i on the diagonal), factored in place by LU with
+// partial pivoting into lu (kMaxOutageRank^2 per case, row-major) and piv; singular when a pivot is
+// zero or not finite (reactances that cancel), besides the cases the host found to island a bus.
+__global__ void outage_lu_kernel(const double *__restrict__ Y, int64_t ldy, const int32_t *__restrict__ col_ptr,
+                                 const int32_t *__restrict__ pos0, const double *__restrict__ sign0,
+                                 const int32_t *__restrict__ pos1, const double *__restrict__ sign1,
+                                 const double *__restrict__ invb, int64_t cases, double *__restrict__ lu,
+                                 int32_t *__restrict__ piv, int32_t *__restrict__ singular) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cases || singular[c]) return;  // a case that islands a bus, found on the host
+  constexpr int R = kMaxOutageRank;
+  const int q0 = col_ptr[c], m = col_ptr[c + 1] - q0;
+  double *a = lu + c * R * R;
+  int32_t *pv = piv + c * R;
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) {
+      double w = -c_dot(pos0[q0 + i], sign0[q0 + i], pos1[q0 + i], sign1[q0 + i], Y + (int64_t)(q0 + j) * ldy);
+      if (i == j) w = __dadd_rn(w, invb[q0 + i]);
+      a[i * R + j] = w;
+    }
+  bool sing = false;
+  for (int k = 0; k < m; ++k) {
+    int p = k;
+    for (int i = k + 1; i < m; ++i)
+      if (fabs(a[i * R + k]) > fabs(a[p * R + k])) p = i;
+    pv[k] = p;
+    if (p != k)
+      for (int j = 0; j < m; ++j) {
+        const double t = a[k * R + j];
+        a[k * R + j] = a[p * R + j], a[p * R + j] = t;
+      }
+    const double d = a[k * R + k];
+    if (d == 0.0 || !isfinite(d)) {
+      sing = true;
+      break;
+    }
+    for (int i = k + 1; i < m; ++i) {
+      const double l = __ddiv_rn(a[i * R + k], d);
+      a[i * R + k] = l;
+      for (int j = k + 1; j < m; ++j) a[i * R + j] = __dsub_rn(a[i * R + j], __dmul_rn(l, a[k * R + j]));
+    }
+  }
+  singular[c] = sing ? 1 : 0;
+}
+
+// One block per scenario column of a case with outaged branches: ctx_i = c_i'theta0, z = W^-1 ctx by
+// the case's LU, and theta = theta0 + sum_j z_j y_j over the unknowns in place, in j order with the
+// products and sums rounded apart as the CPU's x_i += z_j y_i (dc/outage.rs:217-236). A singular
+// case's columns keep theta0 (the case is flagged).
+__global__ void outage_update_kernel(double *__restrict__ theta, int64_t n, const int32_t *__restrict__ case_of,
+                                     const int32_t *__restrict__ col_ptr, const int32_t *__restrict__ pos0,
+                                     const double *__restrict__ sign0, const int32_t *__restrict__ pos1,
+                                     const double *__restrict__ sign1, const double *__restrict__ lu,
+                                     const int32_t *__restrict__ piv, const int32_t *__restrict__ singular,
+                                     const double *__restrict__ Y, int64_t ldy) {
+  constexpr int R = kMaxOutageRank;
+  __shared__ double z[R];
+  const int64_t s = blockIdx.x;
+  const int c = case_of[s];
+  const int q0 = col_ptr[c], m = col_ptr[c + 1] - q0;
+  if (m == 0 || singular[c]) return;  // the whole block
+  double *th = theta + s * n;
+  if (threadIdx.x == 0) {
+    double v[R];
+    for (int i = 0; i < m; ++i) v[i] = c_dot(pos0[q0 + i], sign0[q0 + i], pos1[q0 + i], sign1[q0 + i], th);
+    const double *a = lu + (int64_t)c * R * R;
+    const int32_t *pv = piv + (int64_t)c * R;
+    for (int k = 0; k < m; ++k) {  // P: the row swaps in order, then L (unit) and U
+      const int p = pv[k];
+      if (p != k) {
+        const double t = v[k];
+        v[k] = v[p], v[p] = t;
+      }
+    }
+    for (int i = 1; i < m; ++i)
+      for (int j = 0; j < i; ++j) v[i] = __dsub_rn(v[i], __dmul_rn(a[i * R + j], v[j]));
+    for (int i = m - 1; i >= 0; --i) {
+      for (int j = i + 1; j < m; ++j) v[i] = __dsub_rn(v[i], __dmul_rn(a[i * R + j], v[j]));
+      v[i] = __ddiv_rn(v[i], a[i * R + i]);
+    }
+    for (int i = 0; i < m; ++i) z[i] = v[i];
+  }
+  __syncthreads();
+  for (int64_t r = threadIdx.x; r < n; r += blockDim.x) {
+    double x = th[r];
+    for (int j = 0; j < m; ++j) x = __dadd_rn(x, __dmul_rn(z[j], __ldg(Y + (int64_t)(q0 + j) * ldy + r)));
+    th[r] = x;
+  }
+}
+
+// One block per scenario column: theta over the buses (the slack's 0) and each branch's flow
+// b_k theta_f + (-b_k) theta_t (the row of Bf), zero for the branches the column's case takes out;
+// flags: 1 a flow not finite, 2 an angle not finite or above 1e5 in magnitude (the check of
+// ybus_powerflow's DcStudy::place, dc.rs:558-564).
+__global__ void place_flows_kernel(const double *__restrict__ theta, int64_t n, int32_t n_bus,
+                                   const int32_t *__restrict__ unknown, int32_t nl, const int32_t *__restrict__ br_u_f,
+                                   const int32_t *__restrict__ br_u_t, const double *__restrict__ br_b,
+                                   const int32_t *__restrict__ case_of, const int32_t *__restrict__ out_ptr,
+                                   const int32_t *__restrict__ out_branch, double *__restrict__ theta_bus,
+                                   double *__restrict__ flows, int32_t *__restrict__ flags) {
+  __shared__ int red[32];
+  const int64_t s = blockIdx.x;
+  const double *th = theta + s * n;
+  int bad = 0;
+  for (int i = threadIdx.x; i < n_bus; i += blockDim.x) {
+    const int u = unknown[i];
+    const double t = u < 0 ? 0.0 : th[u];
+    if (u >= 0 && !(fabs(t) <= 1e5)) bad |= 2;
+    if (theta_bus) theta_bus[s * n_bus + i] = t;
+  }
+  const int c = case_of ? case_of[s] : 0;
+  const int o0 = case_of ? out_ptr[c] : 0, o1 = case_of ? out_ptr[c + 1] : 0;
+  for (int l = threadIdx.x; l < nl; l += blockDim.x) {
+    bool out = false;
+    for (int o = o0; o < o1; ++o) out |= out_branch[o] == l;
+    const int uf = br_u_f[l], ut = br_u_t[l];
+    const double tf = uf < 0 ? 0.0 : th[uf], tt = ut < 0 ? 0.0 : th[ut];
+    const double b = br_b[l];
+    const double f = out ? 0.0 : __dadd_rn(__dmul_rn(b, tf), __dmul_rn(-b, tt));
+    if (!isfinite(f)) bad |= 1;
+    if (flows) flows[s * (int64_t)nl + l] = f;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) bad |= __shfl_xor_sync(0xffffffffu, bad, off);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = bad;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) bad |= red[w];
+    flags[s] = bad;
+  }
+}
+
+// Solutions of many scenarios with outages of several branches each: case c takes out the branches
+// branch_ptr[c] .. branch_ptr[c+1] - 1 of `branches` (none: the plain solve) and has the scenario
+// columns scenario_ptr[c] .. scenario_ptr[c+1] - 1 of `injections` (n_bus x S, by bus). On the
+// device: theta0 = B'^-1 p of every scenario, Y = B'^-1 C of every outaged branch (pair solves),
+// every case's W = D^-1 - C'Y factored, every scenario's theta updated, placed over the buses and
+// turned into flows. Outputs (host arrays, each may be null): theta over the buses (n_bus x S),
+// flows (n_branch x S), flags per scenario (place_flows_kernel's), singular per case.
+void dc_solutions(yb_dc_network *net, int64_t cases, const int64_t *branch_ptr, const int64_t *branches,
+                  const int64_t *scenario_ptr, const double *injections, double *theta, double *flows, int32_t *flags,
+                  int32_t *singular) {
+  require(cases >= 1 && scenario_ptr && scenario_ptr[0] == 0, "scenario pointers must start at 0");
+  for (int64_t c = 0; c < cases; ++c) require(scenario_ptr[c + 1] >= scenario_ptr[c], "scenario pointers must not decrease");
+  const int64_t S = scenario_ptr[cases];
+  require(S == 0 || injections, "null injections");
+  if (branch_ptr) {
+    require(branch_ptr[0] == 0, "branch pointers must start at 0");
+    for (int64_t c = 0; c < cases; ++c) require(branch_ptr[c + 1] >= branch_ptr[c], "branch pointers must not decrease");
+    require(branch_ptr[cases] == 0 || branches, "null branches");
+  }
+  yb_factor *f = net->factor;
+  const int64_t n = net->n, nl = net->n_branch, nb = net->n_bus;
+  // per case: its outaged branches sorted without repeats (flows zeroed), and the columns of C of
+  // those that touch an unknown, each with its entries in position order
+  std::vector<int32_t> out_ptr(1, 0), out_branch, col_ptr(1, 0), pu, mu, p0, p1;
+  std::vector<double> s0, s1, invb;
+  for (int64_t c = 0; c < cases; ++c) {
+    std::vector<int64_t> rows;
+    if (branch_ptr)
+      for (int64_t j = branch_ptr[c]; j < branch_ptr[c + 1]; ++j) {
+        require(branches[j] >= 0 && branches[j] < nl, "an outaged branch is out of range");
+        rows.push_back(branches[j]);
+      }
+    std::sort(rows.begin(), rows.end());
+    rows.erase(std::unique(rows.begin(), rows.end()), rows.end());
+    require((int64_t)rows.size() <= kMaxOutageRank, "a case takes out more than 16 branches");
+    for (const int64_t k : rows) {
+      out_branch.push_back((int32_t)k);
+      const int64_t pf = net->unknown[net->from[k]], pt = net->unknown[net->to[k]];
+      if (net->from[k] == net->to[k] || (pf < 0 && pt < 0)) continue;
+      pu.push_back((int32_t)pf), mu.push_back((int32_t)pt);
+      // the entries (position, sign) in position order: the from end +1, the to end -1
+      std::vector<std::pair<int64_t, double>> e;
+      if (pf >= 0) e.push_back({pf, 1.0});
+      if (pt >= 0) e.push_back({pt, -1.0});
+      std::sort(e.begin(), e.end());
+      p0.push_back((int32_t)e[0].first), s0.push_back(e[0].second);
+      p1.push_back(e.size() > 1 ? (int32_t)e[1].first : -1), s1.push_back(e.size() > 1 ? e[1].second : 0.0);
+      invb.push_back(1.0 / net->b[k]);
+    }
+    out_ptr.push_back((int32_t)out_branch.size());
+    col_ptr.push_back((int32_t)pu.size());
+  }
+  const int64_t K = (int64_t)pu.size();
+  // the cases whose outage leaves a bus without a path to the slack (`outaged_branches`' reach
+  // check, dc/outage.rs:243+): W is singular in exact arithmetic, whatever rounding makes of it
+  std::vector<int32_t> islands((size_t)cases, 0);
+  {
+    std::vector<int64_t> parent((size_t)nb);
+    std::vector<uint8_t> out((size_t)nl, 0);
+    auto find = [&](int64_t a) {
+      while (parent[(size_t)a] != a) a = parent[(size_t)a] = parent[(size_t)parent[(size_t)a]];
+      return a;
+    };
+    for (int64_t c = 0; c < cases; ++c) {
+      const int32_t o0 = out_ptr[(size_t)c], o1 = out_ptr[(size_t)c + 1];
+      if (o1 == o0) continue;
+      if (o1 - o0 == 1) {
+        islands[(size_t)c] = net->bridge[(size_t)out_branch[(size_t)o0]] ? 1 : 0;
+        continue;
+      }
+      for (int32_t o = o0; o < o1; ++o) out[(size_t)out_branch[(size_t)o]] = 1;
+      for (int64_t i = 0; i < nb; ++i) parent[(size_t)i] = i;
+      int64_t parts = nb;
+      for (int64_t k = 0; k < nl; ++k) {
+        if (out[(size_t)k]) continue;
+        const int64_t a = find(net->from[k]), b = find(net->to[k]);
+        if (a != b) parent[(size_t)a] = b, --parts;
+      }
+      for (int32_t o = o0; o < o1; ++o) out[(size_t)out_branch[(size_t)o]] = 0;
+      islands[(size_t)c] = parts > 1 ? 1 : 0;
+    }
+  }
+  std::vector<int32_t> case_of(S), bus_of(n), unknown(nb);
+  for (int64_t c = 0; c < cases; ++c)
+    for (int64_t j = scenario_ptr[c]; j < scenario_ptr[c + 1]; ++j) case_of[j] = (int32_t)c;
+  for (int64_t i = 0; i < nb; ++i) {
+    unknown[i] = (int32_t)net->unknown[i];
+    if (net->unknown[i] >= 0) bus_of[net->unknown[i]] = (int32_t)i;
+  }
+  cuda_check(cudaSetDevice(net->gpu->device), "cudaSetDevice");
+  cudaStream_t s = net->gpu->stream;
+  auto &w = net->sol;
+  w.case_of.upload(case_of, s), w.bus_of.upload(bus_of, s), w.unknown.upload(unknown, s);
+  w.out_ptr.upload(out_ptr, s), w.out_branch.upload(out_branch.empty() ? std::vector<int32_t>{0} : out_branch, s);
+  w.col_ptr.upload(col_ptr, s);
+  if (S == 0) {
+    if (singular) std::copy(islands.begin(), islands.end(), singular);
+    return;
+  }
+  w.inj.reserve((size_t)(nb * S)), w.rhs.reserve((size_t)(n * S)), w.theta.reserve((size_t)(n * S));
+  w.flags.reserve((size_t)S);
+  if (theta) w.theta_bus.reserve((size_t)(nb * S));
+  if (flows) w.flows.reserve((size_t)(nl * S));
+  cuda_check(cudaMemcpyAsync(w.inj.get(), injections, sizeof(double) * nb * S, cudaMemcpyHostToDevice, s),
+             "upload injections");
+  unknowns_of_buses_kernel<<<(unsigned)((n * S + 255) / 256), 256, 0, s>>>(w.inj.get(), nb, w.bus_of.get(), n, S,
+                                                                          w.rhs.get());
+  cuda_check(cudaGetLastError(), "unknowns_of_buses_kernel launch");
+  int32_t st = yb_solve_many_device(f, w.rhs.get(), n, w.theta.get(), n, S, YB_FP64, s);
+  if (st != YB_OK) throw host::Error(st, "the scenario solve failed");
+  w.singular.upload(islands, s);
+  if (K > 0) {
+    w.pu.upload(pu, s), w.mu.upload(mu, s), w.p0.upload(p0, s), w.p1.upload(p1, s);
+    w.s0.upload(s0, s), w.s1.upload(s1, s), w.invb.upload(invb, s);
+    w.y.reserve((size_t)(n * K));
+    w.lu.reserve((size_t)(cases * kMaxOutageRank * kMaxOutageRank));
+    w.piv.reserve((size_t)(cases * kMaxOutageRank));
+    solve_pairs_device(f, K, w.pu.get(), w.mu.get(), nullptr, nullptr, nullptr, nullptr, w.y.get(), n, s);
+    outage_lu_kernel<<<(unsigned)((cases + 127) / 128), 128, 0, s>>>(w.y.get(), n, w.col_ptr.get(), w.p0.get(),
+                                                                     w.s0.get(), w.p1.get(), w.s1.get(), w.invb.get(),
+                                                                     cases, w.lu.get(), w.piv.get(), w.singular.get());
+    cuda_check(cudaGetLastError(), "outage_lu_kernel launch");
+    outage_update_kernel<<<(unsigned)S, 256, 0, s>>>(w.theta.get(), n, w.case_of.get(), w.col_ptr.get(), w.p0.get(),
+                                                     w.s0.get(), w.p1.get(), w.s1.get(), w.lu.get(), w.piv.get(),
+                                                     w.singular.get(), w.y.get(), n);
+    cuda_check(cudaGetLastError(), "outage_update_kernel launch");
+  }
+  place_flows_kernel<<<(unsigned)S, 256, 0, s>>>(w.theta.get(), n, (int32_t)nb, w.unknown.get(), (int32_t)nl,
+                                                 net->br_u_f.get(), net->br_u_t.get(), net->br_b.get(), w.case_of.get(),
+                                                 w.out_ptr.get(), w.out_branch.get(), theta ? w.theta_bus.get() : nullptr,
+                                                 flows ? w.flows.get() : nullptr, w.flags.get());
+  cuda_check(cudaGetLastError(), "place_flows_kernel launch");
+  if (theta)
+    cuda_check(cudaMemcpyAsync(theta, w.theta_bus.get(), sizeof(double) * nb * S, cudaMemcpyDeviceToHost, s), "download");
+  if (flows)
+    cuda_check(cudaMemcpyAsync(flows, w.flows.get(), sizeof(double) * nl * S, cudaMemcpyDeviceToHost, s), "download");
+  if (flags) cuda_check(cudaMemcpyAsync(flags, w.flags.get(), sizeof(int32_t) * S, cudaMemcpyDeviceToHost, s), "download");
+  if (singular)
+    cuda_check(cudaMemcpyAsync(singular, w.singular.get(), sizeof(int32_t) * cases, cudaMemcpyDeviceToHost, s),
+               "download");
+  cuda_check(cudaStreamSynchronize(s), "DC solutions");
 }
 
 }  // namespace
@@ -298,10 +604,81 @@ extern "C" int32_t yb_dc_ptdf_columns(yb_dc_network *net, int64_t count, const i
     std::vector<int64_t> plus(count), minus(count, -1);
     for (int64_t k = 0; k < count; ++k) {
       require(buses[k] >= 0 && buses[k] < net->n_bus, "a bus is out of range");
-      plus[k] = net->unknown[buses[k]];  // the slack's column is zero
+      plus[k] = net->unknown[buses[k]];  // the slack injects nothing: its column is zero, or -H w
     }
-    const auto flows = pair_flows(net, plus, minus);
+    // with a distributed slack every column loses the shift H w (the operator's offset, -H w)
+    const bool shifted = !net->negated_shift.empty();
+    if (shifted) {
+      const int32_t st = yb_operator_set_offset(net->flows, net->negated_shift.data());
+      if (st != YB_OK) throw host::Error(st, "setting the shift failed");
+    }
+    std::vector<double> flows;
+    try {
+      flows = pair_flows(net, plus, minus);
+    } catch (...) {
+      if (shifted) yb_operator_set_offset(net->flows, std::vector<double>(net->n_branch, 0.0).data());
+      throw;
+    }
+    if (shifted) {
+      const int32_t st = yb_operator_set_offset(net->flows, std::vector<double>(net->n_branch, 0.0).data());
+      if (st != YB_OK) throw host::Error(st, "clearing the shift failed");
+    }
     std::copy(flows.begin(), flows.end(), out);
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_dc_set_slack_weights(yb_dc_network *net, const double *weights) {
+  return guard([&] {
+    check(net);
+    if (!weights) {
+      net->negated_shift.clear();
+      return YB_OK;
+    }
+    // normalized to sum to 1, as DcSensitivity::new does (dc/sensitivity.rs:101-126)
+    double total = 0.0;
+    for (int64_t i = 0; i < net->n_bus; ++i) total += weights[i];
+    require(total != 0.0 && std::isfinite(total), "the weights don't have a finite, nonzero sum");
+    std::vector<double> rhs((size_t)net->n, 0.0);
+    for (int64_t i = 0; i < net->n_bus; ++i)
+      if (net->unknown[i] >= 0) rhs[(size_t)net->unknown[i]] = weights[i] / total;  // the slack's share drops
+    // H w: the flows of the weighted injections (dc/sensitivity.rs:258-263), from one solve
+    std::vector<double> theta((size_t)net->n);
+    const int32_t st = yb_solve_many(net->factor, rhs.data(), 1, theta.data());
+    if (st != YB_OK) throw host::Error(st, "the shift's solve failed");
+    std::vector<double> shift((size_t)net->n_branch);
+    for (int64_t k = 0; k < net->n_branch; ++k) {
+      const int64_t uf = net->unknown[net->from[k]], ut = net->unknown[net->to[k]];
+      const double tf = uf < 0 ? 0.0 : theta[(size_t)uf], tt = ut < 0 ? 0.0 : theta[(size_t)ut];
+      shift[(size_t)k] = -(net->b[k] * (tf - tt));
+    }
+    net->negated_shift = std::move(shift);
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_dc_solve_many(yb_dc_network *net, int64_t count, const double *injections, double *theta,
+                                    double *flows, int32_t *flags) {
+  return guard([&] {
+    check(net);
+    require(count >= 0, "negative count");
+    if (count == 0) return YB_OK;
+    const int64_t sp[2] = {0, count};
+    dc_solutions(net, 1, nullptr, nullptr, sp, injections, theta, flows, flags, nullptr);
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_dc_outage_solutions(yb_dc_network *net, int64_t cases, const int64_t *branch_ptr,
+                                          const int64_t *branches, const int64_t *scenario_ptr,
+                                          const double *injections, double *theta, double *flows, int32_t *flags,
+                                          int32_t *singular) {
+  return guard([&] {
+    check(net);
+    require(cases >= 0, "negative case count");
+    if (cases == 0) return YB_OK;
+    require(branch_ptr != nullptr, "null branch pointers");
+    dc_solutions(net, cases, branch_ptr, branches, scenario_ptr, injections, theta, flows, flags, singular);
     return YB_OK;
   });
 }
@@ -357,7 +734,7 @@ extern "C" int32_t yb_dc_lodf_columns(yb_dc_network *net, int64_t count, const i
 extern "C" int32_t yb_dc_outage_loadings_batch(yb_dc_network *net, int64_t cases, const int64_t *outaged,
                                                const int64_t *scenario_ptr, const double *injections,
                                                const double *weights, int32_t precision, int64_t *max_branch,
-                                               double *max_loading, int32_t *not_finite, int32_t *singular) {
+                                               double *max_loading, int32_t *flags, int32_t *singular) {
   return guard([&] {
     check(net);
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
@@ -366,7 +743,7 @@ extern "C" int32_t yb_dc_outage_loadings_batch(yb_dc_network *net, int64_t cases
     require(scenario_ptr[0] == 0, "scenario pointers must start at 0");
     for (int64_t c = 0; c < cases; ++c) require(scenario_ptr[c + 1] >= scenario_ptr[c], "scenario pointers must not decrease");
     const int64_t S = scenario_ptr[cases];
-    require(S == 0 || (injections && max_branch && max_loading && not_finite), "null output");
+    require(S == 0 || (injections && max_branch && max_loading && flags), "null output");
     yb_factor *f = net->factor;
     const int64_t n = net->n, nl = net->n_branch;
     // per case: the outaged branch's pair over the unknowns, its slots, 1/b
@@ -461,7 +838,7 @@ extern "C" int32_t yb_dc_outage_loadings_batch(yb_dc_network *net, int64_t cases
     std::vector<int32_t> bad(S), sing(cases);
     cuda_check(cudaMemcpyAsync(max_branch, net->d_row.get(), sizeof(int64_t) * S, cudaMemcpyDeviceToHost, s), "download");
     cuda_check(cudaMemcpyAsync(max_loading, net->d_value.get(), sizeof(double) * S, cudaMemcpyDeviceToHost, s), "download");
-    cuda_check(cudaMemcpyAsync(not_finite, net->d_bad.get(), sizeof(int32_t) * S, cudaMemcpyDeviceToHost, s), "download");
+    cuda_check(cudaMemcpyAsync(flags, net->d_bad.get(), sizeof(int32_t) * S, cudaMemcpyDeviceToHost, s), "download");
     cuda_check(cudaMemcpyAsync(sing.data(), net->d_sing.get(), sizeof(int32_t) * cases, cudaMemcpyDeviceToHost, s),
                "download");
     cuda_check(cudaStreamSynchronize(s), "outage screening");

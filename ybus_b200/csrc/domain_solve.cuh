@@ -256,7 +256,7 @@ struct OutageIO {
   const double *__restrict__ br_b, *__restrict__ weight;
   int64_t *__restrict__ out_row;
   double *__restrict__ out_value;
-  int32_t *__restrict__ out_bad;
+  int32_t *__restrict__ out_bad;  // per column: 1 a flow not finite, 2 an angle not finite or above 1e5
   int32_t *__restrict__ case_singular;
 
   template <class T, int W>
@@ -293,10 +293,12 @@ struct OutageIO {
         const int uf = __ldg(br_u_f + l), ut = __ldg(br_u_t + l);
         const double tf = uf < 0 ? 0.0 : __dadd_rn((double)Ys[(size_t)__ldg(br_slot_f + l) * W + cc], __dmul_rn(z, __ldg(y + uf)));
         const double tt = ut < 0 ? 0.0 : __dadd_rn((double)Ys[(size_t)__ldg(br_slot_t + l) * W + cc], __dmul_rn(z, __ldg(y + ut)));
+        // an angle not finite or above 1e5 in magnitude (every unknown is some branch's end)
+        if ((uf >= 0 && !(fabs(tf) <= 1e5)) || (ut >= 0 && !(fabs(tt) <= 1e5))) bad |= 2;
         const double b = __ldg(br_b + l);
         const double f = l == k ? 0.0 : __dadd_rn(__dmul_rn(b, tf), __dmul_rn(-b, tt));
         if (!isfinite(f)) {
-          bad = 1;
+          bad |= 1;
           continue;
         }
         const double load = fabs(f) * __ldg(weight + l);

@@ -11,6 +11,11 @@ from ._lib import lib, ptr
 from .gpu import FP64, Gpu, _check
 
 
+# The flags of a screened or solved scenario
+FLOW_NOT_FINITE = 1  # a branch flow is not finite
+ANGLE_SUSPECT = 2    # an angle is not finite or above 1e5 in magnitude
+
+
 class DcNetwork:
     """B′ and Bf of a network (bus indices `frm`, `to`, reactances `x`, a slack bus), B′ factored
     on the host and uploaded, Bf kept on the device as an operator on the solutions."""
@@ -73,7 +78,8 @@ class DcNetwork:
     def outage_loadings_batch(self, outaged, scenario_ptr, injections, weights=None, precision: int = FP64):
         """N-1 screening: case c takes out branch outaged[c] under the scenarios
         injections[scenario_ptr[c]:scenario_ptr[c+1]] (each a vector over the buses). Returns
-        (branch, loading, not_finite) per scenario and singular per case."""
+        (branch, loading, flags) per scenario (flags: FLOW_NOT_FINITE | ANGLE_SUSPECT bits) and
+        singular per case."""
         outaged = np.ascontiguousarray(outaged, np.int64)
         sp = np.ascontiguousarray(scenario_ptr, np.int64)
         inj = np.ascontiguousarray(injections, np.float64)
@@ -87,7 +93,57 @@ class DcNetwork:
         sing = np.zeros(max(outaged.size, 1), np.int32)
         _check(lib().yb_dc_outage_loadings_batch(self._h, outaged.size, ptr(outaged), ptr(sp), ptr(inj), ptr(w),
                                                  precision, ptr(row), ptr(val), ptr(bad), ptr(sing)))
-        return row[:total], val[:total], bad[:total].astype(bool), sing[: outaged.size].astype(bool)
+        return row[:total], val[:total], bad[:total], sing[: outaged.size].astype(bool)
+
+    def set_slack_weights(self, weights=None) -> None:
+        """A distributed slack for PTDF columns (weights per bus, normalized to sum to 1), or the
+        single slack again (None)."""
+        w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+        if w is not None and w.shape != (self.n_bus,):
+            raise ValueError("one weight per bus")
+        _check(lib().yb_dc_set_slack_weights(self._h, ptr(w)))
+
+    def solve_many(self, injections):
+        """Angles over the buses (slack 0), branch flows and flags per scenario (each row of
+        `injections` a vector over the buses)."""
+        inj = np.ascontiguousarray(np.atleast_2d(injections), np.float64)
+        if inj.shape[1] != self.n_bus:
+            raise ValueError("one injection vector over the buses per scenario")
+        count = inj.shape[0]
+        theta = np.zeros((count, self.n_bus))
+        flows = np.zeros((count, self.n_branch))
+        flags = np.zeros(max(count, 1), np.int32)
+        _check(lib().yb_dc_solve_many(self._h, count, ptr(inj), ptr(theta), ptr(flows), ptr(flags)))
+        return theta, flows, flags[:count]
+
+    def outage_solutions(self, outages, scenario_ptr, injections):
+        """Whole solutions of outages of one or more branches each: case c takes out the branches
+        outages[c] (a sequence) under the scenarios injections[scenario_ptr[c]:scenario_ptr[c+1]].
+        Returns (theta over the buses, flows, flags) per scenario and singular per case."""
+        cases = len(outages)
+        bp = np.zeros(cases + 1, np.int64)
+        for c, rows in enumerate(outages):
+            bp[c + 1] = bp[c] + len(rows)
+        br = np.ascontiguousarray([k for rows in outages for k in rows] or [0], np.int64)
+        sp = np.ascontiguousarray(scenario_ptr, np.int64)
+        inj = np.ascontiguousarray(np.atleast_2d(injections), np.float64)
+        total = int(sp[-1]) if sp.size else 0
+        if inj.shape != (total, self.n_bus):
+            raise ValueError("one injection vector over the buses per scenario")
+        theta = np.zeros((total, self.n_bus))
+        flows = np.zeros((total, self.n_branch))
+        flags = np.zeros(max(total, 1), np.int32)
+        sing = np.zeros(max(cases, 1), np.int32)
+        _check(lib().yb_dc_outage_solutions(self._h, cases, ptr(bp), ptr(br), ptr(sp), ptr(inj), ptr(theta), ptr(flows),
+                                            ptr(flags), ptr(sing)))
+        return theta, flows, flags[:total], sing[:cases].astype(bool)
+
+    def solve_branch_outages(self, injection, branches):
+        """`DcGpuStudy::solve_branch_outages`: each branch taken out alone under one injection
+        vector over the buses. Returns (theta, flows, flags) per branch and singular per branch."""
+        branches = [int(k) for k in branches]
+        inj = np.repeat(np.ascontiguousarray(injection, np.float64)[None, :], len(branches), axis=0)
+        return self.outage_solutions([[k] for k in branches], np.arange(len(branches) + 1), inj)
 
 
 class FlowLoss:
