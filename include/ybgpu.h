@@ -185,6 +185,13 @@ int32_t yb_domain_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t
 /* Waits for the device and reports YB_ERROR_DEVICE_TIMEOUT (clearing it) if a bounded wait in a
  * kernel of this factor ran out since the last check; the host-array calls check by themselves. */
 int32_t yb_factor_check_error(yb_factor *f);
+/* No ybus counterpart, for tests of the device error path without a fault: the next plain lane
+ * solve of this factor (its first launch only) does not issue the copy of page `page` of block 0's
+ * first warp, so that warp's bounded wait (one second) runs out; the warp stops, waits (bounded)
+ * for its copies in flight and takes its block's remaining barriers, and the solve reports
+ * YB_ERROR_DEVICE_TIMEOUT (yb_factor_check_error, or the host-array call itself). -1 withholds
+ * nothing; the setting applies once. */
+int32_t yb_factor_withhold_lane_page(yb_factor *f, int32_t page);
 /* No ybus counterpart, diagnostics: a device buffer of 512 int64 (or NULL to stop) into which block
  * 0 of the streamed or domain solve writes clock64() marks for its first 4 tiles, as
  * [tile][warp < 16][8]. Streamed solve: 0 tile loaded, 1 own records done, 2 all stages done,
@@ -200,6 +207,18 @@ int32_t yb_factor_get_tile(const yb_factor *f, int32_t precision, int32_t *tile_
  * column-major n x count in the caller's order, solutions likewise, in FP64. Pinned (page-locked)
  * caller memory is copied directly; pageable memory goes through a pinned staging buffer. */
 int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count, double *out);
+/* `Lu::solve_transpose` (lu.rs:506-533) for many right-hand sides, host arrays as yb_solve_many:
+ * solves A' x = b with the factor of A. An LU factor makes the factor of A' = Q U' L' P from its
+ * arrays at the first call and keeps it (yb_factor_from_lu_transposed's); a Cholesky factor solves
+ * as yb_solve_many (A' = A). */
+int32_t yb_solve_many_transpose(yb_factor *f, const double *rhs, int64_t count, double *out);
+/* No ybus counterpart (ybus_sparse's `Cholesky::solve_refined` / `refine_normwise`, accuracy.rs:
+ * 83-205, on the CPU): yb_solve_many_refined_device with host arrays, FP32 substitution and FP64
+ * refinement against the attached matrix (yb_factor_attach_matrix), in blocks of at most the block
+ * width; steps and ratio (either may be NULL) receive each column's corrections and relative
+ * residual ||b - A x||inf / ||b||inf. */
+int32_t yb_solve_many_mixed(yb_factor *f, const double *rhs, int64_t count, double *out, int32_t max_steps,
+                            double tolerance, int32_t *steps, double *ratio);
 /* The same solve on device arrays (leading dimensions ldb, ldx >= n) on `stream` (a
  * cudaStream_t, NULL for the GPU's own), asynchronous, in YB_FP64 or YB_FP32 substitution. */
 int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,

@@ -302,3 +302,37 @@ def test_the_cusparse_comparison_solves_the_same(gpu):
         ms = compare.spsm_solve(chol, b.data_ptr(), x.data_ptr(), 70, width)
         assert ms > 0
         assert worst_relative_difference(x.cpu().numpy(), cpu) < BAR, f"width {width}"
+
+
+@pytest.mark.parametrize("seed", [3, 8])
+def test_host_array_transposed_solve(gpu, seed):
+    # Lu::solve_transpose (lu.rs:506-533) through yb_solve_many_transpose: the factor of A' made
+    # from the LU factor's arrays at the first call, then kept; a Cholesky factor solves as itself
+    a = random_square(250, 4, seed)
+    lu = host.lu(a)
+    factor = GpuFactor.from_lu(gpu, lu)
+    rhs = right_hand_sides(250, 30, seed)
+    cpu = orc.solve_many_lu(lu, rhs, transpose=True)
+    for _ in range(2):
+        assert worst_relative_difference(factor.solve_many_transpose(rhs), cpu) < 1e-12
+    assert worst_relative_difference(factor.solve_many(rhs), orc.solve_many_lu(lu, rhs)) < 1e-12
+    chol = host.cholesky(random_spd(120, 5, seed))
+    cf = GpuFactor.from_cholesky(gpu, chol)
+    r2 = right_hand_sides(120, 9, seed)
+    assert np.array_equal(cf.solve_many_transpose(r2), cf.solve_many(r2))
+
+
+def test_host_array_refined_solve(gpu):
+    # yb_solve_many_mixed: FP32 substitution and FP64 refinement with host arrays, to the tolerance
+    a = random_spd(400, 3, 5)
+    chol = host.cholesky(a)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.attach_matrix(a)
+    factor.set_block_width(16)  # several blocks
+    rhs = right_hand_sides(400, 50, 9)
+    x, steps, ratio = factor.solve_many_mixed(rhs, 4, 1e-10)
+    p, i, v = a.to_csr().arrays()
+    oracle_ratio = np.array([orc.relative_residual(p, i, v, x[k], rhs[k]) for k in range(50)])
+    assert ratio.max() <= 1e-10 and oracle_ratio.max() <= 1.05e-10
+    assert (steps >= 1).all() and (steps <= 4).all()
+    assert worst_relative_difference(x, orc.solve_many(chol, rhs)) < 1e-8

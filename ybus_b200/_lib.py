@@ -81,6 +81,7 @@ SIGNATURES: dict[str, tuple] = {
     "yb_factor_set_tile_kind": (i32, [vp, i32, i32]),
     "yb_factor_set_stream": (i32, [vp, i32, i32, i32, i32, i32]),
     "yb_factor_stream_info": (i32, [vp, i32, P_i32, P_i32, P_i64, P_i64, P_i32, P_i32, P_i32]),
+    "yb_factor_withhold_lane_page": (i32, [vp, i32]),
     "yb_factor_check_error": (i32, [vp]),
     "yb_factor_set_phase_clock": (i32, [vp, vp]),
     "yb_factor_set_tail_level": (i32, [vp, i32, i32]),
@@ -97,6 +98,8 @@ SIGNATURES: dict[str, tuple] = {
     "yb_domain_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp, vp]),
     "yb_lane_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp, vp]),
     "yb_solve_many": (i32, [vp, vp, i64, vp]),
+    "yb_solve_many_transpose": (i32, [vp, vp, i64, vp]),
+    "yb_solve_many_mixed": (i32, [vp, vp, i64, vp, i32, dbl, vp, vp]),
     "yb_solve_many_device": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
     "yb_solve_many_device_noalloc": (i32, [vp, vp, i64, vp, i64, i64, i32, vp]),
     "yb_factor_attach_matrix": (i32, [vp, vp, vp, vp]),

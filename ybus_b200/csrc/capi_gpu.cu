@@ -194,6 +194,20 @@ extern "C" int32_t yb_factor_from_cholesky(yb_gpu *gpu, int64_t n, const int64_t
   });
 }
 
+namespace {
+// Keeps an LU factor's arrays in the factor, for yb_solve_many_transpose.
+void keep_lu_arrays(yb_factor *f, int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
+                    const int64_t *u_ptr, const int64_t *u_idx, const double *u_val, const int64_t *row_perm,
+                    const int64_t *col_perm, bool transposed) {
+  if (n == 0) return;
+  const int64_t ln = l_ptr[n], un = u_ptr[n];
+  f->lu_l_ptr.assign(l_ptr, l_ptr + n + 1), f->lu_l_idx.assign(l_idx, l_idx + ln), f->lu_l_val.assign(l_val, l_val + ln);
+  f->lu_u_ptr.assign(u_ptr, u_ptr + n + 1), f->lu_u_idx.assign(u_idx, u_idx + un), f->lu_u_val.assign(u_val, u_val + un);
+  f->lu_p.assign(row_perm, row_perm + n), f->lu_q.assign(col_perm, col_perm + n);
+  f->has_lu_arrays = true, f->lu_transposed = transposed;
+}
+}  // namespace
+
 extern "C" int32_t yb_factor_from_lu(yb_gpu *gpu, int64_t n, const int64_t *l_ptr, const int64_t *l_idx,
                                      const double *l_val, const int64_t *u_ptr, const int64_t *u_idx,
                                      const double *u_val, const int64_t *row_perm, const int64_t *col_perm,
@@ -207,7 +221,9 @@ extern "C" int32_t yb_factor_from_lu(yb_gpu *gpu, int64_t n, const int64_t *l_pt
     auto lower = host::reorient(l_csc);
     auto upper = host::reorient(u_csc);
     std::vector<int64_t> p(row_perm, row_perm + n), q(col_perm, col_perm + n);
-    *out = make_factor(gpu, n, std::move(lower), true, std::move(upper), p, q, YB_LU);
+    yb_factor *f = make_factor(gpu, n, std::move(lower), true, std::move(upper), p, q, YB_LU);
+    keep_lu_arrays(f, n, l_ptr, l_idx, l_val, u_ptr, u_idx, u_val, row_perm, col_perm, false);
+    *out = f;
     return YB_OK;
   });
 }
@@ -226,7 +242,9 @@ extern "C" int32_t yb_factor_from_lu_transposed(yb_gpu *gpu, int64_t n, const in
     auto lower = csr_from_arrays(n, u_ptr, u_idx, u_val, true);
     auto upper = csr_from_arrays(n, l_ptr, l_idx, l_val, true);
     std::vector<int64_t> p(row_perm, row_perm + n), q(col_perm, col_perm + n);
-    *out = make_factor(gpu, n, std::move(lower), false, std::move(upper), q, p, YB_LU);
+    yb_factor *f = make_factor(gpu, n, std::move(lower), false, std::move(upper), q, p, YB_LU);
+    keep_lu_arrays(f, n, l_ptr, l_idx, l_val, u_ptr, u_idx, u_val, row_perm, col_perm, true);
+    *out = f;
     return YB_OK;
   });
 }
@@ -387,8 +405,17 @@ extern "C" int32_t yb_factor_check_error(yb_factor *f) {
     cuda_check(cudaMemcpy(&word, f->error.get(), sizeof word, cudaMemcpyDeviceToHost), "read error word");
     if (word != 0) {
       cuda_check(cudaMemset(f->error.get(), 0, sizeof word), "clear error word");
-      throw host::Error(host::kDeviceTimeout, "a bounded device wait ran out in the streamed solve");
+      throw host::Error(host::kDeviceTimeout, "a bounded device wait ran out in a solve of this factor");
     }
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_withhold_lane_page(yb_factor *f, int32_t page) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(page >= -1, "page must be -1 or a page index");
+    f->lane_withhold = page;
     return YB_OK;
   });
 }
@@ -757,6 +784,8 @@ void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, doub
   a.blob = d->blob.get();
   a.warp_page = d->warp_page.get();
   a.error = f->error.get();
+  a.withhold = f->lane_withhold;  // a test's withheld page: this call's first launch only
+  f->lane_withhold = -1;
   for (int64_t g0 = 0; g0 < groups_all; g0 += per_launch) {
     const int64_t groups = std::min(per_launch, groups_all - g0);
     const int64_t cols = std::min(count - g0 * 32, groups * 32);
@@ -769,6 +798,7 @@ void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, doub
     if (ev) cuda_check(cudaEventRecord(ev[1], stream), "cudaEventRecord");
     lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
     cuda_check(cudaGetLastError(), "lane_solve_kernel launch");
+    a.withhold = -1;
     if (ev) cuda_check(cudaEventRecord(ev[2], stream), "cudaEventRecord");
     lane_out_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(work, cols, (int32_t)n, groups, d->out_pos.get(), x + g0 * 32 * ldx, ldx);
     cuda_check(cudaGetLastError(), "lane_out_kernel launch");
@@ -948,6 +978,64 @@ template void launch_domain_fp64<BusIO>(yb_factor *, int64_t, const BusIO &, cud
 template void launch_domain_fp64<AdjointIO>(yb_factor *, int64_t, const AdjointIO &, cudaStream_t);
 
 }  // namespace yb
+
+extern "C" int32_t yb_solve_many_transpose(yb_factor *f, const double *rhs, int64_t count, double *out) {
+  return guard([&]() -> int32_t {
+    require(f != nullptr, "null factor");
+    require(!f->is_complex, "a complex factor solves with yb_solve_batch_complex");
+    if (f->kind != YB_LU) return yb_solve_many(f, rhs, count, out);  // a Cholesky factor: A' = A
+    require(f->has_lu_arrays || f->n <= 1, "the factor keeps no LU arrays to transpose");
+    if (f->n <= 1) return yb_solve_many(f, rhs, count, out);  // a single row: its own transpose
+    if (!f->transposed) {
+      yb_factor *t = nullptr;
+      auto make = f->lu_transposed ? yb_factor_from_lu : yb_factor_from_lu_transposed;
+      const int32_t st = make(f->gpu, f->n, f->lu_l_ptr.data(), f->lu_l_idx.data(), f->lu_l_val.data(),
+                              f->lu_u_ptr.data(), f->lu_u_idx.data(), f->lu_u_val.data(), f->lu_p.data(),
+                              f->lu_q.data(), &t);
+      if (st != YB_OK) throw host::Error(st, "making the transposed factor failed");
+      f->transposed.reset(t);
+    }
+    f->transposed->width = f->width;
+    const int32_t st = yb_solve_many(f->transposed.get(), rhs, count, out);
+    if (st != YB_OK) throw host::Error(st, "the transposed solve failed");
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_solve_many_mixed(yb_factor *f, const double *rhs, int64_t count, double *out, int32_t max_steps,
+                                       double tolerance, int32_t *steps, double *ratio) {
+  return guard([&]() -> int32_t {
+    require(f != nullptr, "null factor");
+    require(count >= 0, "negative count");
+    const int64_t n = f->n;
+    if (n == 0 || count == 0) return YB_OK;
+    require(rhs && out, "null array");
+    cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
+    cudaStream_t s = f->gpu->stream;
+    // blocks of at most the block width and of at most 1 GiB of right-hand sides
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>({count, f->width, (int64_t)((size_t(1) << 30) / (8 * n))}));
+    f->mixed_b.reserve((size_t)(n * chunk)), f->mixed_x.reserve((size_t)(n * chunk));
+    f->mixed_ratio.reserve((size_t)chunk), f->mixed_steps.reserve((size_t)chunk);
+    for (int64_t k0 = 0; k0 < count; k0 += chunk) {
+      const int64_t c = std::min(chunk, count - k0);
+      cuda_check(cudaMemcpyAsync(f->mixed_b.get(), rhs + k0 * n, sizeof(double) * n * c, cudaMemcpyHostToDevice, s),
+                 "upload");
+      const int32_t st = yb_solve_many_refined_device(f, f->mixed_b.get(), n, f->mixed_x.get(), n, c, max_steps,
+                                                      tolerance, f->mixed_ratio.get(), f->mixed_steps.get(), s);
+      if (st != YB_OK) throw host::Error(st, "the refined solve failed");
+      cuda_check(cudaMemcpyAsync(out + k0 * n, f->mixed_x.get(), sizeof(double) * n * c, cudaMemcpyDeviceToHost, s),
+                 "download");
+      if (ratio)
+        cuda_check(cudaMemcpyAsync(ratio + k0, f->mixed_ratio.get(), sizeof(double) * c, cudaMemcpyDeviceToHost, s),
+                   "download");
+      if (steps)
+        cuda_check(cudaMemcpyAsync(steps + k0, f->mixed_steps.get(), sizeof(int32_t) * c, cudaMemcpyDeviceToHost, s),
+                   "download");
+      cuda_check(cudaStreamSynchronize(s), "refined solve");
+    }
+    return yb_factor_check_error(f);
+  });
+}
 
 extern "C" int32_t yb_solve_many_device(yb_factor *f, const double *d_rhs, int64_t ldb, double *d_out, int64_t ldx,
                                         int64_t count, int32_t precision, void *stream) {
@@ -1364,6 +1452,7 @@ void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t l
   a.warp_page = d->warp_page.get();
   a.error = f->error.get();
   a.group_active = r.active;
+  a.withhold = -1;
   auto check = [](const char *what) { cuda_check(cudaGetLastError(), what); };
   for (int64_t g0 = 0; g0 < groups_all; g0 += per_launch) {
     const int64_t groups = std::min(per_launch, groups_all - g0);

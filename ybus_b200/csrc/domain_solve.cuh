@@ -904,11 +904,7 @@ __global__ void __launch_bounds__(512, 1) domain_tile_kernel(DomainArgs a, IO io
   // Every copy issued but not consumed (the S run ahead, or more after a wait that ran out) is
   // waited for, bounded, before the block's shared memory is released
   if (lane == 0 && streaming) {
-    for (int64_t kk = consumed; kk < issued; ++kk) {
-      long tries = 0;
-      while (!mbar_try_wait(full + (kk % S), (uint32_t)((kk / S) & 1)) && ++tries < kWaitLimit) {
-      }
-    }
+    for (int64_t kk = consumed; kk < issued; ++kk) mbar_wait_bounded(full + (kk % S), (uint32_t)((kk / S) & 1), nullptr);
   }
 }
 

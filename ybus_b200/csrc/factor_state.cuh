@@ -183,6 +183,7 @@ struct yb_factor {
   yb::DeviceArray<uint8_t> lane_work, lane_partial;  // the lane solve's work and partial arrays
   yb::LaneTiming lane_timing;
   yb::DeviceArray<int32_t> error;  // the device error word (a bounded wait that ran out)
+  int32_t lane_withhold = -1;      // a test's page to withhold in the next plain lane solve, or -1
   long long *phase_clock = nullptr;  // diagnostics buffer of the caller's, or null
   yb::DeviceArray<double> scratch64;
   yb::DeviceArray<float> scratch32;
@@ -211,6 +212,15 @@ struct yb_factor {
   yb::DeviceArray<yb::cplx<double>> za_val;
   yb::PinnedBuffer staging;
   yb::CopyPipeline pipe;
+  // an LU factor's arrays as given (yb_factor_from_lu or _transposed), from which the transposed
+  // solve makes the factor of the transposed matrix at its first use
+  bool has_lu_arrays = false, lu_transposed = false;
+  std::vector<int64_t> lu_l_ptr, lu_l_idx, lu_u_ptr, lu_u_idx, lu_p, lu_q;
+  std::vector<double> lu_l_val, lu_u_val;
+  std::unique_ptr<yb_factor> transposed;
+  // the host-array refined solve's device arrays
+  yb::DeviceArray<double> mixed_b, mixed_x, mixed_ratio;
+  yb::DeviceArray<int32_t> mixed_steps;
   int64_t width = 1;
   yb::Timings timings;
   bool single = false;

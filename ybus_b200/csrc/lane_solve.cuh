@@ -40,6 +40,8 @@ struct LaneArgs {
   const uint8_t *group_active;            // [groups] 0: the group is skipped; null: every group runs
   void *xout;  // null: the solutions overwrite the work array; else an array of the work array's layout
                // that receives them (the backward rows' results and the top solutions the domains read)
+  int32_t withhold;  // for tests of the error path: the page of block 0's first warp whose copy is never
+                     // issued, so that warp's bounded wait runs out (-1: none)
 };
 
 // A warp's shared memory: live slots, the prefetch ring, the page ring and its barriers.
@@ -157,15 +159,18 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
     mbar_fence_init();
   }
   __syncwarp();
+  // the page a test withholds from this warp, or -1
+  const int withheld = (blockIdx.x == 0 && warp == 0) ? a.withhold : -1;
   if (lane == 0)
     for (int s = 0; s < S && s < np; ++s)
-      bulk_page(lane_shared + ring + s * PB, stream + (size_t)s * PB, (uint32_t)PB, full + s);
+      if (s != withheld) bulk_page(lane_shared + ring + s * PB, stream + (size_t)s * PB, (uint32_t)PB, full + s);
   int issued = min(S, np);
   __syncwarp();
 
   int k = 0;               // the page being read
   uint32_t page = ring;    // the record being read
-  bool ok = np > 0 && mbar_wait_bounded(full, 0, a.error);
+  // every lane waits; the warp goes on only if all of them saw the page
+  bool ok = __all_sync(0xffffffffu, np > 0 && mbar_wait_bounded(full, 0, a.error));
   bool ended = false;
   int barriers = 0;
   T z = T(0);  // the forward row's result, or the backward row's running sum
@@ -323,14 +328,14 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
       case kLanePageEnd: {  // the finished page's slot takes page k + S
         __syncwarp();
         if (k + S < np) {
-          if (lane == 0) {
+          if (lane == 0 && k + S != withheld) {
             fence_proxy_async();
             bulk_page(lane_shared + ring + (k % S) * PB, stream + (size_t)(k + S) * PB, (uint32_t)PB, full + k % S);
           }
           issued = k + S + 1;
         }
         ++k;
-        ok = k < np && mbar_wait_bounded(full + k % S, (uint32_t)((k / S) & 1), a.error);
+        ok = __all_sync(0xffffffffu, k < np && mbar_wait_bounded(full + k % S, (uint32_t)((k / S) & 1), a.error));
         page = ring + (uint32_t)(k % S) * PB;
         if (ok) hn = lane_at<uint4>(page);
         continue;

@@ -47,7 +47,16 @@ struct StreamArgs {
   long long *phase_clock;
 };
 
-constexpr long kWaitLimit = 1L << 24;
+// How long a kernel waits for a copy before it gives up, records the failure and returns: one
+// second of the GPU's global timer, far beyond any copy's latency, short enough that a copy that
+// never lands costs a launch a second or two and leaves the context usable.
+constexpr unsigned long long kWaitLimitNs = 1000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -77,13 +86,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Waits for a slot's copy; gives up after kWaitLimit tries, recording the failure. Returns
-// whether the copy completed.
+// Waits for a slot's copy; gives up after kWaitLimitNs, recording the failure in *error (if not
+// null). Returns whether the copy completed. The timer is read only once a first try has failed.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int32_t *error) {
-  long tries = 0;
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (++tries >= kWaitLimit) {
-      atomicExch(error, 1);
+    if (global_ns() - t0 > kWaitLimitNs) {
+      if (error) atomicExch(error, 1);
       return false;
     }
   }
@@ -338,11 +348,7 @@ __global__ void __launch_bounds__(512) stream_tile_kernel(StreamArgs a) {
   // last copy into each slot before the block's shared memory is released
   if (lane == 0 && total_pages > 0) {
     const int64_t first = total_pages > S ? total_pages - S : 0;
-    for (int64_t kk = first; kk < total_pages; ++kk) {
-      long tries = 0;
-      while (!mbar_try_wait(full + (kk % S), (uint32_t)((kk / S) & 1)) && ++tries < kWaitLimit) {
-      }
-    }
+    for (int64_t kk = first; kk < total_pages; ++kk) mbar_wait_bounded(full + (kk % S), (uint32_t)((kk / S) & 1), nullptr);
   }
 }
 

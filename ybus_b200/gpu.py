@@ -313,6 +313,30 @@ class GpuFactor:
         _check(lib().yb_solve_many(self._h, ptr(b), b.shape[0], ptr(out)))
         return out
 
+    def solve_many_transpose(self, rhs) -> np.ndarray:
+        """Solves A' x = b for each right-hand side (`Lu::solve_transpose`, lu.rs:506-533)."""
+        n = self.dim()
+        b = _rhs_array(rhs, n)
+        out = np.empty_like(b)
+        if b.shape[0] == 0 or n == 0:
+            return out
+        _check(lib().yb_solve_many_transpose(self._h, ptr(b), b.shape[0], ptr(out)))
+        return out
+
+    def solve_many_mixed(self, rhs, max_steps: int = 3, tolerance: float = 1e-10):
+        """FP32 substitution with FP64 refinement against the attached matrix, host arrays in and
+        out: returns (x, corrections per column, relative residual per column)."""
+        n = self.dim()
+        b = _rhs_array(rhs, n)
+        out = np.empty_like(b)
+        steps = np.zeros(b.shape[0], np.int32)
+        ratio = np.zeros(b.shape[0])
+        if b.shape[0] == 0 or n == 0:
+            return out, steps, ratio
+        _check(lib().yb_solve_many_mixed(self._h, ptr(b), b.shape[0], ptr(out), max_steps, tolerance, ptr(steps),
+                                         ptr(ratio)))
+        return out, steps, ratio
+
     def solve_many_into(self, b: np.ndarray, out: np.ndarray) -> None:
         """`solve_many` into a caller's (count, n) buffer (pinned buffers are copied directly)."""
         _check(lib().yb_solve_many(self._h, b.ctypes.data, b.shape[0], out.ctypes.data))
