@@ -1,6 +1,8 @@
-"""The multi-process path of the solve (one process per GPU, no data-path exchange), on the CPU:
-two gloo ranks meet at a barrier, agree on the slowest rank's time, and split independent units
-(right-hand sides, outage cases, networks) into shares that cover every unit once."""
+"""The multi-process path of the solve (one process per GPU, no data-path exchange but the
+adjoint's), on the CPU: two gloo ranks meet at a barrier, agree on the slowest rank's time, and
+split independent units (right-hand sides, outage cases by LPT, networks) into shares that cover
+every unit once; ranks that split the adjoint's scenarios reduce dL/db and the loss in rank order
+to the single process's gradient, every rank with the same bits."""
 import os
 import socket
 
@@ -65,3 +67,76 @@ def test_one_process_needs_no_group():
     assert replicas.max_over_ranks(3.5) == 3.5
     replicas.barrier()
     assert replicas.whole_job_rate(13499, 4, 2.0) == 13499 * 4 / 2.0
+
+
+def _adjoint_rank(rank: int, world: int, port: int, out) -> None:
+    # the sharded adjoint on the CPU: this rank's scenarios through the oracle's gradient, then the
+    # one exchange of the path, dL/db and the loss summed over the ranks in rank order
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    import oracle.oracle as orc
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        g, p, limits, chol, position = _adjoint_case()
+        mine = replicas.shard(p.shape[0], rank, world)
+        loss, gp, gb = orc.flow_loss_and_gradient(chol, g.n_bus, g.frm, g.to, g.susceptance, position,
+                                                  p[mine.start:mine.stop], limits)
+        total = replicas.sum_in_rank_order(np.append(gb, loss))
+        out.put((rank, mine.start, mine.stop, gp, total))
+    finally:
+        dist.destroy_process_group()
+
+
+def _adjoint_case():
+    import numpy as np
+
+    from dc_cases import cpu_model
+    from ybus_b200 import grids
+    g = grids.make_grid(300, 100, grids.SEED_BASE + 7)
+    _, chol, position = cpu_model(g)
+    rng = np.random.default_rng(8)
+    p = rng.normal(0.0, 0.1, (37, g.n_bus))
+    p[:, 0] = -p[:, 1:].sum(axis=1)
+    limits = rng.uniform(0.5, 2.0, g.n_branch)
+    return g, p, limits, chol, position
+
+
+def test_sharded_adjoint_gradients_reduce_to_the_single_process_gradient():
+    import numpy as np
+
+    import oracle.oracle as orc
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_adjoint_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = sorted((out.get(timeout=180) for _ in procs), key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    g, p, limits, chol, position = _adjoint_case()
+    loss, gp, gb = orc.flow_loss_and_gradient(chol, g.n_bus, g.frm, g.to, g.susceptance, position, p, limits)
+    # every rank holds the same bits of the reduced dL/db and loss (summed in rank order)
+    assert np.array_equal(results[0][4], results[1][4])
+    total = results[0][4]
+    assert np.abs(total[:-1] - gb).max() <= 1e-12 * np.abs(gb).max()
+    assert abs(total[-1] - loss) <= 1e-12 * abs(loss)
+    # dL/dp needs no exchange: each rank's rows are the single process's rows, bit for bit
+    for rank, start, stop, gp_rank, _ in results:
+        assert np.array_equal(gp_rank, gp[start:stop]), rank
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_lpt_covers_every_unit_once_and_balances(world):
+    import numpy as np
+    w = np.random.default_rng(9).integers(1, 65, 2000)  # outage cases weighted by scenario counts
+    share = replicas.lpt(w, world)
+    assert sorted(u for s in share for u in s) == list(range(w.size))
+    loads = [int(w[s].sum()) for s in share]
+    assert max(loads) - min(loads) <= w.max()  # LPT's bound: within one unit's weight
