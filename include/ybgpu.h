@@ -102,7 +102,7 @@ int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int32_t kind);
  * parallel under a top warp 0 takes, a few tens of live values per lane in shared memory; b, the
  * forward results and x streaming through a work array in HBM). info receives 12 values: {slots,
  * pages, page bytes, forward peak of live values, backward peak, entries of both sweeps, shared
- * memory per block, warps per block, domains, top rows, partial values per block, 0};
+ * memory per block, warps per block, domains, top rows, partial values per block, right-hand sides per lane};
  * YB_ERROR_INVALID_ARGUMENT if the factor admits no lane layout (no postorder serves both sweeps,
  * or too many live values). */
 int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t *info);
@@ -110,6 +110,11 @@ int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t *info);
  * and page bytes (256..16384, a multiple of 16; default 0: the largest of 2048, 1024, 768, 512 with
  * which three blocks fit an SM). */
 int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32_t page_bytes);
+/* No ybus counterpart: how many right-hand sides each lane of the plain lane solve carries, 1 or 2
+ * (a block then solves 32 or 64 right-hand sides; with two, each decoded record serves twice the
+ * arithmetic, and two blocks share an SM instead of three). The refined solve's lane passes keep
+ * one. yb_factor_lane_info reports it (its last value). */
+int32_t yb_factor_set_lane_rhs_per_lane(yb_factor *f, int32_t precision, int32_t rhs_per_lane);
 /* No ybus counterpart: the number of right-hand sides from which the automatic choice takes the
  * lane solve (default 3072). */
 int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t min_count);
@@ -164,14 +169,15 @@ int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_t *tile_wid
 int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t count, int32_t *config, double *best_ms);
 /* No ybus counterpart, diagnostics on the host (no GPU needed): the lane solve's layout for a
  * Cholesky factor given as to yb_factor_from_cholesky, values of `value_bytes` (8 or 4), `warps`
- * warps per block. info receives 12 values: {slots, pages, page bytes, forward peak of live
- * values, backward peak, forward entries, backward entries, warps, domains, top rows, partial
- * values per block, 0}; blob (pages * page_bytes bytes), warp_page (warps + 1), in_pos and out_pos
- * (n each: the work-array position of each row of b and of x) may be NULL. */
+ * warps per block, `rhs_per_lane` (1 or 2) right-hand sides per lane. info receives 12 values:
+ * {slots, pages, page bytes, forward peak of live values, backward peak, forward entries, backward
+ * entries, warps, domains, top rows, partial values per block, right-hand sides per lane}; blob
+ * (pages * page_bytes bytes), warp_page (warps + 1), in_pos and out_pos (n each: the work-array
+ * position of each row of b and of x) may be NULL. */
 int32_t yb_lane_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
                                 const int64_t *perm, int32_t value_bytes, int32_t page_bytes, int32_t max_slots,
-                                int32_t warps, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *in_pos,
-                                int32_t *out_pos);
+                                int32_t warps, int32_t rhs_per_lane, int64_t *info, uint8_t *blob, int32_t *warp_page,
+                                int32_t *in_pos, int32_t *out_pos);
 /* No ybus counterpart, diagnostics on the host (no GPU needed): the domain layout a Cholesky factor
  * given as to yb_factor_from_cholesky gets for `value_bytes` (8 or 4). info receives {cut, top
  * rows, stages, warps, pages, records, entries, page bytes}, top_condition the worse infinity-norm

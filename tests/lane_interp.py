@@ -42,7 +42,7 @@ def warp_steps(lay, warp, work, partial, lanes):
     """Runs one warp's records, yielding at each block barrier."""
     vb = lay["value_bytes"]
     ftype = np.float64 if vb == 8 else np.float32
-    row = 32 * vb
+    row = 32 * vb * lay.get("rpl", 1)  # a slot or row: 32 lanes of rpl values
     live = np.zeros((lay["slots"], lanes))
     ring = np.full((RING, lanes), np.nan)
     pending = np.zeros(RING, bool)  # a prefetched row not read yet

@@ -191,3 +191,64 @@ def test_lane_launch_times_are_recorded_when_asked(gpu):
     factor.solve_many(rhs)
     assert factor.lane_times()["launches"] == 0
     assert worst_relative_difference(x, orc.solve_many(chol, rhs)) < BAR
+
+
+# ---- two right-hand sides per lane (64 per block) --------------------------------------------------
+
+@pytest.mark.parametrize("warps", [1, 3, 8])
+@pytest.mark.parametrize("count", [1, 63, 64, 65, 200])
+@pytest.mark.parametrize("prec,bar", [(FP64, BAR), (FP32, 1e-4)])
+def test_two_per_lane_matches_the_cpu(gpu, count, warps, prec, bar):
+    chol = host.cholesky(random_spd(200, 3, 7))
+    rhs = right_hand_sides(200, count, 11)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    factor.set_tile_kind(prec, LANE)
+    factor.set_lane(prec, warps)
+    factor.set_lane_rhs_per_lane(prec, 2)
+    assert factor.lane_info(prec)["rpl"] == 2
+    d = worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs))
+    assert d < bar, f"count {count} warps {warps}: {d:e}"
+    factor.check_error()
+
+
+@pytest.mark.parametrize("page", [256, 512])
+def test_two_per_lane_with_records_split_over_pages(gpu, page):
+    # dense columns and a star's top row: records and partial sums over several records
+    for chol in (host.cholesky(random_spd(150, 30, 7)), host.cholesky(star_spd(200))):
+        rhs = right_hand_sides(chol.n, 90, 3)
+        factor = GpuFactor.from_cholesky(gpu, chol)
+        factor.set_tile_kind(FP64, LANE)
+        factor.set_lane(FP64, 8, page)
+        factor.set_lane_rhs_per_lane(FP64, 2)
+        d = worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs))
+        assert d < BAR, f"{d:e}"
+        factor.check_error()
+
+
+def test_two_per_lane_on_the_10k_grid_and_the_same_bits_as_one(gpu):
+    # the full 13,499-column PTDF block with the automatic layout for two per lane, against the
+    # oracle on sampled columns; and on one layout (8 warps, 512-byte pages) for both, column for
+    # column the same bits as one right-hand side per lane (the same operations in the same order;
+    # layouts of other warp counts cut other domains and sum in another order)
+    import torch
+    from ybus_b200 import configs
+    g = configs.grid_10k()
+    chol = host.cholesky(configs.bprime(g))
+    rhs = configs.branch_rhs(g)
+    factor = GpuFactor.from_cholesky(gpu, chol)
+    b = torch.from_numpy(rhs).cuda()
+    x1, x2 = torch.empty_like(b), torch.empty_like(b)
+    factor.set_tile_kind(FP64, LANE)
+    factor.set_lane_rhs_per_lane(FP64, 2)
+    factor.solve_many_device(b.data_ptr(), x2.data_ptr(), rhs.shape[0], FP64, None)
+    gpu.synchronize()
+    factor.check_error()
+    sample = np.arange(0, rhs.shape[0], 211)
+    assert worst_relative_difference(x2.cpu().numpy()[sample], orc.solve_many(chol, rhs[sample], threads=8)) < BAR
+    factor.set_lane(FP64, 8, 512)
+    factor.solve_many_device(b.data_ptr(), x2.data_ptr(), rhs.shape[0], FP64, None)
+    factor.set_lane_rhs_per_lane(FP64, 1)
+    factor.solve_many_device(b.data_ptr(), x1.data_ptr(), rhs.shape[0], FP64, None)
+    gpu.synchronize()
+    factor.check_error()
+    assert np.array_equal(x1.cpu().numpy(), x2.cpu().numpy())

@@ -75,3 +75,21 @@ def test_a_top_row_with_more_partials_than_a_record_holds():
     lay = host.lane_layout(chol, 8, 256, warps=8)
     assert lay["top"] >= 1 and lay["partials"] > 14
     assert worst_relative_difference(run(lay, 200, rhs), orc.solve_many(chol, rhs)) < 1e-12
+
+
+@pytest.mark.parametrize("value_bytes,warps,page", [(8, 8, 512), (8, 3, 2048), (4, 8, 1024)])
+def test_two_right_hand_sides_per_lane_scale_only_the_offsets(value_bytes, warps, page):
+    # with two right-hand sides per lane a slot or row holds 64 values: the same records, in the same
+    # pages, with every byte offset doubled; they still solve through the interpreter
+    chol = grid_factor(2000, 700, grids.SEED_BASE + 1)
+    one = host.lane_layout(chol, value_bytes, page, warps=warps, rpl=1)
+    two = host.lane_layout(chol, value_bytes, page, warps=warps, rpl=2)
+    assert two["rpl"] == 2 and one["rpl"] == 1
+    for key in ("slots", "pages", "domains", "top", "partials", "fwd_entries", "bwd_entries"):
+        assert one[key] == two[key], key
+    assert np.array_equal(one["warp_page"], two["warp_page"])
+    assert np.array_equal(one["in_pos"], two["in_pos"]) and np.array_equal(one["out_pos"], two["out_pos"])
+    rhs = np.random.default_rng(5).standard_normal((3, chol.n))
+    bar = 1e-12 if value_bytes == 8 else 1e-4
+    assert worst_relative_difference(run(two, chol.n, rhs), orc.solve_many(chol, rhs)) < bar
+    assert not np.array_equal(one["blob"], two["blob"])

@@ -720,14 +720,15 @@ void launch_domain(yb_factor *f, const TileConfig &cfg, int64_t count, const IO 
 constexpr int32_t kLaneMaxSlots = 256, kLaneAutoSlots = 64;
 constexpr size_t kLaneWorkBytes = size_t(2) << 30;
 
-template <class T> DeviceLane *lane_for(yb_factor *f, int warps, int page_bytes, cudaStream_t stream) {
-  const auto key = std::make_tuple((int)sizeof(T), warps, page_bytes);
+template <class T> DeviceLane *lane_for(yb_factor *f, int warps, int page_bytes, int rpl, cudaStream_t stream) {
+  const auto key = std::make_tuple((int)sizeof(T), warps, page_bytes, rpl);
   auto it = f->lanes.find(key);
   if (it != f->lanes.end()) return it->second.get();
   std::unique_ptr<DeviceLane> d;
   try {
-    const LaneLayout lay = lane_layout(f->plan, (int)sizeof(T), page_bytes, kLaneMaxSlots, warps);
+    const LaneLayout lay = lane_layout(f->plan, (int)sizeof(T), page_bytes, kLaneMaxSlots, warps, rpl);
     d = std::make_unique<DeviceLane>();
+    d->rpl = lay.rpl;
     d->warps = lay.warps, d->slots = lay.slots, d->page_bytes = lay.page_bytes, d->domains = lay.domains;
     d->top = lay.top, d->partials = lay.partials, d->fwd_live = lay.fwd_live, d->bwd_live = lay.bwd_live;
     d->entries = lay.fwd_entries + lay.bwd_entries, d->pages = lay.warp_page.back();
@@ -747,7 +748,7 @@ template <class T> DeviceLane *lane_for(yb_factor *f, int warps, int page_bytes,
 }
 
 template <class T> size_t lane_smem(const DeviceLane *d) {
-  return (size_t)d->warps * lane_warp_bytes<T>(d->slots, kLaneRing, d->page_bytes);
+  return (size_t)d->warps * lane_warp_bytes<T>(d->slots, kLaneRing, d->page_bytes, d->rpl);
 }
 
 // The lane solve of `count` right-hand sides: gather into the work array, solve in place, scatter.
@@ -763,20 +764,21 @@ cudaEvent_t *lane_timing_slot(yb_factor *f) {
   return t.ev[t.used++].data();
 }
 
-template <class T>
-void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
-                 cudaStream_t stream) {
+template <class T, int R>
+void launch_lane_r(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
+                   cudaStream_t stream) {
+  constexpr int64_t G = 32 * R;  // right-hand sides per group (a block)
   const int64_t n = f->n;
-  const size_t group_bytes = (size_t)n * 32 * sizeof(T);
-  const int64_t groups_all = (count + 31) / 32;
+  const size_t group_bytes = (size_t)n * G * sizeof(T);
+  const int64_t groups_all = (count + G - 1) / G;
   const int64_t per_launch = std::max<int64_t>(1, std::min<int64_t>(groups_all, (int64_t)(kLaneWorkBytes / group_bytes)));
   f->lane_work.reserve((size_t)per_launch * group_bytes);
-  f->lane_partial.reserve((size_t)per_launch * std::max(d->partials, 1) * 32 * sizeof(T));
+  f->lane_partial.reserve((size_t)per_launch * std::max(d->partials, 1) * G * sizeof(T));
   T *work = reinterpret_cast<T *>(f->lane_work.get());
   T *partial = reinterpret_cast<T *>(f->lane_partial.get());
   const size_t smem = lane_smem<T>(d);
   if (smem > (size_t)f->gpu->smem_optin) throw host::Error(host::kInvalidArgument, "the lane solve's block does not fit in shared memory");
-  cuda_check(cudaFuncSetAttribute(lane_solve_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+  cuda_check(cudaFuncSetAttribute(lane_solve_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "cudaFuncSetAttribute");
   LaneArgs a{};
   a.n = (int32_t)n;
@@ -788,43 +790,61 @@ void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, doub
   f->lane_withhold = -1;
   for (int64_t g0 = 0; g0 < groups_all; g0 += per_launch) {
     const int64_t groups = std::min(per_launch, groups_all - g0);
-    const int64_t cols = std::min(count - g0 * 32, groups * 32);
+    const int64_t cols = std::min(count - g0 * G, groups * G);
     const unsigned io_grid = (unsigned)lane_io_blocks(groups, n);
     cudaEvent_t *ev = lane_timing_slot(f);
     if (ev) cuda_check(cudaEventRecord(ev[0], stream), "cudaEventRecord");
-    lane_in_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(b + g0 * 32 * ldb, ldb, cols, (int32_t)n, groups, d->in_pos.get(), work,
-                                                                  nullptr);
+    lane_in_kernel<T, R><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(b + g0 * G * ldb, ldb, cols, (int32_t)n, groups,
+                                                                     d->in_pos.get(), work, nullptr);
     cuda_check(cudaGetLastError(), "lane_in_kernel launch");
     if (ev) cuda_check(cudaEventRecord(ev[1], stream), "cudaEventRecord");
-    lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
+    lane_solve_kernel<T, R><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
     cuda_check(cudaGetLastError(), "lane_solve_kernel launch");
     a.withhold = -1;
     if (ev) cuda_check(cudaEventRecord(ev[2], stream), "cudaEventRecord");
-    lane_out_kernel<T><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(work, cols, (int32_t)n, groups, d->out_pos.get(), x + g0 * 32 * ldx, ldx);
+    lane_out_kernel<T, R><<<io_grid, kLaneIoWarps * 32, 0, stream>>>(work, cols, (int32_t)n, groups, d->out_pos.get(),
+                                                                      x + g0 * G * ldx, ldx);
     cuda_check(cudaGetLastError(), "lane_out_kernel launch");
     if (ev) cuda_check(cudaEventRecord(ev[3], stream), "cudaEventRecord");
   }
 }
 
-// The lane layout a solve takes: the configured warps per block, or fewer when a block does not
-// fit shared memory; with page bytes 0, the largest page of 2048, 1024, 768 or 512 bytes with which
-// three blocks fit an SM (each block's rows are a long chain, so the grid should be one wave of as
-// many warps as fit), else 512. Null when the factor admits no lane layout.
-template <class T> DeviceLane *lane_pick(yb_factor *f, const TileConfig &cfg, cudaStream_t stream) {
+// The lane solve of `count` right-hand sides with the layout's right-hand sides per lane.
+template <class T>
+void launch_lane(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
+                 cudaStream_t stream) {
+  if (d->rpl == 2)
+    launch_lane_r<T, 2>(f, d, b, ldb, x, ldx, count, stream);
+  else
+    launch_lane_r<T, 1>(f, d, b, ldb, x, ldx, count, stream);
+}
+
+// The lane layout a solve takes, with `rpl` right-hand sides per lane: the configured warps per
+// block, or fewer when a block does not fit shared memory; with page bytes 0, the largest page of
+// 2048, 1024, 768 or 512 bytes with which three blocks (two with two right-hand sides per lane) fit
+// an SM (each block's rows are a long chain, so the grid should be one wave of as many warps as
+// fit), else 512; with two per lane and no page that lets two blocks fit, fewer warps (down to
+// four) before one block an SM. Null when the factor admits no lane layout.
+template <class T> DeviceLane *lane_pick(yb_factor *f, const TileConfig &cfg, int rpl, cudaStream_t stream) {
+  const size_t blocks = rpl == 1 ? 3 : 2;
+  DeviceLane *fallback = nullptr;
   for (int warps = cfg.lane_warps; warps >= 1; --warps) {
     DeviceLane *d = nullptr;
     if (cfg.lane_page > 0) {
-      d = lane_for<T>(f, warps, cfg.lane_page, stream);
+      d = lane_for<T>(f, warps, cfg.lane_page, rpl, stream);
     } else {
       for (int page : {2048, 1024, 768, 512}) {
-        d = lane_for<T>(f, warps, page, stream);
-        if (!d || 3 * (lane_smem<T>(d) + 1024) <= (size_t)f->gpu->smem_per_sm) break;
+        d = lane_for<T>(f, warps, page, rpl, stream);
+        if (!d || blocks * (lane_smem<T>(d) + 1024) <= (size_t)f->gpu->smem_per_sm) break;
       }
     }
     if (!d) return nullptr;
-    if (lane_smem<T>(d) <= (size_t)f->gpu->smem_optin) return d;
+    if (lane_smem<T>(d) > (size_t)f->gpu->smem_optin) continue;
+    if (rpl == 1 || cfg.lane_page > 0 || blocks * (lane_smem<T>(d) + 1024) <= (size_t)f->gpu->smem_per_sm) return d;
+    if (!fallback) fallback = d;
+    if (warps <= 4) break;
   }
-  return nullptr;
+  return fallback;
 }
 
 template <class T> TileConfig resolve(yb_factor *f, TileConfig cfg) {
@@ -895,7 +915,7 @@ void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t
   auto run = [&](auto zero, const TileConfig &configured, auto &fwd, auto &bwd, auto &scratch, auto &cache) {
     using T = decltype(zero);
     if (configured.kind == kTileLane || (configured.kind == kTileAuto && count >= configured.lane_min_count)) {
-      DeviceLane *d = lane_pick<T>(f, configured, stream);
+      DeviceLane *d = lane_pick<T>(f, configured, configured.lane_rpl, stream);
       if (d && (configured.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane<T>(f, d, b, ldb, x, ldx, count, stream);
         return;
@@ -1254,11 +1274,12 @@ extern "C" int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t 
     require(!f->is_complex, "a complex factor has no lane solve");
     cuda_check(cudaSetDevice(f->gpu->device), "cudaSetDevice");
     const TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
-    DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, t, f->gpu->stream) : lane_pick<float>(f, t, f->gpu->stream);
+    DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, t, t.lane_rpl, f->gpu->stream)
+                                         : lane_pick<float>(f, t, t.lane_rpl, f->gpu->stream);
     if (!d) throw host::Error(host::kInvalidArgument, "the factor admits no lane layout");
     const size_t smem = precision == YB_FP64 ? lane_smem<double>(d) : lane_smem<float>(d);
     const int64_t v[12] = {d->slots, d->pages, d->page_bytes, d->fwd_live, d->bwd_live, d->entries, (int64_t)smem,
-                           d->warps, d->domains, d->top, d->partials, 0};
+                           d->warps, d->domains, d->top, d->partials, d->rpl};
     std::copy(v, v + 12, info);
     return YB_OK;
   });
@@ -1273,6 +1294,16 @@ extern "C" int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t w
             "pages of 256 to 16384 bytes, a multiple of 16, or 0 for the automatic choice");
     TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
     t.lane_warps = warps, t.lane_page = page_bytes;
+    return YB_OK;
+  });
+}
+
+extern "C" int32_t yb_factor_set_lane_rhs_per_lane(yb_factor *f, int32_t precision, int32_t rhs_per_lane) {
+  return guard([&] {
+    require(f != nullptr, "null factor");
+    require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
+    require(rhs_per_lane == 1 || rhs_per_lane == 2, "1 or 2 right-hand sides per lane");
+    (precision == YB_FP64 ? f->tile64 : f->tile32).lane_rpl = rhs_per_lane;
     return YB_OK;
   });
 }
@@ -1443,7 +1474,7 @@ void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t l
   r.ldb = ldb, r.ldx = ldx;
   const size_t smem = lane_smem<T>(d);
   if (smem > (size_t)f->gpu->smem_optin) throw host::Error(host::kInvalidArgument, "the lane solve's block does not fit in shared memory");
-  cuda_check(cudaFuncSetAttribute(lane_solve_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+  cuda_check(cudaFuncSetAttribute(lane_solve_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "cudaFuncSetAttribute");
   LaneArgs a{};
   a.n = (int32_t)n;
@@ -1475,7 +1506,7 @@ void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t l
     for (int32_t pass = 0; pass <= max_steps; ++pass) {
       T *dk = pass == 1 ? dB : dA;  // this pass's correction
       a.xout = dk;
-      lane_solve_kernel<T><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
+      lane_solve_kernel<T, 1><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
       check("lane_solve_kernel launch");
       if (pass == 0)
         lane_residual_kernel<0><<<rows_grid, kResWarps * 32, 0, stream>>>(r, dk, nullptr, nullptr, true);
@@ -1523,7 +1554,7 @@ extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rh
     const TileConfig &t32 = f->tile32;
     if (t32.kind == kTileLane ||
         (t32.kind == kTileAuto && count >= std::max(t32.lane_min_count, t32.refine_lane_min_count))) {
-      DeviceLane *d = lane_pick<float>(f, t32, s);
+      DeviceLane *d = lane_pick<float>(f, t32, 1, s);  // its kernels take groups of 32 columns
       if (d && (t32.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane_refined(f, d, d_rhs, ldb, d_out, ldx, count, max_steps, tolerance, d_ratio, d_steps, s);
         return YB_OK;
@@ -1609,20 +1640,22 @@ extern "C" int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t c
             time_config(run);
           }
         }
-    // the lane solve, when the factor admits it, at 4, 6 and 8 warps per block
-    for (int warps : {4, 6, 8}) {
-      TileConfig run = saved;
-      run.kind = kTileLane, run.lane_warps = warps, run.lane_page = 0;
-      DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, run, s) : lane_pick<float>(f, run, s);
-      if (!d || d->warps != warps) continue;  // none, or the block took fewer warps (timed on its own)
-      time_config(run);
-    }
+    // the lane solve, when the factor admits it, at 4, 6 and 8 warps per block, with one and with
+    // two right-hand sides per lane
+    for (int rpl : {1, 2})
+      for (int warps : {4, 6, 8}) {
+        TileConfig run = saved;
+        run.kind = kTileLane, run.lane_warps = warps, run.lane_page = 0, run.lane_rpl = rpl;
+        DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, run, rpl, s) : lane_pick<float>(f, run, rpl, s);
+        if (!d || d->warps != warps) continue;  // none, or the block took fewer warps (timed on its own)
+        time_config(run);
+      }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     t = std::isfinite(best_time) ? best : saved;
     if (config) {
       if (t.kind == kTileLane) {
-        DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, t, s) : lane_pick<float>(f, t, s);
+        DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, t, t.lane_rpl, s) : lane_pick<float>(f, t, t.lane_rpl, s);
         config[0] = t.kind, config[1] = 0, config[2] = t.lane_warps, config[3] = kLaneRing, config[4] = d->page_bytes;
       } else {
         config[0] = t.kind, config[1] = t.width, config[2] = t.domain_warps, config[3] = t.domain_ring,

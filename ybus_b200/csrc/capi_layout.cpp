@@ -47,8 +47,8 @@ int32_t yb_domain_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t
 
 int32_t yb_lane_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
                                 const int64_t *perm, int32_t value_bytes, int32_t page_bytes, int32_t max_slots,
-                                int32_t warps, int64_t *info, uint8_t *blob, int32_t *warp_page, int32_t *in_pos,
-                                int32_t *out_pos) {
+                                int32_t warps, int32_t rhs_per_lane, int64_t *info, uint8_t *blob, int32_t *warp_page,
+                                int32_t *in_pos, int32_t *out_pos) {
   return guard([&] {
     require(n >= 0 && l_ptr && perm && info, "null argument");
     host::Compressed<double> lower;
@@ -66,9 +66,9 @@ int32_t yb_lane_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *
     upper.by_rows = true;
     std::vector<int64_t> p(perm, perm + n);
     const Plan<double> plan = build_plan<double>(n, lower, false, upper, p, p);
-    const LaneLayout lay = lane_layout(plan, value_bytes, page_bytes, max_slots, warps);
+    const LaneLayout lay = lane_layout(plan, value_bytes, page_bytes, max_slots, warps, rhs_per_lane);
     const int64_t v[12] = {lay.slots, lay.warp_page.back(), lay.page_bytes, lay.fwd_live, lay.bwd_live, lay.fwd_entries,
-                           lay.bwd_entries, lay.warps, lay.domains, lay.top, lay.partials, 0};
+                           lay.bwd_entries, lay.warps, lay.domains, lay.top, lay.partials, lay.rpl};
     std::copy(v, v + 12, info);
     if (blob) std::copy(lay.blob.begin(), lay.blob.end(), blob);
     if (warp_page) std::copy(lay.warp_page.begin(), lay.warp_page.end(), warp_page);

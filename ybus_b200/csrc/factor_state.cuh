@@ -111,6 +111,7 @@ struct TileConfig {
   // fewer leave SMs idle, where the domain solve's tiles spread over all of them)
   int64_t lane_min_count = 3072;
   int lane_warps = 8, lane_page = 0;  // the lane solve's warps per block (one group of 32 right-hand sides), page bytes
+  int lane_rpl = 1;                   // right-hand sides per lane of the plain lane solve (1 or 2)
   // the refined solve takes the lane solve from this many right-hand sides on (its passes cost more
   // launches than the plain solve's, so its crossover with the fused domain refinement lies higher)
   int64_t refine_lane_min_count = 5120;
@@ -119,6 +120,7 @@ struct TileConfig {
 // A lane layout on the device (LaneLayout in plan.hpp).
 struct DeviceLane {
   int32_t warps = 0, slots = 0, page_bytes = 0, domains = 0, top = 0, partials = 0, fwd_live = 0, bwd_live = 0;
+  int32_t rpl = 1;  // right-hand sides per lane the layout's offsets count
   int64_t entries = 0, pages = 0;
   DeviceArray<uint8_t> blob;
   DeviceArray<int32_t> warp_page, in_pos, out_pos;
@@ -179,7 +181,7 @@ struct yb_factor {
   // domain layouts by shape (value bytes, warps, page bytes, cut); a null entry: the factor admits none
   std::map<std::tuple<int, int, int, int>, std::unique_ptr<yb::DeviceDomain>> domains;
   // lane layouts by (value bytes, warps, page bytes); a null entry: the factor admits none
-  std::map<std::tuple<int, int, int>, std::unique_ptr<yb::DeviceLane>> lanes;
+  std::map<std::tuple<int, int, int, int>, std::unique_ptr<yb::DeviceLane>> lanes;
   yb::DeviceArray<uint8_t> lane_work, lane_partial;  // the lane solve's work and partial arrays
   yb::LaneTiming lane_timing;
   yb::DeviceArray<int32_t> error;  // the device error word (a bounded wait that ran out)

@@ -61,13 +61,15 @@ struct Slots {
 // p is work_row[p]) and prefetch-ring slot, and puts a kLanePrefetch record, with the offsets of the
 // rows it copies, before every kLaneBatch rows.
 template <class T> struct PageWriter {
-  static constexpr uint32_t kEntry = sizeof(T) == 8 ? 16 : 8, kRow = 32 * sizeof(T);
+  static constexpr uint32_t kEntry = sizeof(T) == 8 ? 16 : 8;
+  uint32_t kRow;  // a live slot's, work row's or partial row's bytes: 32 lanes of rpl values
   int32_t page_bytes;
   std::vector<uint8_t> &blob;
   const std::vector<int32_t> &work_row;
   size_t pos = 0;
   int32_t start = 0, len = 0, step = 1, row_i = 0;
-  PageWriter(std::vector<uint8_t> &b, int32_t pb, const std::vector<int32_t> &wr) : page_bytes(pb), blob(b), work_row(wr) {
+  PageWriter(std::vector<uint8_t> &b, int32_t pb, const std::vector<int32_t> &wr, uint32_t row_bytes)
+      : kRow(row_bytes), page_bytes(pb), blob(b), work_row(wr) {
     open();
   }
   void open() {
@@ -219,11 +221,12 @@ struct Cut {
 };
 
 template <class V, class T>
-LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int32_t warps) {
+LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int32_t warps, int32_t rpl) {
   const int32_t n = plan.n;
   LaneLayout lay;
   lay.page_bytes = page_bytes;
   lay.value_bytes = (int32_t)sizeof(T);
+  lay.rpl = rpl;
   lay.warps = warps;
   struct Row {
     int32_t p0 = 0, p1 = 0;
@@ -412,7 +415,7 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
     }
     for (auto &t : top_sums) std::sort(t.begin(), t.end(), [&](int32_t a, int32_t b) { return newpos[a] < newpos[b]; });
   }
-  const uint32_t row_bytes = 32u * (uint32_t)sizeof(T);  // a live slot, or a work or partial row
+  const uint32_t row_bytes = 32u * (uint32_t)sizeof(T) * (uint32_t)rpl;  // a live slot, or a work or partial row
   auto off = [&](int32_t s) { return (uint32_t)s * row_bytes; };
   auto self_of = [&](int32_t s) { return (uint32_t)s * row_bytes / 16; };  // headers hold slot offsets / 16
   std::vector<std::pair<T, uint32_t>> entries;
@@ -462,7 +465,7 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   };
   lay.warp_page.assign(1, 0);
   for (int32_t w = 0; w < warps; ++w) {
-    PageWriter<T> pw(lay.blob, page_bytes, work_row);
+    PageWriter<T> pw(lay.blob, page_bytes, work_row, row_bytes);
     const int32_t p0 = warp_start[w], p1 = warp_start[w + 1] - 1;
     {  // forward domains, each ending with its flush
       Slots slots;
@@ -549,15 +552,17 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
 }  // namespace
 
 template <class T>
-LaneLayout lane_layout(const Plan<T> &plan, int32_t value_bytes, int32_t page_bytes, int32_t max_slots, int32_t warps) {
+LaneLayout lane_layout(const Plan<T> &plan, int32_t value_bytes, int32_t page_bytes, int32_t max_slots, int32_t warps,
+                       int32_t rpl) {
   if (page_bytes < 256 || page_bytes % 16)
     throw host::Error(host::kInvalidArgument, "pages must be 16-byte multiples of at least 256 bytes");
   if (warps < 1 || warps > 32) throw host::Error(host::kInvalidArgument, "1 to 32 warps per block");
-  if (value_bytes == 8) return build<T, double>(plan, page_bytes, max_slots, warps);
-  if (value_bytes == 4) return build<T, float>(plan, page_bytes, max_slots, warps);
+  if (rpl != 1 && rpl != 2) throw host::Error(host::kInvalidArgument, "1 or 2 right-hand sides per lane");
+  if (value_bytes == 8) return build<T, double>(plan, page_bytes, max_slots, warps, rpl);
+  if (value_bytes == 4) return build<T, float>(plan, page_bytes, max_slots, warps, rpl);
   throw host::Error(host::kInvalidArgument, "values must be 8 or 4 bytes");
 }
 
-template LaneLayout lane_layout(const Plan<double> &, int32_t, int32_t, int32_t, int32_t);
+template LaneLayout lane_layout(const Plan<double> &, int32_t, int32_t, int32_t, int32_t, int32_t);
 
 }  // namespace yb

@@ -44,10 +44,12 @@ struct LaneArgs {
                      // issued, so that warp's bounded wait runs out (-1: none)
 };
 
-// A warp's shared memory: live slots, the prefetch ring, the page ring and its barriers.
-template <class T> __host__ __device__ inline size_t lane_warp_bytes(int32_t slots, int32_t ring, int32_t page_bytes) {
-  const size_t b = (size_t)slots * 32 * sizeof(T) + (size_t)kLaneRows * 32 * sizeof(T) + (size_t)ring * page_bytes +
-                   (size_t)ring * 8;
+// A warp's shared memory: live slots, the prefetch ring, the page ring and its barriers, with rpl
+// right-hand sides per lane (a slot and a ring row hold 32 * rpl values).
+template <class T>
+__host__ __device__ inline size_t lane_warp_bytes(int32_t slots, int32_t ring, int32_t page_bytes, int32_t rpl = 1) {
+  const size_t row = (size_t)32 * sizeof(T) * rpl;
+  const size_t b = (size_t)slots * row + (size_t)kLaneRows * row + (size_t)ring * page_bytes + (size_t)ring * 8;
   return (b + 127) & ~(size_t)127;
 }
 
@@ -81,58 +83,107 @@ __device__ __forceinline__ void lane_entry(uint32_t e, float &v, uint32_t &word,
 // takes the barriers its stream did not reach at the kernel's end).
 __device__ __forceinline__ void lane_barrier() { asm volatile("barrier.sync 0;" ::: "memory"); }
 
-// acc[offset] -= val * z for C entries (C known at compile time) at shared offset e; the offsets of
-// one record are distinct, so every accumulator is read before any is written.
-template <class T, int C> __device__ __forceinline__ void lane_scatter_n(uint32_t e, T z, uint32_t live) {
+// A lane's values: one per right-hand side it carries (R = 1 or 2, adjacent columns of the group),
+// loaded and stored together, 8 or 16 bytes, in shared and in global memory.
+template <class T, int R> struct Lv {
+  T v[R];
+};
+template <class T, int R> __device__ __forceinline__ Lv<T, R> lv_load(const void *p) {
+  Lv<T, R> x;
+  if constexpr (R == 1) {
+    x.v[0] = *reinterpret_cast<const T *>(p);
+  } else if constexpr (sizeof(T) == 8) {
+    const double2 q = *reinterpret_cast<const double2 *>(p);
+    x.v[0] = q.x, x.v[1] = q.y;
+  } else {
+    const float2 q = *reinterpret_cast<const float2 *>(p);
+    x.v[0] = q.x, x.v[1] = q.y;
+  }
+  return x;
+}
+template <class T, int R> __device__ __forceinline__ void lv_store(void *p, const Lv<T, R> &x) {
+  if constexpr (R == 1)
+    *reinterpret_cast<T *>(p) = x.v[0];
+  else if constexpr (sizeof(T) == 8)
+    *reinterpret_cast<double2 *>(p) = make_double2(x.v[0], x.v[1]);
+  else
+    *reinterpret_cast<float2 *>(p) = make_float2(x.v[0], x.v[1]);
+}
+template <class T, int R> __device__ __forceinline__ Lv<T, R> lv_ld(uint32_t off) { return lv_load<T, R>(lane_shared + off); }
+template <class T, int R> __device__ __forceinline__ void lv_st(uint32_t off, const Lv<T, R> &x) {
+  lv_store<T, R>(lane_shared + off, x);
+}
+template <class T, int R> __device__ __forceinline__ Lv<T, R> lv_zero() {
+  Lv<T, R> x;
+#pragma unroll
+  for (int r = 0; r < R; ++r) x.v[r] = T(0);
+  return x;
+}
+
+// acc[offset] -= val * z for C entries (C known at compile time) at shared offset e, for each of
+// the lane's R right-hand sides; the offsets of one record are distinct, so every accumulator is
+// read before any is written.
+template <class T, int R, int C> __device__ __forceinline__ void lane_scatter_n(uint32_t e, const Lv<T, R> &z, uint32_t live) {
   constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8;
-  T v[C], a[C];
+  T v[C];
+  Lv<T, R> a[C];
   uint32_t o[C], w;
 #pragma unroll
   for (int c = 0; c < C; ++c) lane_entry(e + c * E, v[c], w, o[c]);
 #pragma unroll
-  for (int c = 0; c < C; ++c) a[c] = lane_at<T>(live + o[c]);
+  for (int c = 0; c < C; ++c) a[c] = lv_ld<T, R>(live + o[c]);
 #pragma unroll
-  for (int c = 0; c < C; ++c) lane_at<T>(live + o[c]) = fma(-v[c], z, a[c]);
+  for (int c = 0; c < C; ++c) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) a[c].v[r] = fma(-v[c], z.v[r], a[c].v[r]);
+    lv_st<T, R>(live + o[c], a[c]);
+  }
 }
 
 // acc -= val * x[offset] over C entries, in stored order.
-template <class T, int C> __device__ __forceinline__ T lane_gather_n(uint32_t e, T acc, uint32_t live) {
+template <class T, int R, int C> __device__ __forceinline__ Lv<T, R> lane_gather_n(uint32_t e, Lv<T, R> acc, uint32_t live) {
   constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8;
-  T v[C], x[C];
+  T v[C];
+  Lv<T, R> x[C];
   uint32_t o[C], w;
 #pragma unroll
   for (int c = 0; c < C; ++c) lane_entry(e + c * E, v[c], w, o[c]);
 #pragma unroll
-  for (int c = 0; c < C; ++c) x[c] = lane_at<T>(live + o[c]);
+  for (int c = 0; c < C; ++c) x[c] = lv_ld<T, R>(live + o[c]);
 #pragma unroll
-  for (int c = 0; c < C; ++c) acc = fma(-v[c], x[c], acc);
+  for (int c = 0; c < C; ++c)
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc.v[r] = fma(-v[c], x[c].v[r], acc.v[r]);
   return acc;
 }
 
 // The same for any count, four at a time.
-template <class T> __device__ __forceinline__ void lane_scatter(uint32_t e, uint32_t count, T z, uint32_t live) {
+template <class T, int R>
+__device__ __forceinline__ void lane_scatter(uint32_t e, uint32_t count, const Lv<T, R> &z, uint32_t live) {
   constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8;
   uint32_t i = 0;
-  for (; i + 4 <= count; i += 4) lane_scatter_n<T, 4>(e + i * E, z, live);
-  for (; i < count; ++i) lane_scatter_n<T, 1>(e + i * E, z, live);
+  for (; i + 4 <= count; i += 4) lane_scatter_n<T, R, 4>(e + i * E, z, live);
+  for (; i < count; ++i) lane_scatter_n<T, R, 1>(e + i * E, z, live);
 }
-template <class T> __device__ __forceinline__ T lane_gather(uint32_t e, uint32_t count, T acc, uint32_t live) {
+template <class T, int R>
+__device__ __forceinline__ Lv<T, R> lane_gather(uint32_t e, uint32_t count, Lv<T, R> acc, uint32_t live) {
   constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8;
   uint32_t i = 0;
-  for (; i + 4 <= count; i += 4) acc = lane_gather_n<T, 4>(e + i * E, acc, live);
-  for (; i < count; ++i) acc = lane_gather_n<T, 1>(e + i * E, acc, live);
+  for (; i + 4 <= count; i += 4) acc = lane_gather_n<T, R, 4>(e + i * E, acc, live);
+  for (; i < count; ++i) acc = lane_gather_n<T, R, 1>(e + i * E, acc, live);
   return acc;
 }
 
-// Block g solves the 32 right-hand sides of group g in `work` in place; `partial` holds each
-// block's partial array. Three blocks share an SM (as many as its shared memory holds), so the
-// launch bound lets each thread take up to 80 registers: the compiler then keeps the records'
-// fields and addresses in registers instead of recomputing them (13 % fewer instructions and 7 %
-// less time than with the 44 registers it picks unbounded).
-template <class T>
-__global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneArgs a, T *__restrict__ work,
+// Block g solves the 32 R right-hand sides of group g in `work` in place (R per lane: the records'
+// decoding then serves R times the arithmetic); `partial` holds each block's partial array. With
+// R = 1 three blocks share an SM (as many as its shared memory holds), so the launch bound lets each
+// thread take up to 80 registers: the compiler then keeps the records' fields and addresses in
+// registers instead of recomputing them (13 % fewer instructions and 7 % less time than with the
+// 44 registers it picks unbounded); with R = 2 two blocks do.
+template <class T, int R>
+__global__ void __launch_bounds__(kLaneMaxWarps * 32, R == 1 ? 3 : 2) lane_solve_kernel(LaneArgs a, T *__restrict__ work,
                                                                        T *__restrict__ partial) {
-  constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8, ROW = 32 * sizeof(T);
+  constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8, VB = sizeof(T) * R, ROW = 32 * VB;
   // The warp index through a shuffle from lane 0: the compiler then knows it (and the shared
   // offsets, record fields and branches derived from it) to be the same across the warp, and keeps
   // the records' decoding on the uniform datapath instead of every lane's registers.
@@ -140,20 +191,20 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
   const int lane = threadIdx.x & 31, warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
   constexpr int S = kLaneRing;  // known here, so the ring's slot and phase are a mask and a shift
   const int PB = a.page_bytes;
-  const uint32_t base = (uint32_t)(warp * lane_warp_bytes<T>(a.slots, S, PB));
-  const uint32_t live = base + lane * (uint32_t)sizeof(T);                     // this lane's slot 0
-  const uint32_t rows = base + (uint32_t)a.slots * ROW + lane * (uint32_t)sizeof(T);  // its ring slot 0
+  const uint32_t base = (uint32_t)(warp * lane_warp_bytes<T>(a.slots, S, PB, R));
+  const uint32_t live = base + lane * VB;                     // this lane's slot 0
+  const uint32_t rows = base + (uint32_t)a.slots * ROW + lane * VB;  // its ring slot 0
   const uint32_t ring = base + (uint32_t)a.slots * ROW + (uint32_t)kLaneRows * ROW;  // the page ring
   uint64_t *full = &lane_at<uint64_t>(ring + (uint32_t)S * PB);
   const uint32_t smem_s = smem_u32(lane_shared);  // the shared window address of offset 0
-  uint8_t *w_lane = reinterpret_cast<uint8_t *>(work + (size_t)blockIdx.x * a.n * 32 + lane);
-  uint8_t *x_lane = a.xout ? reinterpret_cast<uint8_t *>(static_cast<T *>(a.xout) + (size_t)blockIdx.x * a.n * 32 + lane)
-                           : w_lane;
-  uint8_t *part_lane = reinterpret_cast<uint8_t *>(partial + (size_t)blockIdx.x * a.partials * 32 + lane);
+  uint8_t *w_lane = reinterpret_cast<uint8_t *>(work + ((size_t)blockIdx.x * a.n * 32 + lane) * R);
+  uint8_t *x_lane =
+      a.xout ? reinterpret_cast<uint8_t *>(static_cast<T *>(a.xout) + ((size_t)blockIdx.x * a.n * 32 + lane) * R) : w_lane;
+  uint8_t *part_lane = reinterpret_cast<uint8_t *>(partial + ((size_t)blockIdx.x * a.partials * 32 + lane) * R);
   const int p0 = __ldg(a.warp_page + warp), np = __ldg(a.warp_page + warp + 1) - p0;
   const uint8_t *stream = a.blob + (size_t)p0 * PB;
 
-  for (int s = 0; s < a.slots; ++s) lane_at<T>(live + s * ROW) = T(0);
+  for (int s = 0; s < a.slots; ++s) lv_st<T, R>(live + s * ROW, lv_zero<T, R>());
   if (lane == 0) {
     for (int s = 0; s < S; ++s) mbar_init(full + s, 1);
     mbar_fence_init();
@@ -173,7 +224,7 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
   bool ok = __all_sync(0xffffffffu, np > 0 && mbar_wait_bounded(full, 0, a.error));
   bool ended = false;
   int barriers = 0;
-  T z = T(0);  // the forward row's result, or the backward row's running sum
+  Lv<T, R> z = lv_zero<T, R>();  // the forward row's result, or the backward row's running sum
   // the header of the record being read, loaded while the record before it runs (pages are written
   // only by the bulk copies, never by a record)
   uint4 hn = lane_at<uint4>(page);
@@ -192,17 +243,19 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
       dinv = __uint_as_float(h.z);
     // the start of a forward row: z from b and the row's accumulator, into the work row
     auto forward = [&]() {
-      T &acc = lane_at<T>(self);
-      const T b = lane_at<T>(b_at) + acc;
-      acc = T(0);
-      z = b * dinv;
-      *reinterpret_cast<T *>(w_lane + h.y) = z;
+      const Lv<T, R> acc = lv_ld<T, R>(self), b = lv_ld<T, R>(b_at);
+      lv_st<T, R>(self, lv_zero<T, R>());
+#pragma unroll
+      for (int r = 0; r < R; ++r) z.v[r] = (b.v[r] + acc.v[r]) * dinv;
+      lv_store<T, R>(w_lane + h.y, z);
     };
     // the end of a backward row: x into its slot and its row of the output
     auto backward = [&]() {
-      const T x = z * dinv;
-      lane_at<T>(self) = x;
-      *reinterpret_cast<T *>(x_lane + h.y) = x;
+      Lv<T, R> x;
+#pragma unroll
+      for (int r = 0; r < R; ++r) x.v[r] = z.v[r] * dinv;
+      lv_st<T, R>(self, x);
+      lv_store<T, R>(x_lane + h.y, x);
     };
     // a prefetch block: the batch's rows into their half of the ring, then the batch before waited for
     auto prefetch = [&](uint32_t at) {
@@ -214,7 +267,7 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
       for (int q = 0; q < kLaneBatch; ++q)
         if (q < (int)nrows)
           asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst + q * ROW), "l"(w_lane + off[q]),
-                       "n"(sizeof(T))
+                       "n"(VB)
                        : "memory");
       cp_async_commit();
       cp_async_wait<1>();
@@ -230,15 +283,15 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
   case K: {                                                               \
     if (PRE) prefetch(e + padded(C));                                     \
     forward();                                                            \
-    if (C > 0) lane_scatter_n<T, (C > 0 ? C : 1)>(e, z, live);            \
+    if (C > 0) lane_scatter_n<T, R, (C > 0 ? C : 1)>(e, z, live);         \
     page = next;                                                          \
     continue;                                                             \
   }
 #define YB_LANE_BWD(K, C, PRE)                                            \
   case K: {                                                               \
     if (PRE) prefetch(e + padded(C));                                     \
-    const T b = lane_at<T>(b_at);                                         \
-    z = C > 0 ? lane_gather_n<T, (C > 0 ? C : 1)>(e, b, live) : b;        \
+    const Lv<T, R> b = lv_ld<T, R>(b_at);                                 \
+    z = C > 0 ? lane_gather_n<T, R, (C > 0 ? C : 1)>(e, b, live) : b;     \
     backward();                                                           \
     page = next;                                                          \
     continue;                                                             \
@@ -263,34 +316,37 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
       YB_LANE_BWD(kLaneBwdPre1 + 3, 4, true)
 #undef YB_LANE_FWD
 #undef YB_LANE_BWD
-      case kLaneFwdRowN: forward(); lane_scatter<T>(e, count, z, live); break;
-      case kLaneFwdMore: lane_scatter<T>(e, count, z, live); break;
-      case kLaneBwdRowN: z = lane_gather<T>(e, count, lane_at<T>(b_at), live); backward(); break;
-      case kLaneBwdBegin: z = lane_gather<T>(e, count, lane_at<T>(b_at), live); break;
-      case kLaneBwdMore: z = lane_gather<T>(e, count, z, live); break;
-      case kLaneBwdEnd: z = lane_gather<T>(e, count, z, live); backward(); break;
+      case kLaneFwdRowN: forward(); lane_scatter<T, R>(e, count, z, live); break;
+      case kLaneFwdMore: lane_scatter<T, R>(e, count, z, live); break;
+      case kLaneBwdRowN: z = lane_gather<T, R>(e, count, lv_ld<T, R>(b_at), live); backward(); break;
+      case kLaneBwdBegin: z = lane_gather<T, R>(e, count, lv_ld<T, R>(b_at), live); break;
+      case kLaneBwdMore: z = lane_gather<T, R>(e, count, z, live); break;
+      case kLaneBwdEnd: z = lane_gather<T, R>(e, count, z, live); backward(); break;
       case kLanePrefetch: prefetch(e); break;
       case kLanePhase:
         cp_async_wait<0>();
         __threadfence();  // the rows this lane stored are what the phase's copies read
         break;
       case kLaneTopSum: {  // the row and up to four partials in flight at a time, added in order
-        T *row = reinterpret_cast<T *>(w_lane + h.y);
-        T acc = *row;
+        uint8_t *row = w_lane + h.y;
+        Lv<T, R> acc = lv_load<T, R>(row);
         for (uint32_t c = 0; c < count; c += 4) {
-          T p[4];
+          Lv<T, R> p[4];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             T v;
             uint32_t w, o;
             lane_entry(e + min(c + q, count - 1) * E, v, w, o);
-            p[q] = *reinterpret_cast<const T *>(part_lane + w);
+            p[q] = lv_load<T, R>(part_lane + w);
           }
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            if (c + q < count) acc += p[q];
+            if (c + q < count) {
+#pragma unroll
+              for (int r = 0; r < R; ++r) acc.v[r] += p[q].v[r];
+            }
         }
-        *row = acc;
+        lv_store<T, R>(row, acc);
         break;
       }
       case kLaneFlush:
@@ -298,24 +354,24 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, 3) lane_solve_kernel(LaneA
           T v;
           uint32_t w, o;
           lane_entry(e + c * E, v, w, o);
-          *reinterpret_cast<T *>(part_lane + w) = lane_at<T>(live + o);
-          lane_at<T>(live + o) = T(0);
+          lv_store<T, R>(part_lane + w, lv_ld<T, R>(live + o));
+          lv_st<T, R>(live + o, lv_zero<T, R>());
         }
         break;
       case kLaneImport:  // four loads in flight at a time
         for (uint32_t c = 0; c < count; c += 4) {
-          T x[4];
+          Lv<T, R> x[4];
           uint32_t o[4];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             T v;
             uint32_t w;
             lane_entry(e + min(c + q, count - 1) * E, v, w, o[q]);
-            x[q] = *reinterpret_cast<const T *>(x_lane + w);
+            x[q] = lv_load<T, R>(x_lane + w);
           }
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            if (c + q < count) lane_at<T>(live + o[q]) = x[q];
+            if (c + q < count) lv_st<T, R>(live + o[q], x[q]);
         }
         break;
       case kLaneBarrier:
@@ -402,11 +458,12 @@ __host__ __device__ inline int64_t lane_io_blocks(int64_t groups, int64_t n) {
   return (groups * ((n + 31) / 32) + kLaneIoWarps - 1) / kLaneIoWarps;
 }
 
-// b (natural rows, column-major, ldb) into the work array [group][work row][lane] (b's row i to
-// work row in_pos[i]); right-hand sides past `count` are zero. Each lane reads its row of the
-// group's 32 right-hand sides, one coalesced load across the warp per right-hand side, and stores
-// the whole 32-value work row in 32-byte pieces: no shared memory, no barrier.
-template <class T>
+// b (natural rows, column-major, ldb) into the work array [group][work row][32 R values] (b's row i
+// to work row in_pos[i]; the row's values are the group's 32 R columns in order, so lane l's R
+// values are columns R l .. R l + R - 1); right-hand sides past `count` are zero. Each lane reads its
+// row of the group's columns, 32 at a time, one coalesced load across the warp per column, and
+// stores each 32-value piece of the work row in 32-byte pieces: no shared memory, no barrier.
+template <class T, int R = 1>
 __global__ void __launch_bounds__(kLaneIoWarps * 32) lane_in_kernel(const double *__restrict__ b, int64_t ldb, int64_t count,
                                                                    int32_t n, int64_t groups,
                                                                    const int32_t *__restrict__ in_pos,
@@ -418,18 +475,22 @@ __global__ void __launch_bounds__(kLaneIoWarps * 32) lane_in_kernel(const double
   if (g >= groups || (group_active && !group_active[g])) return;
   const int i = (int)(w % chunks) * 32 + lane;
   if (i >= n) return;
-  double v[32];
+  T *row = work + ((size_t)g * n + __ldg(in_pos + i)) * 32 * R;
 #pragma unroll
-  for (int c = 0; c < 32; ++c) {
-    const int64_t col = g * 32 + c;
-    v[c] = col < count ? b[col * ldb + i] : 0.0;
+  for (int h = 0; h < R; ++h) {
+    double v[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+      const int64_t col = (g * R + h) * 32 + c;
+      v[c] = col < count ? b[col * ldb + i] : 0.0;
+    }
+    lane_row_store(row + h * 32, v);
   }
-  lane_row_store(work + ((size_t)g * n + __ldg(in_pos + i)) * 32, v);
 }
 
 // The work array (solutions in their work rows) into x (natural rows, column-major, ldx): x's
 // row i from work row out_pos[i], the mirror of lane_in_kernel.
-template <class T>
+template <class T, int R = 1>
 __global__ void __launch_bounds__(kLaneIoWarps * 32) lane_out_kernel(const T *__restrict__ work, int64_t count, int32_t n,
                                                                     int64_t groups, const int32_t *__restrict__ out_pos,
                                                                     double *__restrict__ x, int64_t ldx) {
@@ -439,12 +500,16 @@ __global__ void __launch_bounds__(kLaneIoWarps * 32) lane_out_kernel(const T *__
   if (g >= groups) return;
   const int i = (int)(w % chunks) * 32 + lane;
   if (i >= n) return;
-  double v[32];
-  lane_row_load(work + ((size_t)g * n + __ldg(out_pos + i)) * 32, v);
+  const T *row = work + ((size_t)g * n + __ldg(out_pos + i)) * 32 * R;
 #pragma unroll
-  for (int c = 0; c < 32; ++c) {
-    const int64_t col = g * 32 + c;
-    if (col < count) x[col * ldx + i] = v[c];
+  for (int h = 0; h < R; ++h) {
+    double v[32];
+    lane_row_load(row + h * 32, v);
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+      const int64_t col = (g * R + h) * 32 + c;
+      if (col < count) x[col * ldx + i] = v[c];
+    }
   }
 }
 

@@ -195,6 +195,7 @@ constexpr int kLaneBatch = 4;              // work rows per prefetch
 constexpr int kLaneRows = 2 * kLaneBatch;  // slots of a warp's prefetch ring
 struct LaneLayout {
   int32_t warps = 1, slots = 0, page_bytes = 0, value_bytes = 0;
+  int32_t rpl = 1;  // right-hand sides per lane: a slot or row holds 32 * rpl values
   int32_t domains = 0, top = 0, partials = 0;  // partials: partial-array values per block
   int32_t fwd_live = 0, bwd_live = 0;          // the peak number of live values in each sweep
   int64_t fwd_entries = 0, bwd_entries = 0;
@@ -220,10 +221,12 @@ Plan<T> build_plan(int64_t n, const host::Compressed<T> &lower, bool unit_lower,
                    const host::Compressed<T> &upper, const std::vector<int64_t> &in_perm,
                    const std::vector<int64_t> &out_perm);
 
-// Builds the lane layout of `plan` for values of `value_bytes` (8 or 4) and `warps` warps per block.
-// Throws host::Error (kInvalidArgument) when no postorder serves both sweeps, or (kTooLarge) when
-// more than `max_slots` slots would be needed.
+// Builds the lane layout of `plan` for values of `value_bytes` (8 or 4), `warps` warps per block and
+// `rpl` (1 or 2) right-hand sides per lane: the records are the same but for their byte offsets,
+// which count slots and rows of 32 * rpl values. Throws host::Error (kInvalidArgument) when no
+// postorder serves both sweeps, or (kTooLarge) when more than `max_slots` slots would be needed.
 template <class T>
-LaneLayout lane_layout(const Plan<T> &plan, int32_t value_bytes, int32_t page_bytes, int32_t max_slots, int32_t warps);
+LaneLayout lane_layout(const Plan<T> &plan, int32_t value_bytes, int32_t page_bytes, int32_t max_slots, int32_t warps,
+                       int32_t rpl = 1);
 
 }  // namespace yb

@@ -237,13 +237,17 @@ class GpuFactor:
         return {"tile": w.value, "cut": cut.value, "top": top.value, "records": rec.value, "bytes": by.value,
                 "smem": sm.value, "model_cycles": cyc.value}
 
+    def set_lane_rhs_per_lane(self, precision: int, rhs_per_lane: int) -> None:
+        """How many right-hand sides each lane of the plain lane solve carries (1 or 2)."""
+        _check(lib().yb_factor_set_lane_rhs_per_lane(self._h, precision, rhs_per_lane))
+
     def lane_info(self, precision: int = FP64) -> dict:
         """The lane solve's layout: slots, pages, peaks of live values, shared memory per block,
         warps per block, domains, top rows and partial values per block."""
         v = np.zeros(12, np.int64)
         _check(lib().yb_factor_lane_info(self._h, precision, ptr(v)))
         keys = ("slots", "pages", "page_bytes", "fwd_live", "bwd_live", "entries", "smem", "warps", "domains", "top",
-                "partials")
+                "partials", "rpl")
         return dict(zip(keys, (int(a) for a in v)))
 
     def set_lane(self, precision: int, warps: int, page_bytes: int = 0) -> None:
