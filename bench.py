@@ -13,7 +13,7 @@ Our arm times, on the device with CUDA events, K steps of the solve with inputs 
 headline), the same block in blocks of 64, 256 and 1,024 columns (`modes_by_width`), the solve
 through the host-array C ABI call with pinned host buffers, copies included (`e2e`), and the
 other configurations of the path (`workloads`: the N-1 screening batch, the flow-loss adjoint, the
-complex multi-network batch). `--impl reference` times the reference's CPU solve path (the
+complex multi-network batch, the Newton-Raphson Jacobian's LU solve). `--impl reference` times the reference's CPU solve path (the
 oracle's restatement of ybus_sparse's `par_solve_many`) on all host cores, loading no GPU library.
 """
 from __future__ import annotations
@@ -53,8 +53,8 @@ def parse():
     p.add_argument("--no-extras", action="store_true",
                    help="time the headline modes only (no block widths, workloads or comparison): for profiling")
     p.add_argument("--rhs", type=int, default=0, help="solve only the first RHS (a smaller case for profiling)")
-    p.add_argument("--workload", default="ptdf", choices=["ptdf", "n1", "adjoint", "complex"],
-                   help="ptdf: the headline PTDF block with the other workloads as extra keys; n1, adjoint, complex: "
+    p.add_argument("--workload", default="ptdf", choices=["ptdf", "n1", "adjoint", "complex", "jacobian"],
+                   help="ptdf: the headline PTDF block with the other workloads as extra keys; n1, adjoint, complex, jacobian: "
                         "one of the other workloads alone, one JSON line")
     return p.parse_args()
 
@@ -348,7 +348,45 @@ def workload_complex(gpu, steps: int, warm: int, rank: int, world: int, device: 
                        "split": f"networks by LPT over {world} GPU(s)"}, "modes": modes}
 
 
-WORKLOADS = {"n1": workload_n1, "adjoint": workload_adjoint, "complex": workload_complex}
+def workload_jacobian(gpu, steps: int, warm: int, rank: int, world: int, device: int) -> dict:
+    """The Newton-Raphson Jacobian of the 10,000-bus complex network (order 17,998, AMD LU on the
+    host; the reference's other matrix for its GPU survey): 4,096 right-hand sides, device arrays,
+    FP64, split over the ranks by columns."""
+    import torch
+
+    from ybus_b200 import FP64, GpuFactor, configs, replicas
+    sysj = configs.jacobian_system()
+    mine = replicas.shard(sysj.rhs.shape[0], rank, world)
+    rhs = np.ascontiguousarray(sysj.rhs[mine.start:mine.stop])
+    factor = GpuFactor.from_lu(gpu, sysj.lu)
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    # a stream of our own: the legacy default stream's handle is 0, which the C ABI reads as the
+    # library's own stream, and the events must be on the stream the solves run on
+    stream = torch.cuda.Stream()
+
+    def run():
+        factor.solve_many_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], FP64, stream.cuda_stream)
+
+    for _ in range(warm):
+        run()
+    torch.cuda.synchronize()
+    replicas.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    factor.check_error()
+    ms = replicas.max_over_ranks(e0.elapsed_time(e1) / steps)
+    return {"metric": "Newton-Raphson Jacobian RHS solved/s, device arrays", "value": sysj.rhs.shape[0] / (ms / 1e3),
+            "unit": "RHS/s", "higher_is_better": True, "ms_per_step": ms,
+            "config": {"n_bus": sysj.n_bus, "order": int(sysj.lu.n), "lu_entries": int(sysj.lu.l.idx.size + sysj.lu.u.idx.size),
+                       "rhs": int(sysj.rhs.shape[0]), "split": f"columns over {world} GPU(s)"}}
+
+
+WORKLOADS = {"n1": workload_n1, "adjoint": workload_adjoint, "complex": workload_complex, "jacobian": workload_jacobian}
 
 
 def init_ranks():

@@ -1,0 +1,50 @@
+"""The Newton-Raphson Jacobian's LU solve on the GPU (the reference's second matrix for its GPU
+survey, ybus_powerflow/examples/cuda_survey.rs:213-235, through `GpuFactor::from_lu`): the 10,000-
+bus network's Jacobian (order 17,998) factored by AMD LU on the host, 4,096 right-hand sides
+solved and transposed-solved through the C ABI, against the oracle's LU solves (lu.rs:640-649,
+770-785, 506-533) at the reference's bar."""
+import numpy as np
+import pytest
+
+import oracle.oracle as orc
+from fixtures import worst_relative_difference
+from ybus_b200 import FP64, GpuFactor, configs
+
+pytestmark = pytest.mark.gpu
+
+BAR = 1e-12
+
+
+@pytest.fixture(scope="module")
+def system():
+    return configs.jacobian_system()
+
+
+def test_jacobian_solves_match_the_oracle(gpu, system):
+    import torch
+    factor = GpuFactor.from_lu(gpu, system.lu)
+    rhs = system.rhs
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    factor.solve_many_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], FP64, None)
+    gpu.synchronize()
+    factor.check_error()
+    xs = x.cpu().numpy()
+    sample = np.arange(0, rhs.shape[0], 97)
+    assert worst_relative_difference(xs[sample], orc.solve_many_lu(system.lu, rhs[sample], threads=8)) < BAR
+    # every 17th solution's relative residual against the matrix itself, against the oracle's own
+    # solution's: the LU factor's threshold pivoting sets both (up to 2.3e-10 here), and solutions
+    # that differ by rounding move it by a small factor (1.6 at most measured)
+    p, i, v = system.jacobian.to_csr().arrays()
+    cols = np.arange(0, rhs.shape[0], 17)
+    cpu = orc.solve_many_lu(system.lu, rhs[cols], threads=8)
+    for k, c in zip(cols, cpu):
+        mine, theirs = orc.relative_residual(p, i, v, xs[k], rhs[k]), orc.relative_residual(p, i, v, c, rhs[k])
+        assert mine <= 4.0 * theirs + 1e-13, (k, mine, theirs)
+
+
+def test_jacobian_transposed_solves_match_the_oracle(gpu, system):
+    factor = GpuFactor.from_lu(gpu, system.lu)
+    rhs = system.rhs[:256]
+    cpu = orc.solve_many_lu(system.lu, rhs, threads=8, transpose=True)
+    assert worst_relative_difference(factor.solve_many_transpose(rhs), cpu) < BAR

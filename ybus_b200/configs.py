@@ -14,6 +14,10 @@ slack); seeds are `grids.SEED_BASE + configuration number`.
 4. The 10,000-bus grid; 1,024 injection scenarios as in 3; branch limits U[0.5, 2.0].
 5. 16 complex Ybus networks of N log-uniform in [500, 70,000] buses (1.3 branches per bus, r/x in
    [0.1, 0.5], shunt b in [0, 0.05]); 128 complex right-hand sides N(0,1) + iN(0,1) each.
+
+Beside them, the Newton-Raphson Jacobian of a complex network (the reference's other matrix for its
+GPU survey, ybus_powerflow/examples/cuda_survey.rs:213-235): bus 0 the slack, a fifth of the
+others PV, voltages near flat, LU-factored with AMD as the survey does.
 """
 from __future__ import annotations
 
@@ -120,3 +124,69 @@ def complex_network(n_bus: int, index: int, count: int = COMPLEX_RHS, seed: int 
     rng = np.random.default_rng(seed * 100 + index)
     b = rng.standard_normal((count, int(n_bus))) + 1j * rng.standard_normal((count, int(n_bus)))
     return ComplexNetwork(int(n_bus), a, host.lu(a, host.COLAMD), b)
+
+
+JACOBIAN_PV_SHARE, JACOBIAN_RHS = 0.2, 4096
+
+
+@dataclasses.dataclass
+class JacobianSystem:
+    n_bus: int
+    pv: np.ndarray  # int64: the PV buses
+    pq: np.ndarray  # int64: the PQ buses
+    voltage: np.ndarray  # complex128 [n_bus]
+    ybus: object  # scipy CSC, complex128
+    jacobian: host.Matrix  # CSC, float64, (len(pv) + 2 len(pq)) square
+    lu: host.HostLu
+    rhs: np.ndarray  # float64 (count, order)
+
+
+def power_injections(ybus, v: np.ndarray) -> np.ndarray:
+    """S = V conj(Ybus V) at every bus (`newtonpf`'s mismatch without the schedule)."""
+    return v * np.conj(ybus @ v)
+
+
+def jacobian_matrix(ybus, v: np.ndarray, pv: np.ndarray, pq: np.ndarray):
+    """The Newton-Raphson Jacobian at voltages `v` (`AcModel::jacobian`, ybus_powerflow/src/ac.rs:
+    1134-1150): the real power at the PV and PQ buses and the reactive power at the PQ buses
+    differentiated by the angles at the PV and PQ buses and the magnitudes at the PQ buses, in that
+    order, from the published derivatives of S = V conj(Ybus V):
+    dS/dtheta = j diag(V) conj(diag(I) - Ybus diag(V)) and
+    dS/d|V| = diag(V) conj(Ybus diag(V/|V|)) + conj(diag(I)) diag(V/|V|), I = Ybus V.
+    Returns a scipy CSC matrix."""
+    import scipy.sparse as sp
+    i = ybus @ v
+    dv = sp.diags(v)
+    dn = sp.diags(v / np.abs(v))
+    ds_da = 1j * dv @ np.conj(sp.diags(i) - ybus @ dv)
+    ds_dm = dv @ np.conj(ybus @ dn) + np.conj(sp.diags(i)) @ dn
+    pvpq = np.concatenate([pv, pq])
+    ds_da, ds_dm = sp.csr_matrix(ds_da), sp.csr_matrix(ds_dm)
+    j11 = ds_da[pvpq][:, pvpq].real
+    j12 = ds_dm[pvpq][:, pq].real
+    j21 = ds_da[pq][:, pvpq].imag
+    j22 = ds_dm[pq][:, pq].imag
+    return sp.bmat([[j11, j12], [j21, j22]], format="csc")
+
+
+def jacobian_system(n_bus: int = N_BUS, count: int = JACOBIAN_RHS, seed: int = grids.SEED_BASE + 7) -> JacobianSystem:
+    """The Jacobian of a seeded complex network of `n_bus` buses, its AMD LU on the host and
+    `count` right-hand sides N(0, 1)."""
+    import scipy.sparse as sp
+    gc = grids.make_complex_grid(int(n_bus), seed)
+    r, c, v = grids.ybus_triplets(gc)
+    ybus = sp.csc_matrix((v, (r, c)), shape=(n_bus, n_bus))
+    rng = np.random.default_rng(seed)
+    others = np.arange(1, n_bus)
+    pv = np.sort(rng.choice(others, int(round(JACOBIAN_PV_SHARE * others.size)), replace=False)).astype(np.int64)
+    pq = np.setdiff1d(others, pv).astype(np.int64)
+    vm = rng.uniform(0.95, 1.05, n_bus)
+    va = rng.normal(0.0, 0.05, n_bus)
+    va[0] = 0.0
+    voltage = vm * np.exp(1j * va)
+    jm = jacobian_matrix(ybus, voltage, pv, pq).tocoo()
+    m = jm.shape[0]
+    jac = host.Matrix.from_triplets(m, m, jm.row.astype(np.int64), jm.col.astype(np.int64), jm.data, by_rows=False)
+    lu = host.lu(jac, host.AMD)
+    rhs = np.random.default_rng(seed + 1).standard_normal((count, m))
+    return JacobianSystem(int(n_bus), pv, pq, voltage, ybus, jac, lu, rhs)
