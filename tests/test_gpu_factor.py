@@ -171,7 +171,8 @@ def test_repeated_solves_give_the_same_bits(gpu):
 
 @pytest.mark.parametrize("pinned", [False, True])
 def test_host_array_solve_overlaps_many_chunks(gpu, pinned):
-    # 5,000 right-hand sides pass through the copy pipeline in 8 chunks, twice round its 4 slots
+    # 5,000 right-hand sides pass through the copy pipeline in chunks of 625 and a halving tail
+    # (625, 320, 256, 49): 10 chunks, more than twice round its 4 slots
     import torch
     chol = host.cholesky(random_spd(300, 3, 7))
     rhs = right_hand_sides(300, 5000, 29)
@@ -181,7 +182,7 @@ def test_host_array_solve_overlaps_many_chunks(gpu, pinned):
         tb, tx = torch.from_numpy(b).pin_memory(), torch.zeros(out.shape, dtype=torch.float64).pin_memory()
         b, out = tb.numpy(), tx.numpy()
     factor.solve_many_into(b, out)
-    assert factor.timings().blocks == 8
+    assert factor.timings().blocks == 10
     sample = np.arange(0, 5000, 41)
     assert worst_relative_difference(out[sample], orc.solve_many(chol, rhs[sample])) < BAR
     again = np.zeros_like(out)

@@ -1133,12 +1133,19 @@ extern "C" int32_t yb_solve_many(yb_factor *f, const double *rhs, int64_t count,
       f->timings.download += down * 1e-3;
       f->timings.blocks += 1;
     };
+    // The uploads are the pipeline's bottleneck (the host link), so a call costs every upload plus
+    // the last chunk's solve and download: over the last two chunks' worth of columns the chunks
+    // halve, down to 256 columns, so that tail is short.
+    const int64_t tail_min = std::min<int64_t>(chunk, 256);
+    auto next_cols = [&](int64_t left) -> int64_t {
+      if (left > 2 * chunk || left <= tail_min) return std::min(chunk, left);
+      return std::min(chunk, std::max(tail_min, (left / 2 + 31) / 32 * 32));
+    };
     int64_t c = 0;
     try {
-      for (int64_t k0 = 0; k0 < count; k0 += chunk, ++c) {
+      for (int64_t k0 = 0, cols = next_cols(count); k0 < count; k0 += cols, cols = next_cols(count - k0), ++c) {
         const int slot = (int)(c % S);
         finish(slot);  // the slot's previous chunk is back: its buffers are free
-        const int64_t cols = std::min(chunk, count - k0);
         const size_t bytes = (size_t)(n * cols) * sizeof(double);
         double *db = f->dev_b.get() + slot * slot_values, *dx = f->dev_x.get() + slot * slot_values;
         cudaEvent_t *e = pipe.ev[slot];
