@@ -161,10 +161,12 @@ int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_t *tile_wid
                               int64_t *records, int64_t *bytes, int64_t *smem_bytes, double *model_cycles);
 /* No ybus counterpart: the autotuner. Times the solve of `count` right-hand sides for a precision
  * over the domain solve's shapes (warps 8/12/16, pages 1536/2048 bytes, 2 or 3 pages in flight, the
- * widest tile that fits and half of it) and the lane solve's (4, 6 or 8 warps per block, when the
- * factor admits a lane layout) and keeps the fastest for the factor, for solves of about that many
- * right-hand sides. config receives {kind, tile width (0 for the lane solve), warps, ring, page
- * bytes} and best_ms its time (either may be NULL). With nothing to time, the configuration is left
+ * widest tile that fits and half of it), the global-scratch solve's (tile widths 1 to 32, 256 or
+ * 512 threads) and the lane solve's (4, 6 or 8 warps per block, one or two right-hand sides per
+ * lane, when the factor admits a lane layout) and keeps the fastest for the factor, for solves of
+ * about that many right-hand sides. config receives {kind, tile width (0 for the lane solve),
+ * warps, ring, page bytes} (for the global-scratch solve: {kind, tile width, warps, blocks per SM,
+ * 0}) and best_ms its time (either may be NULL). With nothing to time, the configuration is left
  * as it was. */
 int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t count, int32_t *config, double *best_ms);
 /* No ybus counterpart, diagnostics on the host (no GPU needed): the lane solve's layout for a

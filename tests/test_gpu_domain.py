@@ -12,7 +12,7 @@ from ybus_b200 import FP32, FP64, GpuFactor, grids, host
 pytestmark = pytest.mark.gpu
 
 BAR = 1e-12
-DOMAIN, LANE = 4, 5
+DOMAIN, LANE, GLOBAL = 4, 5, 2
 
 
 @pytest.mark.parametrize("tile", [1, 2, 4, 8, 16])
@@ -105,6 +105,9 @@ def test_autotune_keeps_the_fastest_domain_shape_and_the_same_solutions(gpu):
             assert best["warps"] in (8, 12, 16) and best["ring"] in (2, 3)
             assert best["page_bytes"] in (1536, 2048) and best["tile"] >= 1
             assert factor.domain_info(prec)["tile"] == best["tile"]
+        elif best["kind"] == GLOBAL:
+            assert best["tile"] in (1, 2, 4, 8, 16, 32) and best["warps"] in (8, 16)
+            assert factor.tile(prec)[:2] == (best["tile"], 32 * best["warps"])
         else:
             assert best["kind"] == LANE and best["warps"] in (4, 6, 8) and best["tile"] == 0
             assert factor.lane_info(prec)["warps"] == best["warps"]
@@ -129,6 +132,6 @@ def test_autotune_on_a_large_block_of_a_grid_keeps_the_faster_solve(gpu):
     chol = host.cholesky(host.Matrix.from_triplets(2000, 2000, r, c, v).select(keep, keep))
     factor = GpuFactor.from_cholesky(gpu, chol)
     best = factor.autotune(FP64, 8192)
-    assert best["kind"] in (DOMAIN, LANE) and best["ms"] > 0
+    assert best["kind"] in (DOMAIN, LANE, GLOBAL) and best["ms"] > 0
     rhs = np.random.default_rng(9).standard_normal((300, chol.n))
     assert worst_relative_difference(factor.solve_many(rhs), orc.solve_many(chol, rhs)) < BAR

@@ -48,3 +48,13 @@ def test_jacobian_transposed_solves_match_the_oracle(gpu, system):
     rhs = system.rhs[:256]
     cpu = orc.solve_many_lu(system.lu, rhs, threads=8, transpose=True)
     assert worst_relative_difference(factor.solve_many_transpose(rhs), cpu) < BAR
+
+
+def test_the_autotuner_finds_a_faster_solve_for_the_jacobian(gpu, system):
+    # the Jacobian's LU admits no lane layout and its domain tiles hold one column in shared
+    # memory; the autotuner also times the global-scratch solve and keeps what is fastest
+    factor = GpuFactor.from_lu(gpu, system.lu)
+    best = factor.autotune(FP64, 1024)
+    assert best["ms"] > 0
+    rhs = system.rhs[:300]
+    assert worst_relative_difference(factor.solve_many(rhs), orc.solve_many_lu(system.lu, rhs, threads=8)) < BAR

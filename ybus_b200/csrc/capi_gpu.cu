@@ -1647,6 +1647,19 @@ extern "C" int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t c
             time_config(run);
           }
         }
+    // the global-scratch solve (every factor admits it: working vectors in global memory, the
+    // fallback for factors whose tiles do not fit shared memory) at each tile width and two block
+    // sizes
+    for (int w : {1, 2, 4, 8, 16, 32})
+      for (int threads : {256, 512}) {
+        TileConfig run = saved;
+        run.kind = kTileGlobal, run.width = w, run.threads = threads, run.blocks_per_sm = 2;
+        try {
+          time_config(run);
+        } catch (const host::Error &) {
+          continue;
+        }
+      }
     // the lane solve, when the factor admits it, at 4, 6 and 8 warps per block, with one and with
     // two right-hand sides per lane
     for (int rpl : {1, 2})
@@ -1661,7 +1674,9 @@ extern "C" int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t c
     cudaEventDestroy(e1);
     t = std::isfinite(best_time) ? best : saved;
     if (config) {
-      if (t.kind == kTileLane) {
+      if (t.kind == kTileGlobal) {
+        config[0] = t.kind, config[1] = t.width, config[2] = t.threads / 32, config[3] = t.blocks_per_sm, config[4] = 0;
+      } else if (t.kind == kTileLane) {
         DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, t, t.lane_rpl, s) : lane_pick<float>(f, t, t.lane_rpl, s);
         config[0] = t.kind, config[1] = 0, config[2] = t.lane_warps, config[3] = kLaneRing, config[4] = d->page_bytes;
       } else {
