@@ -8,6 +8,16 @@ FWD_ROW0, FWD_PRE1, BWD_ROW0, BWD_PRE1 = 0, 5, 9, 14
 FWD_ROWN, FWD_MORE, BWD_ROWN, BWD_BEGIN, BWD_MORE, BWD_END = range(18, 24)
 PREFETCH, PHASE, TOP_SUM, FLUSH, IMPORT, BARRIER, END, PAGE_END = range(24, 32)
 RING, BATCH = 8, 4
+PAGE_RING, BARRIERS = 2, 4
+TOP_SUMS, TOP_LOAD, TOP_ROW, TOP_ROW_MORE = range(4)  # the modes of a TOP_SUM record
+
+
+def warp_bytes(lay):
+    """A warp's shared bytes (lane_warp_bytes_of): slots, the prefetch ring, the page ring and its
+    barriers, rounded to 128; the dense top's block-wide offsets count in them."""
+    row = 32 * lay["value_bytes"] * lay.get("rpl", 1)
+    b = lay["slots"] * row + RING * row + PAGE_RING * lay["page_bytes"] + PAGE_RING * 8
+    return (b + 127) // 128 * 128
 
 
 def records(lay, warp):
@@ -38,12 +48,13 @@ def records(lay, warp):
             pos += 16 + ((count * entry + 15) & ~15)
 
 
-def warp_steps(lay, warp, work, partial, lanes):
-    """Runs one warp's records, yielding at each block barrier."""
+def warp_steps(lay, warp, work, partial, lanes, lives):
+    """Runs one warp's records, yielding at each block barrier; lives[w] is warp w's slots."""
     vb = lay["value_bytes"]
     ftype = np.float64 if vb == 8 else np.float32
     row = 32 * vb * lay.get("rpl", 1)  # a slot or row: 32 lanes of rpl values
-    live = np.zeros((lay["slots"], lanes))
+    live = lives[warp]
+    wb = warp_bytes(lay)
     ring = np.full((RING, lanes), np.nan)
     pending = np.zeros(RING, bool)  # a prefetched row not read yet
     z = None
@@ -102,9 +113,25 @@ def warp_steps(lay, warp, work, partial, lanes):
             assert not pending.any(), "a phase that leaves prefetched rows unread"
             ring[:] = np.nan
         elif kind == TOP_SUM:
-            assert 0 <= w < work.shape[0], "a row outside the work array"
-            for k in words:
-                work[w] = work[w] + partial[k // row]
+            mode = int(tail[:4].view(np.uint32)[0])
+            if mode == TOP_SUMS:
+                assert 0 <= w < work.shape[0], "a row outside the work array"
+                for k in words:
+                    work[w] = work[w] + partial[k // row]
+            elif mode == TOP_LOAD:
+                for p, o in zip(words, offs):
+                    assert 2 <= o // row < lay["slots"], "a top value loaded into the zero or the sink slot"
+                    live[o // row] = work[p // row]
+            else:
+                assert mode in (TOP_ROW, TOP_ROW_MORE), f"unknown top mode {mode}"
+                assert 0 <= w < work.shape[0], "a row outside the work array"
+                acc = np.zeros(lanes) if mode == TOP_ROW else work[w].copy()
+                for v, a in zip(vals, offs):
+                    owner, rest = divmod(int(a), wb)
+                    assert 0 <= owner < lay["warps"] and rest % row == 0 and 2 <= rest // row < lay["slots"], \
+                        "a dense top offset outside every warp's slots"
+                    acc = acc + v * lives[owner][rest // row]
+                work[w] = acc
         elif kind == FLUSH:
             for k, o in zip(words, offs):
                 partial[k // row] = live[o // row]
@@ -128,8 +155,9 @@ def run(lay, n, rhs):
     work = np.zeros((n, lanes))
     work[lay["in_pos"]] = rhs.T
     partial = np.zeros((max(lay["partials"], 1), lanes))
-    warps = [warp_steps(lay, w, work, partial, lanes) for w in range(lay["warps"])]
-    for _ in range(4):  # the epochs around the three barriers
+    lives = [np.zeros((lay["slots"], lanes)) for _ in range(lay["warps"])]
+    warps = [warp_steps(lay, w, work, partial, lanes, lives) for w in range(lay["warps"])]
+    for _ in range(BARRIERS + 1):  # the epochs around the barriers
         for g in warps:
             next(g, None)
     return work[lay["out_pos"]].T.copy()

@@ -28,7 +28,11 @@ def test_lane_records_solve_the_fixture(page, fill, warps):
     lay = host.lane_layout(chol, 8, page, warps=warps)
     d = worst_relative_difference(run(lay, chol.n, rhs), orc.solve_many(chol, rhs))
     assert d < 1e-12, f"page {page} warps {warps}: {d:e}"
-    assert lay["fwd_entries"] == lay["bwd_entries"] == int(np.asarray(chol.l.ptr)[-1]) - chol.n
+    # every entry of L below its diagonal in each sweep's records, but a dense top's (its rows
+    # are then one dense map, not substitution records)
+    assert lay["fwd_entries"] == lay["bwd_entries"] <= int(np.asarray(chol.l.ptr)[-1]) - chol.n
+    if warps == 1:
+        assert lay["fwd_entries"] == int(np.asarray(chol.l.ptr)[-1]) - chol.n
 
 
 def test_lane_records_in_fp32_are_close():

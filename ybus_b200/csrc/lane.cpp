@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <tuple>
 #include <vector>
 
 #include "plan.hpp"
@@ -149,6 +150,26 @@ template <class T> struct PageWriter {
       pos += bytes_of(take);
       done += take;
     }
+  }
+  // The dense top's records (kLaneTopSum with a mode in the header's third word): entries {val or
+  // a 32-bit word, offset}, split as the pages need, the first record of mode `first`, the rest of
+  // mode `more`; returns the blob positions of the entries' offset fields, in order.
+  std::vector<size_t> moded(uint32_t word, uint32_t first, uint32_t more, const std::vector<std::pair<T, uint32_t>> &entries,
+                            const uint32_t *words) {
+    std::vector<size_t> at_offset;
+    size_t done = 0;
+    while (done < entries.size()) {
+      const size_t take = std::min(most_entries(), entries.size() - done);
+      room(bytes_of(take));
+      const uint32_t mode[2] = {done == 0 ? first : more, 0};
+      put(0, kLaneTopSum, (uint32_t)take, word, mode, 8);
+      entries_at(at(), entries, words, done, take);
+      for (size_t e = 0; e < take; ++e)
+        at_offset.push_back(blob.size() - (size_t)page_bytes + pos + 16 + e * kEntry + sizeof(T));
+      pos += bytes_of(take);
+      done += take;
+    }
+    return at_offset;
   }
   // Records with entries {a 32-bit word in val's place, offset}, split as the pages need.
   void words(uint32_t kind, uint32_t self, const std::vector<std::pair<T, uint32_t>> &entries,
@@ -418,6 +439,90 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   const uint32_t row_bytes = 32u * (uint32_t)sizeof(T) * (uint32_t)rpl;  // a live slot, or a work or partial row
   auto off = [&](int32_t s) { return (uint32_t)s * row_bytes; };
   auto self_of = [&](int32_t s) { return (uint32_t)s * row_bytes / 16; };  // headers hold slot offsets / 16
+  // The dense top: with several warps and a top of 2 to kLaneDenseTopMost rows, its forward and
+  // backward substitution is one linear map x_T = M r_T from the top rows' right-hand sides (after
+  // the partial sums) to their solutions; M is that substitution applied to the identity, in FP64
+  // here, kept when its condition (||M||inf ||M^-1||inf) is at most kLaneDenseTopCondition.
+  // Between the second and third barriers every warp loads its share of r_T (the top rows
+  // `share` at a time, in position order) into its slots 2..; between the third and fourth it
+  // forms its share of x_T from every warp's slots, so the top no longer runs as warp 0's chain.
+  const int32_t t = n - top0;
+  const int32_t share = warps > 1 ? (t + warps - 1) / warps : 0;
+  std::vector<double> dense_m;
+  bool dense = warps > 1 && t > 1 && t <= kLaneDenseTopMost && 2 + share <= std::min(max_slots, 255);
+  if (dense) {
+    std::vector<int32_t> tidx(n, -1);
+    for (int32_t p = top0; p < n; ++p) tidx[at[p]] = p - top0;
+    dense_m.assign((size_t)t * t, 0.0);
+    std::vector<double> acc_t(t), z(t), x(t);
+    for (int32_t e = 0; e < t && dense; ++e) {
+      std::fill(acc_t.begin(), acc_t.end(), 0.0);
+      for (int32_t p = 0; p < t; ++p) {
+        const int32_t j = at[top0 + p];
+        z[p] = ((p == e ? 1.0 : 0.0) + acc_t[p]) * frow[j].dinv;
+        for (int32_t q = col_ptr[j]; q < col_ptr[j + 1]; ++q) {
+          const int32_t r = tidx[col_row[q]];
+          if (r < 0) dense = false;  // a top row updates no row below the top
+          else acc_t[r] -= col_val[q] * z[p];
+        }
+      }
+      for (int32_t p = t - 1; p >= 0; --p) {
+        const int32_t j = at[top0 + p];
+        double v = z[p];
+        for (int32_t q = brow[j].p0; q < brow[j].p1; ++q) {
+          const int32_t c = tidx[plan.bwd.col[q]];
+          if (c < 0) dense = false;
+          else v -= (double)plan.bwd.val[q] * x[c];
+        }
+        x[p] = v * brow[j].dinv;
+      }
+      for (int32_t i = 0; i < t; ++i) dense_m[(size_t)i * t + e] = x[i];
+    }
+    if (dense) {
+      // ||M^-1||inf by Gauss-Jordan elimination with partial pivoting on a copy
+      std::vector<double> a(dense_m), inv((size_t)t * t, 0.0);
+      for (int32_t i = 0; i < t; ++i) inv[(size_t)i * t + i] = 1.0;
+      for (int32_t k = 0; k < t && dense; ++k) {
+        int32_t piv = k;
+        for (int32_t i = k + 1; i < t; ++i)
+          if (std::abs(a[(size_t)i * t + k]) > std::abs(a[(size_t)piv * t + k])) piv = i;
+        if (a[(size_t)piv * t + k] == 0.0) {
+          dense = false;
+          break;
+        }
+        if (piv != k)
+          for (int32_t j = 0; j < t; ++j) {
+            std::swap(a[(size_t)k * t + j], a[(size_t)piv * t + j]);
+            std::swap(inv[(size_t)k * t + j], inv[(size_t)piv * t + j]);
+          }
+        const double d = a[(size_t)k * t + k];
+        for (int32_t j = 0; j < t; ++j) a[(size_t)k * t + j] /= d, inv[(size_t)k * t + j] /= d;
+        for (int32_t i = 0; i < t; ++i) {
+          if (i == k) continue;
+          const double f = a[(size_t)i * t + k];
+          if (f == 0.0) continue;
+          for (int32_t j = 0; j < t; ++j) a[(size_t)i * t + j] -= f * a[(size_t)k * t + j], inv[(size_t)i * t + j] -= f * inv[(size_t)k * t + j];
+        }
+      }
+      auto norm = [&](const std::vector<double> &m) {
+        double most = 0;
+        for (int32_t i = 0; i < t; ++i) {
+          double row = 0;
+          for (int32_t j = 0; j < t; ++j) row += std::abs(m[(size_t)i * t + j]);
+          most = std::max(most, row);
+        }
+        return most;
+      };
+      if (dense) {
+        lay.top_condition = norm(dense_m) * norm(inv);
+        dense = std::isfinite(lay.top_condition) && lay.top_condition <= kLaneDenseTopCondition;
+      }
+    }
+  }
+  lay.dense_top = dense;
+  // the dense rows' offsets into other warps' slots, patched when the slot count is known:
+  // (blob position, warp, slot)
+  std::vector<std::tuple<size_t, int32_t, int32_t>> patches;
   std::vector<std::pair<T, uint32_t>> entries;
   std::vector<uint32_t> words;
   std::vector<int32_t> acc(n, -1), xslot(n, -1), readers(n, 0);
@@ -492,7 +597,15 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
       pw.sums((uint32_t)work_of[j] * row_bytes, entries, words);
     }
     pw.simple(kLaneBarrier);
-    if (w == 0 && top0 < n) {  // the top, forward then backward
+    if (dense) {  // this warp's share of r_T into its slots 2..
+      entries.clear();
+      words.clear();
+      for (int32_t i = w * share; i < std::min(t, (w + 1) * share); ++i) {
+        entries.push_back({T(0), off(2 + i - w * share)});
+        words.push_back((uint32_t)work_row[top0 + i] * row_bytes);
+      }
+      if (!entries.empty()) pw.moded(0, kTopLoad, kTopLoad, entries, words.data());
+    } else if (w == 0 && top0 < n) {  // the top, forward then backward
       Slots slots;
       pw.phase(top0, n - top0, false);
       forward_rows(pw, slots, top0, n - 1);
@@ -504,6 +617,14 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
       backward_rows(pw, bslots, top0, n - 1);
       peak_b = std::max(peak_b, bslots.peak);
     }
+    pw.simple(kLaneBarrier);
+    if (dense)  // this warp's share of x_T, each a dense row over every warp's slots, into the output
+      for (int32_t i = w * share; i < std::min(t, (w + 1) * share); ++i) {
+        entries.clear();
+        for (int32_t j = 0; j < t; ++j) entries.push_back({(T)dense_m[(size_t)i * t + j], 0u});
+        const auto at_off = pw.moded((uint32_t)work_row[top0 + i] * row_bytes, kTopRow, kTopRowMore, entries, nullptr);
+        for (int32_t j = 0; j < t; ++j) patches.push_back({at_off[(size_t)j], j / share, 2 + j % share});
+      }
     pw.simple(kLaneBarrier);
     {  // backward domains in reverse, each starting with the top solutions it reads
       Slots slots;
@@ -538,8 +659,18 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   lay.fwd_live = peak_f;
   lay.bwd_live = peak_b;
   lay.slots = 2 + std::max(peak_f, peak_b);
+  if (dense) lay.slots = std::max(lay.slots, 2 + share);
   if (lay.slots > std::min(max_slots, 255))
     throw host::Error(host::kTooLarge, "the lane solve would keep more live values than its shared memory holds");
+  {  // the dense rows' block-wide offsets: warp w's slot s at w * (a warp's shared bytes) + s * row
+    const size_t wb = lane_warp_bytes_of((int32_t)sizeof(T), lay.slots, kLaneRing, page_bytes, rpl);
+    for (const auto &[at_blob, warp, slot] : patches) {
+      const size_t v = (size_t)warp * wb + (size_t)slot * row_bytes;
+      if (v > UINT32_MAX) throw host::Error(host::kTooLarge, "a dense top offset does not fit 32 bits");
+      const uint32_t o = (uint32_t)v;
+      std::memcpy(lay.blob.data() + at_blob, &o, 4);
+    }
+  }
   lay.in_pos.resize(n);
   lay.out_pos.resize(n);
   for (int32_t i = 0; i < n; ++i) {

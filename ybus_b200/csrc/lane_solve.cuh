@@ -28,8 +28,6 @@
 
 namespace yb {
 
-constexpr int kLaneBarriers = 3;             // block barriers in every warp's stream
-constexpr int kLaneRing = 2;                 // pages in flight per warp (a power of two)
 constexpr int kLaneMaxWarps = 8;             // warps per block at most
 
 struct LaneArgs {
@@ -44,13 +42,10 @@ struct LaneArgs {
                      // issued, so that warp's bounded wait runs out (-1: none)
 };
 
-// A warp's shared memory: live slots, the prefetch ring, the page ring and its barriers, with rpl
-// right-hand sides per lane (a slot and a ring row hold 32 * rpl values).
+// A warp's shared memory (lane_warp_bytes_of in plan.hpp) for values of type T.
 template <class T>
 __host__ __device__ inline size_t lane_warp_bytes(int32_t slots, int32_t ring, int32_t page_bytes, int32_t rpl = 1) {
-  const size_t row = (size_t)32 * sizeof(T) * rpl;
-  const size_t b = (size_t)slots * row + (size_t)kLaneRows * row + (size_t)ring * page_bytes + (size_t)ring * 8;
-  return (b + 127) & ~(size_t)127;
+  return lane_warp_bytes_of((int32_t)sizeof(T), slots, ring, page_bytes, rpl);
 }
 
 template <int BYTES> __device__ __forceinline__ void cp_async_lane(void *dst, const void *src) {
@@ -328,6 +323,45 @@ __global__ void __launch_bounds__(kLaneMaxWarps * 32, R == 1 ? 3 : 2) lane_solve
         __threadfence();  // the rows this lane stored are what the phase's copies read
         break;
       case kLaneTopSum: {  // the row and up to four partials in flight at a time, added in order
+        if (h.z == kTopLoad) {  // the dense top: this warp's share of its right-hand sides into slots
+          for (uint32_t c = 0; c < count; c += 4) {
+            Lv<T, R> r[4];
+            uint32_t o[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              T v;
+              uint32_t w;
+              lane_entry(e + min(c + q, count - 1) * E, v, w, o[q]);
+              r[q] = lv_load<T, R>(w_lane + w);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (c + q < count) lv_st<T, R>(live + o[q], r[q]);
+          }
+          break;
+        }
+        if (h.z == kTopRow || h.z == kTopRowMore) {  // a dense top row over every warp's slots
+          Lv<T, R> acc = h.z == kTopRow ? lv_zero<T, R>() : lv_load<T, R>(x_lane + h.y);
+          const uint32_t lane_off = (uint32_t)lane * VB;  // the offsets are this block's, lane 0's
+          for (uint32_t c = 0; c < count; c += 4) {
+            T v[4];
+            Lv<T, R> r[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              uint32_t w, o;
+              lane_entry(e + min(c + q, count - 1) * E, v[q], w, o);
+              r[q] = lv_ld<T, R>(lane_off + o);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (c + q < count) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) acc.v[k] = fma(v[q], r[q].v[k], acc.v[k]);
+              }
+          }
+          lv_store<T, R>(x_lane + h.y, acc);
+          break;
+        }
         uint8_t *row = w_lane + h.y;
         Lv<T, R> acc = lv_load<T, R>(row);
         for (uint32_t c = 0; c < count; c += 4) {

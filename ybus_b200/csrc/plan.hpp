@@ -167,7 +167,10 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
 //   kLanePhase: a new run of rows: earlier copies are finished and this lane's stores are visible
 //     to its copies.
 //   kLaneFlush: per entry, the partial row `word` takes slot `offset`, which is zeroed.
-//   kLaneTopSum: the work row `word` += the partial rows of its entries' words, in order.
+//   kLaneTopSum: the work row `word` += the partial rows of its entries' words, in order (mode
+//     kTopSums); mode kTopLoad: per entry, slot `offset` takes the work row `word`; modes kTopRow
+//     and kTopRowMore: the output row `word` = (0, or its value so far) + val * the value at the
+//     block-wide shared offset `offset` (another warp's slot), per entry in order.
 //   kLaneImport: per entry, slot `offset` takes the work row `word`.
 //   kLaneBarrier: a block barrier (every warp's stream has three); kLaneEnd ends the stream;
 //   kLanePageEnd ends its page (every page has one).
@@ -191,12 +194,40 @@ enum LaneKind : uint32_t {
   kLaneEnd = 30,
   kLanePageEnd = 31
 };
+// The modes of a kLaneTopSum record (the header's third word): the top rows' partial sums, or one
+// of the dense top's records: a warp's share of the top's right-hand sides into its slots, or a
+// top row's solution as a dense row over every warp's slots (the first record of the row, or one
+// continuing it).
+enum LaneTopMode : uint32_t { kTopSums = 0, kTopLoad = 1, kTopRow = 2, kTopRowMore = 3 };
+constexpr int kLaneDenseTopMost = 192;  // the largest top taken as a dense map
+constexpr double kLaneDenseTopCondition = 1e8;  // the largest condition of that map
 constexpr int kLaneBatch = 4;              // work rows per prefetch
 constexpr int kLaneRows = 2 * kLaneBatch;  // slots of a warp's prefetch ring
+constexpr int kLaneRing = 2;               // pages in flight per warp (a power of two)
+constexpr int kLaneBarriers = 4;           // block barriers in every warp's stream
+
+#if defined(__CUDACC__)
+#define YB_HOST_DEVICE __host__ __device__
+#else
+#define YB_HOST_DEVICE
+#endif
+
+// A lane-solve warp's shared memory: live slots, the prefetch ring, the page ring and its
+// barriers, for values of `value_bytes` and `rpl` right-hand sides per lane (a slot and a ring row
+// hold 32 * rpl values), rounded to 128 bytes; warp w's part starts at w times this. The layout
+// builder writes offsets into other warps' slots from it, the kernel places each warp's part by it.
+inline YB_HOST_DEVICE size_t lane_warp_bytes_of(int32_t value_bytes, int32_t slots, int32_t ring, int32_t page_bytes,
+                                                int32_t rpl) {
+  const size_t row = (size_t)32 * value_bytes * rpl;
+  const size_t b = (size_t)slots * row + (size_t)kLaneRows * row + (size_t)ring * page_bytes + (size_t)ring * 8;
+  return (b + 127) & ~(size_t)127;
+}
 struct LaneLayout {
   int32_t warps = 1, slots = 0, page_bytes = 0, value_bytes = 0;
   int32_t rpl = 1;  // right-hand sides per lane: a slot or row holds 32 * rpl values
   int32_t domains = 0, top = 0, partials = 0;  // partials: partial-array values per block
+  bool dense_top = false;                      // the top is solved as a dense map by every warp
+  double top_condition = 0;                    // that map's condition (0: not computed)
   int32_t fwd_live = 0, bwd_live = 0;          // the peak number of live values in each sweep
   int64_t fwd_entries = 0, bwd_entries = 0;
   double cost = 0;                             // the cut's estimate of a block's time (work units)
