@@ -439,7 +439,7 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   const uint32_t row_bytes = 32u * (uint32_t)sizeof(T) * (uint32_t)rpl;  // a live slot, or a work or partial row
   auto off = [&](int32_t s) { return (uint32_t)s * row_bytes; };
   auto self_of = [&](int32_t s) { return (uint32_t)s * row_bytes / 16; };  // headers hold slot offsets / 16
-  // The dense top: with several warps and a top of 2 to kLaneDenseTopMost rows, its forward and
+  // The dense top: in FP64, with several warps and a top of 2 to kLaneDenseTopMost rows, its forward and
   // backward substitution is one linear map x_T = M r_T from the top rows' right-hand sides (after
   // the partial sums) to their solutions; M is that substitution applied to the identity, in FP64
   // here, kept when its condition (||M||inf ||M^-1||inf) is at most kLaneDenseTopCondition.
@@ -449,7 +449,9 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
   const int32_t t = n - top0;
   const int32_t share = warps > 1 ? (t + warps - 1) / warps : 0;
   std::vector<double> dense_m;
-  bool dense = warps > 1 && t > 1 && t <= kLaneDenseTopMost && 2 + share <= std::min(max_slots, 255);
+  // (FP64 only: in FP32 the map's rounding, about its condition times FP32's epsilon, slowed the
+  // refined solve's convergence enough to cost it a third pass on the 10,000-bus block)
+  bool dense = sizeof(T) == 8 && warps > 1 && t > 1 && t <= kLaneDenseTopMost && 2 + share <= std::min(max_slots, 255);
   if (dense) {
     std::vector<int32_t> tidx(n, -1);
     for (int32_t p = top0; p < n; ++p) tidx[at[p]] = p - top0;
