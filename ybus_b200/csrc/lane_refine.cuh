@@ -136,12 +136,14 @@ template <> struct Iterate8<2> {
 // (64 bytes) at a time, and each row of x a lane reads is one 32-byte load, the four lanes of a row
 // covering its 128-byte line, so an instruction touches 8 lines (against 16 with two lanes per row
 // and 32 with one column per lane: L1's request rate, not DRAM, bounds this kernel). A row's
-// neighbours are read AT_ONCE at a time. R goes in FP32 to the work array (the next pass's
+// neighbours are read AT_ONCE at a time. The first pass fits four blocks an SM (64 registers, a
+// few bytes spilled: 955 to 773 us on the 10k-bus block); the later passes, whose iterates come in
+// two parts, keep three (at four they spill 64 bytes and slow from 1.33 to 1.50 ms). R goes in FP32 to the work array (the next pass's
 // right-hand side); each column's ||R||inf (and on the first pass ||b||inf) is reduced over the
 // block's rows in shared memory and then taken by one atomic maximum of its bit pattern per block;
 // x_k goes to the caller's columns of write_mask.
 template <int BASE>
-__global__ void __launch_bounds__(kResWarps * 32, 3) lane_residual_kernel(LaneRefineArgs a, const float *__restrict__ d,
+__global__ void __launch_bounds__(kResWarps * 32, BASE == 0 ? 4 : 3) lane_residual_kernel(LaneRefineArgs a, const float *__restrict__ d,
                                                                         const float *__restrict__ base32,
                                                                         const double *__restrict__ base64, bool first) {
   constexpr int AT = Iterate8<BASE>::AT_ONCE;
