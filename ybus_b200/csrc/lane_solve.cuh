@@ -2,14 +2,17 @@
 // lane of a warp runs the same rows in the same order (the factor's records are read once per warp,
 // from shared memory, at addresses all lanes share), each on its own right-hand side, so the rows
 // need no barriers, no reductions across lanes and no divergence. The warps of a block take
-// different subtree domains of the elimination tree on the same 32 right-hand sides; warp 0 takes
-// the top above them between two block barriers, with the domains' updates of top rows handed over
-// through a partial array (which all warps add into the top rows' right-hand sides between the
-// first two barriers) and the top's solutions handed back through the work array (LaneLayout in
-// plan.hpp). The order keeps a few tens of values alive per lane, in shared memory; the right-hand
-// sides, the forward results and the solutions stream through the work array in HBM laid out
-// [group][work row][lane], a row's values in the work row of the row of b that feeds it, so every
-// row a warp reads or writes is one contiguous 32-value line.
+// different subtree domains of the elimination tree on the same 32 right-hand sides; the top above
+// them is solved between the second and fourth of four block barriers, with the domains' updates
+// of top rows handed over through a partial array (which all warps add into the top rows'
+// right-hand sides between the first two barriers) and the top's solutions handed back through the
+// work array (LaneLayout in plan.hpp). In FP64 the top is a dense map every warp takes a share of
+// (its right-hand sides into each warp's slots, then each solution as a dense row over all warps'
+// slots); otherwise warp 0 runs its rows as a chain. The order keeps a few tens of values alive
+// per lane, in shared memory; the right-hand sides, the forward results and the solutions stream
+// through the work array in HBM laid out [group][work row][lane], a row's values in the work row of
+// the row of b that feeds it, so every row a warp reads or writes is one contiguous 32-value line
+// (R = 2 right-hand sides per lane: 64 values, lane l's two adjacent).
 //
 // Three launches make a solve: the gather of b (natural rows, column-major) into the work array,
 // the lane solve in place, and the scatter of the work array into x; with the work rows in b's own
