@@ -142,9 +142,10 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
 // The factor for the lane solve (lane_solve.cuh: one right-hand side per lane, every lane of a warp
 // taking the same rows, `warps` warps per block of 32 right-hand sides). The rows are in a postorder
 // of the forward elimination forest with larger subtrees first, cut into subtree domains (dealt to
-// the warps) under a top (taken by warp 0 between the second and third block barriers; between the
-// first and second, every warp adds the domains' partial sums of a share of the top rows into their
-// right-hand sides); each warp's part is one stream of records in fixed-size pages.
+// the warps) under a top (between the first and second block barriers every warp adds the domains'
+// partial sums of a share of the top rows into their right-hand sides; the top itself is solved
+// between the second and fourth, as a dense map every warp takes a share of in FP64, else by warp
+// 0 as a chain); each warp's part is one stream of records in fixed-size pages.
 //
 // A record is a 16-byte header, then `count` entries of 16 bytes (FP64) or 8 (FP32): {T val, or a
 // 32-bit word in its place; uint32 offset}. The header: uint32 {self (16 bits), kind (5 bits), ring
@@ -172,7 +173,7 @@ DomainLayout domain_layout(const Plan<T> &plan, int32_t value_bytes, int32_t war
 //     and kTopRowMore: the output row `word` = (0, or its value so far) + val * the value at the
 //     block-wide shared offset `offset` (another warp's slot), per entry in order.
 //   kLaneImport: per entry, slot `offset` takes the work row `word`.
-//   kLaneBarrier: a block barrier (every warp's stream has three); kLaneEnd ends the stream;
+//   kLaneBarrier: a block barrier (every warp's stream has four); kLaneEnd ends the stream;
 //   kLanePageEnd ends its page (every page has one).
 enum LaneKind : uint32_t {
   kLaneFwdRow0 = 0,  // .. kLaneFwdRow0 + 4
