@@ -568,8 +568,8 @@ def main():
             io_bytes = count * 16 * n  # each of the gather and the scatter reads and writes 8 n per RHS
             r["kernels"]["gather_gbs"] = io_bytes / (kernels["gather_ms"] / 1e3) / 1e9
             r["kernels"]["scatter_gbs"] = io_bytes / (kernels["scatter_ms"] / 1e3) / 1e9
-        # the mode's roofline over its whole step (every launch of it): SURVEY's byte model over the
-        # step's time, against the measured copy bandwidth
+        # the mode's roofline over its whole step (every launch of it): the mode's algorithmic bytes
+        # over the step's time, against the measured copy bandwidth
         step_gbs = r["algorithmic_bytes_per_launch"] / (launch_ms / 1e3) / 1e9
         r["step_roofline"] = {"achieved": step_gbs, "peak": peak, "unit": "GB/s", "frac": step_gbs / peak}
         results[mode] = r
