@@ -180,6 +180,14 @@ int32_t yb_lane_layout_cholesky(int64_t n, const int64_t *l_ptr, const int64_t *
                                 const int64_t *perm, int32_t value_bytes, int32_t page_bytes, int32_t max_slots,
                                 int32_t warps, int32_t rhs_per_lane, int64_t *info, uint8_t *blob, int32_t *warp_page,
                                 int32_t *in_pos, int32_t *out_pos);
+/* No ybus counterpart, diagnostics on the host (no GPU needed): the lane solve's layout for an LU
+ * factor given as to yb_factor_from_lu (L and U in CSC, row and column permutations), the other
+ * arguments and outputs as yb_lane_layout_cholesky's. */
+int32_t yb_lane_layout_lu(int64_t n, const int64_t *l_ptr, const int64_t *l_idx, const double *l_val,
+                          const int64_t *u_ptr, const int64_t *u_idx, const double *u_val, const int64_t *row_perm,
+                          const int64_t *col_perm, int32_t value_bytes, int32_t page_bytes, int32_t max_slots,
+                          int32_t warps, int32_t rhs_per_lane, int64_t *info, uint8_t *blob, int32_t *warp_page,
+                          int32_t *in_pos, int32_t *out_pos);
 /* No ybus counterpart, diagnostics on the host (no GPU needed): the domain layout a Cholesky factor
  * given as to yb_factor_from_cholesky gets for `value_bytes` (8 or 4). info receives {cut, top
  * rows, stages, warps, pages, records, entries, page bytes}, top_condition the worse infinity-norm

@@ -13,6 +13,7 @@ from ybus_b200 import FP64, GpuFactor, configs
 pytestmark = pytest.mark.gpu
 
 BAR = 1e-12
+AUTO, GLOBAL, LANE = 0, 2, 5  # yb_factor_set_tile_kind's kinds
 
 
 @pytest.fixture(scope="module")
@@ -20,15 +21,22 @@ def system():
     return configs.jacobian_system()
 
 
-def test_jacobian_solves_match_the_oracle(gpu, system):
+@pytest.mark.parametrize("kind", [AUTO, LANE, GLOBAL])
+def test_jacobian_solves_match_the_oracle(gpu, system, kind):
     import torch
     factor = GpuFactor.from_lu(gpu, system.lu)
+    factor.set_tile_kind(FP64, kind)
     rhs = system.rhs
     b = torch.from_numpy(rhs).cuda()
     x = torch.empty_like(b)
+    factor.time_lane(True)
     factor.solve_many_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], FP64, None)
     gpu.synchronize()
     factor.check_error()
+    # at 4,096 right-hand sides the automatic choice takes the lane solve: the forest of L's and
+    # U's joint pattern orders both sweeps of the pivoted LU
+    assert (factor.lane_times()["launches"] > 0) == (kind != GLOBAL)
+    factor.time_lane(False)
     xs = x.cpu().numpy()
     sample = np.arange(0, rhs.shape[0], 97)
     assert worst_relative_difference(xs[sample], orc.solve_many_lu(system.lu, rhs[sample], threads=8)) < BAR
@@ -51,8 +59,9 @@ def test_jacobian_transposed_solves_match_the_oracle(gpu, system):
 
 
 def test_the_autotuner_finds_a_faster_solve_for_the_jacobian(gpu, system):
-    # the Jacobian's LU admits no lane layout and its domain tiles hold one column in shared
-    # memory; the autotuner also times the global-scratch solve and keeps what is fastest
+    # at 1,024 right-hand sides (32 lane blocks) the Jacobian's domain tiles hold one column in
+    # shared memory; the autotuner also times the lane and the global-scratch solves and keeps what
+    # is fastest
     factor = GpuFactor.from_lu(gpu, system.lu)
     best = factor.autotune(FP64, 1024)
     assert best["ms"] > 0

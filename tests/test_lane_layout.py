@@ -1,14 +1,14 @@
 """The lane solve's layout, checked on the CPU: the record streams the layout builder makes,
 executed by a host interpreter of the kernel's semantics (warps between block barriers), solve the
-reference's fixture matrices and the synthetic grids to the oracle's solutions, with few live
-values (no GPU)."""
+reference's fixture matrices, the synthetic grids and pivoted LU factors (a Newton-Raphson
+Jacobian among them) to the oracle's solutions, with few live values (no GPU)."""
 import numpy as np
 import pytest
 
 import oracle.oracle as orc
-from fixtures import random_spd, right_hand_sides, star_spd, worst_relative_difference
+from fixtures import random_spd, random_square, right_hand_sides, star_spd, worst_relative_difference
 from lane_interp import run
-from ybus_b200 import YbError, grids, host
+from ybus_b200 import YbError, configs, grids, host
 
 
 def grid_factor(n_bus, extra, seed):
@@ -97,3 +97,25 @@ def test_two_right_hand_sides_per_lane_scale_only_the_offsets(value_bytes, warps
     bar = 1e-12 if value_bytes == 8 else 1e-4
     assert worst_relative_difference(run(two, chol.n, rhs), orc.solve_many(chol, rhs)) < bar
     assert not np.array_equal(one["blob"], two["blob"])
+
+
+@pytest.mark.parametrize("warps", [1, 4, 8])
+@pytest.mark.parametrize("seed", [3, 4])
+def test_lane_records_of_a_pivoted_lu_solve_it(seed, warps):
+    # a threshold-pivoted LU (P A Q = L U): U's entries need not follow L's elimination tree, so
+    # the forest is the tree of both triangles' joint pattern; b's rows enter by P, x's leave by Q
+    a = random_square(250, 4, seed)
+    lu = host.lu(a)
+    rhs = right_hand_sides(250, 6, seed + 1)
+    lay = host.lane_layout(lu, 8, 1024, 256, warps)
+    assert worst_relative_difference(run(lay, lu.n, rhs), orc.solve_many_lu(lu, rhs)) < 1e-12
+    assert not np.array_equal(lay["in_pos"], lay["out_pos"])
+
+
+@pytest.mark.parametrize("warps", [1, 8])
+def test_lane_records_of_a_jacobian_lu_solve_it(warps):
+    # the Newton-Raphson Jacobian of a 2,000-bus network (order 3,598), AMD LU on the host
+    s = configs.jacobian_system(2000, count=4)
+    lay = host.lane_layout(s.lu, 8, 1024, 256, warps)
+    assert lay["slots"] <= 64  # few enough for the automatic choice to take the lane solve
+    assert worst_relative_difference(run(lay, s.lu.n, s.rhs), orc.solve_many_lu(s.lu, s.rhs)) < 1e-12

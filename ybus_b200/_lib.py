@@ -98,6 +98,7 @@ SIGNATURES: dict[str, tuple] = {
     "yb_factor_domain_info": (i32, [vp, i32, P_i32, P_i32, P_i32, P_i64, P_i64, P_i64, P_dbl]),
     "yb_domain_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp, vp]),
     "yb_lane_layout_cholesky": (i32, [i64, vp, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp]),
+    "yb_lane_layout_lu": (i32, [i64, vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp]),
     "yb_solve_many": (i32, [vp, vp, i64, vp]),
     "yb_solve_many_transpose": (i32, [vp, vp, i64, vp]),
     "yb_solve_many_mixed": (i32, [vp, vp, i64, vp, i32, dbl, vp, vp]),

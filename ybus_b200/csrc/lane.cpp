@@ -258,14 +258,43 @@ LaneLayout build(const Plan<V> &plan, int32_t page_bytes, int32_t max_slots, int
     frow[plan.fwd.row[p]] = {plan.fwd.ptr[p], plan.fwd.ptr[p + 1], (double)plan.fwd.dinv[p]};
     brow[plan.bwd.row[p]] = {plan.bwd.ptr[p], plan.bwd.ptr[p + 1], (double)plan.bwd.dinv[p]};
   }
-  // the forest, subtree sizes and the postorder with larger subtrees first
-  std::vector<int32_t> parent(n, -1);
+  // The forest: the elimination tree of the two triangles' joint pattern, by Liu's algorithm with
+  // path compression over the entries (i, k), k < i, of the forward triangle and of the backward
+  // one transposed. Every entry's larger index is then an ancestor of its smaller, so one
+  // postorder serves the forward sweep and its reverse the backward. For a Cholesky factor this is
+  // the factor's own elimination tree (each column's parent its first off-diagonal row); for an LU
+  // factor it also covers U's entries, which L's tree alone need not order.
+  std::vector<int32_t> below_ptr(n + 1, 0), below;  // backward entries by column: rows r < c with U(r, c)
   for (int32_t r = 0; r < n; ++r)
-    for (int32_t q = frow[r].p0; q < frow[r].p1; ++q) {
-      const int32_t c = plan.fwd.col[q];
-      if (c >= r) throw host::Error(host::kInvalidArgument, "the forward sweep is not lower triangular");
-      if (parent[c] < 0 || r < parent[c]) parent[c] = r;
+    for (int32_t q = brow[r].p0; q < brow[r].p1; ++q) {
+      const int32_t c = plan.bwd.col[q];
+      if (c <= r) throw host::Error(host::kInvalidArgument, "the backward sweep is not upper triangular");
+      ++below_ptr[c + 1];
     }
+  for (int32_t c = 0; c < n; ++c) below_ptr[c + 1] += below_ptr[c];
+  below.resize(below_ptr[n]);
+  {
+    std::vector<int32_t> fill(below_ptr.begin(), below_ptr.end() - 1);
+    for (int32_t r = 0; r < n; ++r)
+      for (int32_t q = brow[r].p0; q < brow[r].p1; ++q) below[fill[plan.bwd.col[q]]++] = r;
+  }
+  std::vector<int32_t> parent(n, -1), ancestor(n, -1);
+  for (int32_t i = 0; i < n; ++i) {
+    auto join = [&](int32_t k) {
+      while (ancestor[k] >= 0 && ancestor[k] != i) {
+        const int32_t up = ancestor[k];
+        ancestor[k] = i;
+        k = up;
+      }
+      if (ancestor[k] < 0) ancestor[k] = i, parent[k] = i;
+    };
+    for (int32_t q = frow[i].p0; q < frow[i].p1; ++q) {
+      const int32_t c = plan.fwd.col[q];
+      if (c >= i) throw host::Error(host::kInvalidArgument, "the forward sweep is not lower triangular");
+      join(c);
+    }
+    for (int32_t q = below_ptr[i]; q < below_ptr[i + 1]; ++q) join(below[q]);
+  }
   std::vector<int64_t> size(n, 1);
   for (int32_t c = 0; c < n; ++c)
     if (parent[c] >= 0) size[parent[c]] += size[c];

@@ -205,7 +205,7 @@ class GpuFactor:
         _check(lib().yb_factor_set_tile(self._h, precision, width, threads, blocks_per_sm))
 
     def set_tile_kind(self, precision: int, kind: int) -> None:
-        """0 automatic, 1 shared-memory, 2 global-scratch, 3 streamed, 4 domain tile solve."""
+        """0 automatic, 1 shared-memory, 2 global-scratch, 3 streamed, 4 domain tile, 5 lane solve."""
         _check(lib().yb_factor_set_tile_kind(self._h, precision, kind))
 
     def set_stream(self, precision: int, warps: int = 8, ring: int = 4, page_bytes: int = 2048,

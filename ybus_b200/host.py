@@ -201,22 +201,33 @@ def domain_layout(chol: HostCholesky, value_bytes: int = 8, warps: int = 16, pag
             "value_bytes": value_bytes, "top_condition": cond.value}
 
 
-def lane_layout(chol: HostCholesky, value_bytes: int = 8, page_bytes: int = 2048, max_slots: int = 1 << 20,
-                warps: int = 1, rpl: int = 1) -> dict:
-    """The lane solve's records for a Cholesky factor, built on the host (no GPU): every warp's
-    pages and each row's position in the work array (diagnostics and tests); `rpl` right-hand
-    sides per lane (1 or 2)."""
+def lane_layout(factor: "HostCholesky | HostLu", value_bytes: int = 8, page_bytes: int = 2048,
+                max_slots: int = 1 << 20, warps: int = 1, rpl: int = 1) -> dict:
+    """The lane solve's records for a Cholesky or a real LU factor, built on the host (no GPU):
+    every warp's pages and each row's position in the work array (diagnostics and tests); `rpl`
+    right-hand sides per lane (1 or 2)."""
     info = np.zeros(12, np.int64)
-    l = chol.l
-    val = np.ascontiguousarray(l.val, dtype=np.float64)
-    args = (chol.n, ptr(l.ptr), ptr(l.idx), ptr(val), ptr(chol.perm), value_bytes, page_bytes, max_slots, warps, rpl)
-    check(_lib.lib().yb_lane_layout_cholesky(*args, ptr(info), None, None, None, None))
+    n = factor.n
+    if isinstance(factor, HostLu):
+        if factor.is_complex:
+            raise ValueError("a real LU factor only")
+        lv = np.ascontiguousarray(factor.l.val, dtype=np.float64)
+        uv = np.ascontiguousarray(factor.u.val, dtype=np.float64)
+        fn = _lib.lib().yb_lane_layout_lu
+        args = (n, ptr(factor.l.ptr), ptr(factor.l.idx), ptr(lv), ptr(factor.u.ptr), ptr(factor.u.idx), ptr(uv),
+                ptr(factor.row_perm), ptr(factor.col_perm), value_bytes, page_bytes, max_slots, warps, rpl)
+    else:
+        l = factor.l
+        val = np.ascontiguousarray(l.val, dtype=np.float64)
+        fn = _lib.lib().yb_lane_layout_cholesky
+        args = (n, ptr(l.ptr), ptr(l.idx), ptr(val), ptr(factor.perm), value_bytes, page_bytes, max_slots, warps, rpl)
+    check(fn(*args, ptr(info), None, None, None, None))
     slots, pages, pb, fwd_live, bwd_live, fwd_entries, bwd_entries, w, domains, top, partials, r = (int(v) for v in info)
     blob = np.zeros(pages * pb, np.uint8)
     warp_page = np.zeros(w + 1, np.int32)
-    in_pos = np.zeros(chol.n, np.int32)
-    out_pos = np.zeros(chol.n, np.int32)
-    check(_lib.lib().yb_lane_layout_cholesky(*args, ptr(info), ptr(blob), ptr(warp_page), ptr(in_pos), ptr(out_pos)))
+    in_pos = np.zeros(n, np.int32)
+    out_pos = np.zeros(n, np.int32)
+    check(fn(*args, ptr(info), ptr(blob), ptr(warp_page), ptr(in_pos), ptr(out_pos)))
     return {"slots": slots, "pages": pages, "page_bytes": pb, "fwd_live": fwd_live, "bwd_live": bwd_live,
             "fwd_entries": fwd_entries, "bwd_entries": bwd_entries, "warps": w, "domains": domains, "top": top,
             "partials": partials, "blob": blob, "warp_page": warp_page, "in_pos": in_pos, "out_pos": out_pos,
