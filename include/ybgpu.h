@@ -103,12 +103,12 @@ int32_t yb_factor_set_tile_kind(yb_factor *f, int32_t precision, int32_t kind);
  * forward results and x streaming through a work array in HBM). info receives 12 values: {slots,
  * pages, page bytes, forward peak of live values, backward peak, entries of both sweeps, shared
  * memory per block, warps per block, domains, top rows, partial values per block, right-hand sides per lane};
- * YB_ERROR_INVALID_ARGUMENT if the factor admits no lane layout (no postorder serves both sweeps,
- * or too many live values). */
+ * YB_ERROR_INVALID_ARGUMENT if the factor admits no lane layout (too many live values). */
 int32_t yb_factor_lane_info(yb_factor *f, int32_t precision, int64_t *info);
-/* No ybus counterpart: the lane solve's shape for a precision: warps per block (1..8, default 8)
- * and page bytes (256..16384, a multiple of 16; default 0: the largest of 2048, 1024, 768, 512 with
- * which three blocks fit an SM). */
+/* No ybus counterpart: the lane solve's shape for a precision: warps per block (1..16, default 8;
+ * blocks of more than 8 warps run one to an SM, for blocks of fewer groups of 32 than SMs) and page
+ * bytes (256..16384, a multiple of 16; default 0: the largest of 2048, 1024, 768, 512 with which
+ * three blocks fit an SM). */
 int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32_t page_bytes);
 /* No ybus counterpart: how many right-hand sides each lane of the plain lane solve carries, 1 or 2
  * (a block then solves 32 or 64 right-hand sides; with two, each decoded record serves twice the
@@ -162,8 +162,8 @@ int32_t yb_factor_domain_info(yb_factor *f, int32_t precision, int32_t *tile_wid
 /* No ybus counterpart: the autotuner. Times the solve of `count` right-hand sides for a precision
  * over the domain solve's shapes (warps 8/12/16, pages 1536/2048 bytes, 2 or 3 pages in flight, the
  * widest tile that fits and half of it), the global-scratch solve's (tile widths 1 to 32, 256 or
- * 512 threads) and the lane solve's (4, 6 or 8 warps per block, one or two right-hand sides per
- * lane, when the factor admits a lane layout) and keeps the fastest for the factor, for solves of
+ * 512 threads) and the lane solve's (4, 6 or 8 warps per block with one or two right-hand sides
+ * per lane, 12 or 16 with one, when the factor admits a lane layout) and keeps the fastest for the factor, for solves of
  * about that many right-hand sides. config receives {kind, tile width (0 for the lane solve),
  * warps, ring, page bytes} (for the global-scratch solve: {kind, tile width, warps, blocks per SM,
  * 0}) and best_ms its time (either may be NULL). With nothing to time, the configuration is left

@@ -109,7 +109,7 @@ def test_autotune_keeps_the_fastest_domain_shape_and_the_same_solutions(gpu):
             assert best["tile"] in (1, 2, 4, 8, 16, 32) and best["warps"] in (8, 16)
             assert factor.tile(prec)[:2] == (best["tile"], 32 * best["warps"])
         else:
-            assert best["kind"] == LANE and best["warps"] in (4, 6, 8) and best["tile"] == 0
+            assert best["kind"] == LANE and best["warps"] in (4, 6, 8, 12, 16) and best["tile"] == 0
             assert factor.lane_info(prec)["warps"] == best["warps"]
         if prec == FP64:
             d = worst_relative_difference(factor.solve_many(rhs), cpu)

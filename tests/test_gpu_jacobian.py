@@ -51,6 +51,23 @@ def test_jacobian_solves_match_the_oracle(gpu, system, kind):
         assert mine <= 4.0 * theirs + 1e-13, (k, mine, theirs)
 
 
+def test_jacobian_solves_in_blocks_of_sixteen_warps(gpu, system):
+    # 128 groups of 32 on 148 SMs: blocks of 16 warps, one an SM, halve each warp's chain of rows
+    import torch
+    factor = GpuFactor.from_lu(gpu, system.lu)
+    factor.set_tile_kind(FP64, LANE)
+    factor.set_lane(FP64, 16)
+    assert factor.lane_info(FP64)["warps"] == 16
+    rhs = system.rhs
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.empty_like(b)
+    factor.solve_many_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], FP64, None)
+    gpu.synchronize()
+    factor.check_error()
+    sample = np.arange(0, rhs.shape[0], 89)
+    assert worst_relative_difference(x.cpu().numpy()[sample], orc.solve_many_lu(system.lu, rhs[sample], threads=8)) < BAR
+
+
 def test_jacobian_transposed_solves_match_the_oracle(gpu, system):
     factor = GpuFactor.from_lu(gpu, system.lu)
     rhs = system.rhs[:256]

@@ -15,9 +15,10 @@ BAR = 1e-12
 LANE = 5
 
 
-@pytest.mark.parametrize("warps", [1, 2, 4, 8])
+@pytest.mark.parametrize("warps", [1, 2, 4, 8, 9, 16])
 @pytest.mark.parametrize("count", [1, 31, 32, 33, 200])
 def test_lane_solve_matches_the_cpu(gpu, count, warps):
+    # 9 and 16: the kernel instance for blocks of more than 8 warps, one block an SM
     chol = host.cholesky(random_spd(200, 3, 7))
     rhs = right_hand_sides(200, count, 11)
     factor = GpuFactor.from_cholesky(gpu, chol)
@@ -121,9 +122,11 @@ def test_lane_solve_on_the_10k_grid(gpu):
     assert factor.lane_info(FP64)["slots"] <= 48
     b = torch.from_numpy(rhs).cuda()
     x = torch.empty_like(b)
-    for prec, bar, warps in ((FP64, BAR, 1), (FP64, BAR, 6), (FP64, BAR, 8), (FP32, 1e-3, 4)):
+    for prec, bar, warps in ((FP64, BAR, 1), (FP64, BAR, 6), (FP64, BAR, 8), (FP64, BAR, 12), (FP64, BAR, 16),
+                             (FP32, 1e-3, 4), (FP32, 1e-3, 16)):
         factor.set_tile_kind(prec, LANE)
         factor.set_lane(prec, warps)
+        assert factor.lane_info(prec)["warps"] == warps
         x.zero_()
         factor.solve_many_device(b.data_ptr(), x.data_ptr(), rhs.shape[0], prec, None)
         gpu.synchronize()

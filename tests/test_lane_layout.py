@@ -18,7 +18,7 @@ def grid_factor(n_bus, extra, seed):
     return host.cholesky(host.Matrix.from_triplets(n_bus, n_bus, r, c, v).select(keep, keep))
 
 
-@pytest.mark.parametrize("warps", [1, 3, 8])
+@pytest.mark.parametrize("warps", [1, 3, 8, 16])
 @pytest.mark.parametrize("page", [256, 2048])
 @pytest.mark.parametrize("fill", [2, 6, 30])
 def test_lane_records_solve_the_fixture(page, fill, warps):
@@ -112,7 +112,7 @@ def test_lane_records_of_a_pivoted_lu_solve_it(seed, warps):
     assert not np.array_equal(lay["in_pos"], lay["out_pos"])
 
 
-@pytest.mark.parametrize("warps", [1, 8])
+@pytest.mark.parametrize("warps", [1, 8, 16])
 def test_lane_records_of_a_jacobian_lu_solve_it(warps):
     # the Newton-Raphson Jacobian of a 2,000-bus network (order 3,598), AMD LU on the host
     s = configs.jacobian_system(2000, count=4)

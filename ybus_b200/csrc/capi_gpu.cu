@@ -764,6 +764,24 @@ cudaEvent_t *lane_timing_slot(yb_factor *f) {
   return t.ev[t.used++].data();
 }
 
+// The lane shape a solve of `count` right-hand sides takes: the configured one, or, when no caller
+// or autotuner set the warps and the groups of 32 fit one wave of one block an SM, blocks of
+// kLaneMaxWarps warps (measured on the 10,000-bus B′ at 4,096 right-hand sides: 0.61 against
+// 0.76 ms per solve; on the 10,000-bus Jacobian: 1.37 against 1.84 ms).
+TileConfig lane_shape(const yb_factor *f, TileConfig cfg, int64_t count) {
+  if (cfg.lane_warps_auto && cfg.lane_rpl == 1 && cfg.lane_page == 0 && (count + 31) / 32 <= f->gpu->sm_count)
+    cfg.lane_warps = kLaneMaxWarps;
+  return cfg;
+}
+
+// The lane kernel for a layout's warps per block (the three-per-SM instance up to 8 warps, the
+// one-per-SM instance above), its dynamic shared memory allowed.
+template <class T, int R> auto lane_kernel(const DeviceLane *d, size_t smem) {
+  auto k = d->warps > kLaneNarrowWarps ? lane_solve_kernel<T, R, true> : lane_solve_kernel<T, R, false>;
+  cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "cudaFuncSetAttribute");
+  return k;
+}
+
 template <class T, int R>
 void launch_lane_r(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count,
                    cudaStream_t stream) {
@@ -778,8 +796,7 @@ void launch_lane_r(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, do
   T *partial = reinterpret_cast<T *>(f->lane_partial.get());
   const size_t smem = lane_smem<T>(d);
   if (smem > (size_t)f->gpu->smem_optin) throw host::Error(host::kInvalidArgument, "the lane solve's block does not fit in shared memory");
-  cuda_check(cudaFuncSetAttribute(lane_solve_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-             "cudaFuncSetAttribute");
+  const auto kernel = lane_kernel<T, R>(d, smem);
   LaneArgs a{};
   a.n = (int32_t)n;
   a.slots = d->slots, a.page_bytes = d->page_bytes, a.partials = d->partials;
@@ -798,7 +815,7 @@ void launch_lane_r(yb_factor *f, DeviceLane *d, const double *b, int64_t ldb, do
                                                                      d->in_pos.get(), work, nullptr);
     cuda_check(cudaGetLastError(), "lane_in_kernel launch");
     if (ev) cuda_check(cudaEventRecord(ev[1], stream), "cudaEventRecord");
-    lane_solve_kernel<T, R><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
+    kernel<<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
     cuda_check(cudaGetLastError(), "lane_solve_kernel launch");
     a.withhold = -1;
     if (ev) cuda_check(cudaEventRecord(ev[2], stream), "cudaEventRecord");
@@ -915,7 +932,7 @@ void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t
   auto run = [&](auto zero, const TileConfig &configured, auto &fwd, auto &bwd, auto &scratch, auto &cache) {
     using T = decltype(zero);
     if (configured.kind == kTileLane || (configured.kind == kTileAuto && count >= configured.lane_min_count)) {
-      DeviceLane *d = lane_pick<T>(f, configured, configured.lane_rpl, stream);
+      DeviceLane *d = lane_pick<T>(f, lane_shape(f, configured, count), configured.lane_rpl, stream);
       if (d && (configured.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane<T>(f, d, b, ldb, x, ldx, count, stream);
         return;
@@ -1296,11 +1313,11 @@ extern "C" int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t w
   return guard([&] {
     require(f != nullptr, "null factor");
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
-    require(warps >= 1 && warps <= kLaneMaxWarps, "1 to 8 warps per block");
+    require(warps >= 1 && warps <= kLaneMaxWarps, "1 to 16 warps per block");
     require(page_bytes == 0 || (page_bytes >= 256 && page_bytes <= 16384 && page_bytes % 16 == 0),
             "pages of 256 to 16384 bytes, a multiple of 16, or 0 for the automatic choice");
     TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
-    t.lane_warps = warps, t.lane_page = page_bytes;
+    t.lane_warps = warps, t.lane_page = page_bytes, t.lane_warps_auto = false;
     return YB_OK;
   });
 }
@@ -1481,8 +1498,7 @@ void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t l
   r.ldb = ldb, r.ldx = ldx;
   const size_t smem = lane_smem<T>(d);
   if (smem > (size_t)f->gpu->smem_optin) throw host::Error(host::kInvalidArgument, "the lane solve's block does not fit in shared memory");
-  cuda_check(cudaFuncSetAttribute(lane_solve_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-             "cudaFuncSetAttribute");
+  const auto kernel = lane_kernel<T, 1>(d, smem);
   LaneArgs a{};
   a.n = (int32_t)n;
   a.slots = d->slots, a.page_bytes = d->page_bytes, a.partials = d->partials;
@@ -1513,7 +1529,7 @@ void launch_lane_refined(yb_factor *f, DeviceLane *d, const double *b, int64_t l
     for (int32_t pass = 0; pass <= max_steps; ++pass) {
       T *dk = pass == 1 ? dB : dA;  // this pass's correction
       a.xout = dk;
-      lane_solve_kernel<T, 1><<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
+      kernel<<<(unsigned)groups, d->warps * 32, smem, stream>>>(a, work, partial);
       check("lane_solve_kernel launch");
       if (pass == 0)
         lane_residual_kernel<0><<<rows_grid, kResWarps * 32, 0, stream>>>(r, dk, nullptr, nullptr, true);
@@ -1561,7 +1577,7 @@ extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rh
     const TileConfig &t32 = f->tile32;
     if (t32.kind == kTileLane ||
         (t32.kind == kTileAuto && count >= std::max(t32.lane_min_count, t32.refine_lane_min_count))) {
-      DeviceLane *d = lane_pick<float>(f, t32, 1, s);  // its kernels take groups of 32 columns
+      DeviceLane *d = lane_pick<float>(f, lane_shape(f, t32, count), 1, s);  // its kernels take groups of 32 columns
       if (d && (t32.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane_refined(f, d, d_rhs, ldb, d_out, ldx, count, max_steps, tolerance, d_ratio, d_steps, s);
         return YB_OK;
@@ -1661,11 +1677,13 @@ extern "C" int32_t yb_factor_autotune(yb_factor *f, int32_t precision, int64_t c
         }
       }
     // the lane solve, when the factor admits it, at 4, 6 and 8 warps per block, with one and with
-    // two right-hand sides per lane
+    // two right-hand sides per lane, and with one at 12 and 16 (one block an SM: for fewer groups
+    // than SMs)
     for (int rpl : {1, 2})
-      for (int warps : {4, 6, 8}) {
+      for (int warps : {4, 6, 8, 12, 16}) {
+        if (rpl == 2 && warps > kLaneNarrowWarps) continue;
         TileConfig run = saved;
-        run.kind = kTileLane, run.lane_warps = warps, run.lane_page = 0, run.lane_rpl = rpl;
+        run.kind = kTileLane, run.lane_warps = warps, run.lane_page = 0, run.lane_rpl = rpl, run.lane_warps_auto = false;
         DeviceLane *d = precision == YB_FP64 ? lane_pick<double>(f, run, rpl, s) : lane_pick<float>(f, run, rpl, s);
         if (!d || d->warps != warps) continue;  // none, or the block took fewer warps (timed on its own)
         time_config(run);

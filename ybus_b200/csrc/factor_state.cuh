@@ -112,6 +112,9 @@ struct TileConfig {
   int64_t lane_min_count = 3072;
   int lane_warps = 8, lane_page = 0;  // the lane solve's warps per block (one group of 32 right-hand sides), page bytes
   int lane_rpl = 1;                   // right-hand sides per lane of the plain lane solve (1 or 2)
+  // lane_warps not set by a caller or the autotuner: a solve of no more groups of 32 than SMs then
+  // takes blocks of kLaneMaxWarps (one an SM, each warp's chain of rows shorter)
+  bool lane_warps_auto = true;
   // the refined solve takes the lane solve from this many right-hand sides on (its passes cost more
   // launches than the plain solve's, so its crossover with the fused domain refinement lies higher)
   int64_t refine_lane_min_count = 5120;

@@ -31,7 +31,8 @@
 
 namespace yb {
 
-constexpr int kLaneMaxWarps = 8;             // warps per block at most
+constexpr int kLaneMaxWarps = 16;            // warps per block at most
+constexpr int kLaneNarrowWarps = 8;          // at most these take the kernel bounded to three blocks per SM
 
 struct LaneArgs {
   int32_t n, slots, page_bytes, partials;
@@ -174,13 +175,15 @@ __device__ __forceinline__ Lv<T, R> lane_gather(uint32_t e, uint32_t count, Lv<T
 
 // Block g solves the 32 R right-hand sides of group g in `work` in place (R per lane: the records'
 // decoding then serves R times the arithmetic); `partial` holds each block's partial array. With
-// R = 1 three blocks share an SM (as many as its shared memory holds), so the launch bound lets each
-// thread take up to 80 registers: the compiler then keeps the records' fields and addresses in
-// registers instead of recomputing them (13 % fewer instructions and 7 % less time than with the
-// 44 registers it picks unbounded); with R = 2 two blocks do.
-template <class T, int R>
-__global__ void __launch_bounds__(kLaneMaxWarps * 32, R == 1 ? 3 : 2) lane_solve_kernel(LaneArgs a, T *__restrict__ work,
-                                                                       T *__restrict__ partial) {
+// R = 1 three blocks of up to 8 warps share an SM (as many as its shared memory holds), so the
+// launch bound lets each thread take up to 80 registers: the compiler then keeps the records'
+// fields and addresses in registers instead of recomputing them (13 % fewer instructions and 7 %
+// less time than with the 44 registers it picks unbounded); with R = 2 two blocks do. WIDE blocks
+// of 9 to 16 warps run one to an SM: for grids of fewer groups than SMs, where each warp's chain
+// of rows, not the SM's issue, sets the time and more warps shorten the chains.
+template <class T, int R, bool WIDE = false>
+__global__ void __launch_bounds__(WIDE ? kLaneMaxWarps * 32 : kLaneNarrowWarps * 32, WIDE ? 1 : (R == 1 ? 3 : 2))
+    lane_solve_kernel(LaneArgs a, T *__restrict__ work, T *__restrict__ partial) {
   constexpr uint32_t E = sizeof(T) == 8 ? 16 : 8, VB = sizeof(T) * R, ROW = 32 * VB;
   // The warp index through a shuffle from lane 0: the compiler then knows it (and the shared
   // offsets, record fields and branches derived from it) to be the same across the warp, and keeps
