@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--no-extras", action="store_true",
                    help="time the headline modes only (no block widths, workloads or comparison): for profiling")
     p.add_argument("--rhs", type=int, default=0, help="solve only the first RHS (a smaller case for profiling)")
+    p.add_argument("--lane-warps", type=int, default=0,
+                   help="jacobian: the lane solve at this many warps per block instead of the autotuner's pick "
+                        "(a fixed kernel for profiling)")
     p.add_argument("--workload", default="ptdf", choices=["ptdf", "n1", "adjoint", "complex", "jacobian"],
                    help="ptdf: the headline PTDF block with the other workloads as extra keys; n1, adjoint, complex, jacobian: "
                         "one of the other workloads alone, one JSON line")
@@ -348,10 +351,11 @@ def workload_complex(gpu, steps: int, warm: int, rank: int, world: int, device: 
                        "split": f"networks by LPT over {world} GPU(s)"}, "modes": modes}
 
 
-def workload_jacobian(gpu, steps: int, warm: int, rank: int, world: int, device: int) -> dict:
+def workload_jacobian(gpu, steps: int, warm: int, rank: int, world: int, device: int, lane_warps: int = 0) -> dict:
     """The Newton-Raphson Jacobian of the 10,000-bus complex network (order 17,998, AMD LU on the
     host; the reference's other matrix for its GPU survey): 4,096 right-hand sides, device arrays,
-    FP64, split over the ranks by columns."""
+    FP64, split over the ranks by columns; the autotuner picks the solve, or `lane_warps` fixes the
+    lane solve's blocks."""
     import torch
 
     from ybus_b200 import FP64, GpuFactor, configs, replicas
@@ -359,7 +363,12 @@ def workload_jacobian(gpu, steps: int, warm: int, rank: int, world: int, device:
     mine = replicas.shard(sysj.rhs.shape[0], rank, world)
     rhs = np.ascontiguousarray(sysj.rhs[mine.start:mine.stop])
     factor = GpuFactor.from_lu(gpu, sysj.lu)
-    tuned = factor.autotune(FP64, rhs.shape[0])  # as a caller would, once per factor
+    if lane_warps:
+        factor.set_tile_kind(FP64, 5)
+        factor.set_lane(FP64, lane_warps)
+        tuned = {"kind": 5, "tile": 0, "warps": lane_warps, "fixed": True}
+    else:
+        tuned = factor.autotune(FP64, rhs.shape[0])  # as a caller would, once per factor
     b = torch.from_numpy(rhs).cuda()
     x = torch.empty_like(b)
     # a stream of our own: the legacy default stream's handle is 0, which the C ABI reads as the
@@ -413,7 +422,8 @@ def run_workload(a) -> int:
     gpu = Gpu.new(local)
     line = {"workload": a.workload, "n_gpus": world, "steps": max(a.steps, 1), "warmup": max(a.warmup, 1),
             "data": "synthetic"}
-    line.update(WORKLOADS[a.workload](gpu, max(a.steps, 1), max(a.warmup, 1), rank, world, local))
+    extra = {"lane_warps": a.lane_warps} if a.workload == "jacobian" and a.lane_warps else {}
+    line.update(WORKLOADS[a.workload](gpu, max(a.steps, 1), max(a.warmup, 1), rank, world, local, **extra))
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
