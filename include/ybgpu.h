@@ -116,7 +116,8 @@ int32_t yb_factor_set_lane(yb_factor *f, int32_t precision, int32_t warps, int32
  * one. yb_factor_lane_info reports it (its last value). */
 int32_t yb_factor_set_lane_rhs_per_lane(yb_factor *f, int32_t precision, int32_t rhs_per_lane);
 /* No ybus counterpart: the number of right-hand sides from which the automatic choice takes the
- * lane solve (default 3072). */
+ * lane solve; -1 (the default): 1,536 when the domain solve's automatic tiles hold two or more
+ * columns, else 64 (the measured crossovers). */
 int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t min_count);
 /* No ybus counterpart: the number of right-hand sides from which yb_solve_many_refined_device takes
  * the FP32 lane solve (default 5120, the measured crossover with the refinement fused into the
@@ -124,7 +125,8 @@ int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t mi
  * too, whichever is higher). */
 int32_t yb_factor_set_refine_lane_min_count(yb_factor *f, int64_t min_count);
 /* No ybus counterpart: the thresholds the automatic choice applies for a precision: the plain
- * solve's lane threshold and the refined solve's (either output may be NULL). */
+ * solve's lane threshold (the automatic one resolved for this factor) and the refined solve's
+ * (either output may be NULL). */
 int32_t yb_factor_lane_min_counts(const yb_factor *f, int32_t precision, int64_t *lane_min_count,
                                   int64_t *refine_lane_min_count);
 /* No ybus counterpart: with on = 1, every lane-solve launch from now on records CUDA events around

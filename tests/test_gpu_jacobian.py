@@ -51,6 +51,20 @@ def test_jacobian_solves_match_the_oracle(gpu, system, kind):
         assert mine <= 4.0 * theirs + 1e-13, (k, mine, theirs)
 
 
+def test_the_automatic_threshold_takes_the_lane_solve_from_two_groups(gpu, system):
+    # the Jacobian's domain tiles hold one column: the lane solve is the faster from 64 right-hand
+    # sides on, and the automatic choice takes it there
+    factor = GpuFactor.from_lu(gpu, system.lu)
+    assert factor.domain_info(FP64)["tile"] == 1
+    assert factor.lane_min_count(FP64) == 64
+    rhs = system.rhs[:256]
+    factor.time_lane(True)
+    x = factor.solve_many(rhs)
+    assert factor.lane_times()["launches"] > 0
+    factor.time_lane(False)
+    assert worst_relative_difference(x, orc.solve_many_lu(system.lu, rhs, threads=8)) < BAR
+
+
 def test_jacobian_solves_in_blocks_of_sixteen_warps(gpu, system):
     # 128 groups of 32 on 148 SMs: blocks of 16 warps, one an SM, halve each warp's chain of rows
     import torch

@@ -120,6 +120,8 @@ def test_lane_solve_on_the_10k_grid(gpu):
     rhs = np.random.default_rng(5).standard_normal((1000, chol.n))
     factor = GpuFactor.from_cholesky(gpu, chol)
     assert factor.lane_info(FP64)["slots"] <= 48
+    # its domain tiles hold two columns: the automatic choice keeps the domain solve below 1,536
+    assert factor.domain_info(FP64)["tile"] >= 2 and factor.lane_min_count(FP64) == 1536
     b = torch.from_numpy(rhs).cuda()
     x = torch.empty_like(b)
     for prec, bar, warps in ((FP64, BAR, 1), (FP64, BAR, 6), (FP64, BAR, 8), (FP64, BAR, 12), (FP64, BAR, 16),

@@ -925,13 +925,27 @@ template <class T> TileArgs<T> base_args(yb_factor *f, const DeviceSweep<T> &fwd
   return a;
 }
 
+// The count of right-hand sides from which the automatic choice takes the lane solve: the
+// configured one, or by the domain solve's automatic tile. Where its tiles hold two or more columns
+// the domain solve is the faster below about 1,500 (measured on the 10,000-bus B′, tiles of 2: 0.34
+// against 0.45 ms at 1,024 right-hand sides, 0.50 against 0.47 at 1,536, 0.58 against 0.50 at
+// 2,048); where they hold one column, or it has none, the lane solve is the faster from two groups
+// of 32 (the 10,000-bus Jacobian: 1.01 against 0.98 ms at 64, 7.05 against 1.09 ms at 1,024).
+template <class T> int64_t lane_threshold(yb_factor *f, const TileConfig &cfg) {
+  if (cfg.lane_min_count >= 0) return cfg.lane_min_count;
+  TileConfig automatic = cfg;
+  automatic.kind = kTileAuto;
+  const TileConfig d = resolve<T>(f, automatic);
+  return d.kind == kTileDomain && d.width >= 2 ? 1536 : 64;
+}
+
 // Solves `count` right-hand sides already on the device, in `precision`, on `stream`.
 void solve_device(yb_factor *f, const double *b, int64_t ldb, double *x, int64_t ldx, int64_t count, int precision,
                   cudaStream_t stream) {
   if (count <= 0 || f->n == 0) return;
   auto run = [&](auto zero, const TileConfig &configured, auto &fwd, auto &bwd, auto &scratch, auto &cache) {
     using T = decltype(zero);
-    if (configured.kind == kTileLane || (configured.kind == kTileAuto && count >= configured.lane_min_count)) {
+    if (configured.kind == kTileLane || (configured.kind == kTileAuto && count >= lane_threshold<T>(f, configured))) {
       DeviceLane *d = lane_pick<T>(f, lane_shape(f, configured, count), configured.lane_rpl, stream);
       if (d && (configured.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane<T>(f, d, b, ldb, x, ldx, count, stream);
@@ -1336,7 +1350,7 @@ extern "C" int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision,
   return guard([&] {
     require(f != nullptr, "null factor");
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
-    require(min_count >= 0, "negative count");
+    require(min_count >= -1, "a count, or -1 for the automatic threshold");
     (precision == YB_FP64 ? f->tile64 : f->tile32).lane_min_count = min_count;
     return YB_OK;
   });
@@ -1356,8 +1370,9 @@ extern "C" int32_t yb_factor_lane_min_counts(const yb_factor *f, int32_t precisi
   return guard([&] {
     require(f != nullptr, "null factor");
     require(precision == YB_FP64 || precision == YB_FP32, "unknown precision");
-    const TileConfig &t = precision == YB_FP64 ? f->tile64 : f->tile32;
-    if (lane_min_count) *lane_min_count = t.lane_min_count;
+    yb_factor *g = const_cast<yb_factor *>(f);  // the automatic threshold may build the domain layout
+    if (lane_min_count)
+      *lane_min_count = precision == YB_FP64 ? lane_threshold<double>(g, g->tile64) : lane_threshold<float>(g, g->tile32);
     if (refine_lane_min_count) *refine_lane_min_count = f->tile32.refine_lane_min_count;
     return YB_OK;
   });
@@ -1576,7 +1591,7 @@ extern "C" int32_t yb_solve_many_refined_device(yb_factor *f, const double *d_rh
     cudaStream_t s = stream ? (cudaStream_t)stream : f->gpu->stream;
     const TileConfig &t32 = f->tile32;
     if (t32.kind == kTileLane ||
-        (t32.kind == kTileAuto && count >= std::max(t32.lane_min_count, t32.refine_lane_min_count))) {
+        (t32.kind == kTileAuto && count >= std::max(lane_threshold<float>(f, t32), t32.refine_lane_min_count))) {
       DeviceLane *d = lane_pick<float>(f, lane_shape(f, t32, count), 1, s);  // its kernels take groups of 32 columns
       if (d && (t32.kind == kTileLane || d->slots <= kLaneAutoSlots)) {
         launch_lane_refined(f, d, d_rhs, ldb, d_out, ldx, count, max_steps, tolerance, d_ratio, d_steps, s);

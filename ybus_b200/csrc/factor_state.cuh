@@ -108,8 +108,9 @@ struct TileConfig {
   // (first forward level of the top block; -1: chosen by the layout's cost model)
   int domain_warps = 16, domain_ring = 2, domain_page = 2048, domain_cut = -1;
   // the automatic choice takes the lane solve from this many right-hand sides on (one warp per 32:
-  // fewer leave SMs idle, where the domain solve's tiles spread over all of them)
-  int64_t lane_min_count = 3072;
+  // fewer leave SMs idle, where the domain solve's tiles spread over all of them); -1: by the
+  // factor's domain tiles (lane_threshold in capi_gpu.cu)
+  int64_t lane_min_count = -1;
   int lane_warps = 8, lane_page = 0;  // the lane solve's warps per block (one group of 32 right-hand sides), page bytes
   int lane_rpl = 1;                   // right-hand sides per lane of the plain lane solve (1 or 2)
   // lane_warps not set by a caller or the autotuner: a solve of no more groups of 32 than SMs then

@@ -255,7 +255,8 @@ class GpuFactor:
         _check(lib().yb_factor_set_lane(self._h, precision, warps, page_bytes))
 
     def set_lane_min_count(self, precision: int, min_count: int) -> None:
-        """The number of right-hand sides from which the automatic choice takes the lane solve."""
+        """The number of right-hand sides from which the automatic choice takes the lane solve
+        (-1: the automatic threshold, by the factor's domain tiles)."""
         _check(lib().yb_factor_set_lane_min_count(self._h, precision, min_count))
 
     def set_refine_lane_min_count(self, min_count: int) -> None:
