@@ -120,7 +120,7 @@ int32_t yb_factor_set_lane_rhs_per_lane(yb_factor *f, int32_t precision, int32_t
  * columns, else 64 (the measured crossovers). */
 int32_t yb_factor_set_lane_min_count(yb_factor *f, int32_t precision, int64_t min_count);
 /* No ybus counterpart: the number of right-hand sides from which yb_solve_many_refined_device takes
- * the FP32 lane solve (default 5120, the measured crossover with the refinement fused into the
+ * the FP32 lane solve (default 2048, the measured crossover with the refinement fused into the
  * domain solve on the 10,000-bus B'; the FP32 lane threshold of yb_factor_set_lane_min_count applies
  * too, whichever is higher). */
 int32_t yb_factor_set_refine_lane_min_count(yb_factor *f, int64_t min_count);
@@ -400,7 +400,7 @@ int32_t yb_factor_attach_matrix(yb_factor *f, const int64_t *a_ptr, const int64_
  * the substitutions in FP32, the residual and the update x += d in FP64 against the attached A, up
  * to max_steps corrections per tile, until every column's ||r||inf / ||b||inf <= tolerance or the
  * residual stops halving. Each column keeps, as refine_normwise does, its best iterate: x, d_ratio
- * and d_steps are those of the iterate with the smallest relative residual. From 5,120 right-hand
+ * and d_steps are those of the iterate with the smallest relative residual. From 2,048 right-hand
  * sides on (yb_factor_set_refine_lane_min_count; or the FP32 lane threshold of
  * yb_factor_set_lane_min_count, if higher) the passes run on the lane solve, the stop rule applied
  * per column and the solve skipping groups of 32 columns that have all stopped, with each pass's

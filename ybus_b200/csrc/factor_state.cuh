@@ -117,8 +117,9 @@ struct TileConfig {
   // takes blocks of kLaneMaxWarps (one an SM, each warp's chain of rows shorter)
   bool lane_warps_auto = true;
   // the refined solve takes the lane solve from this many right-hand sides on (its passes cost more
-  // launches than the plain solve's, so its crossover with the fused domain refinement lies higher)
-  int64_t refine_lane_min_count = 5120;
+  // launches than the plain solve's, so its crossover with the fused domain refinement lies higher:
+  // 2,048 on the 10,000-bus B′ with blocks of 16 warps up to one wave)
+  int64_t refine_lane_min_count = 2048;
 };
 
 // A lane layout on the device (LaneLayout in plan.hpp).
