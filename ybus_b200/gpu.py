@@ -251,7 +251,7 @@ class GpuFactor:
         return dict(zip(keys, (int(a) for a in v)))
 
     def set_lane(self, precision: int, warps: int, page_bytes: int = 0) -> None:
-        """The lane solve's warps per block (1..8) and page bytes (0: the automatic choice)."""
+        """The lane solve's warps per block (1..16) and page bytes (0: the automatic choice)."""
         _check(lib().yb_factor_set_lane(self._h, precision, warps, page_bytes))
 
     def set_lane_min_count(self, precision: int, min_count: int) -> None:
