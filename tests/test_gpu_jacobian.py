@@ -89,6 +89,20 @@ def test_jacobian_transposed_solves_match_the_oracle(gpu, system):
     assert worst_relative_difference(factor.solve_many_transpose(rhs), cpu) < BAR
 
 
+def test_the_transposed_factor_takes_the_lane_solve(gpu, system):
+    # A' = Q U' L' P: U' (not unit) forward, L' backward; the joint pattern's forest orders both
+    factor = GpuFactor.from_lu_transposed(gpu, system.lu)
+    factor.set_tile_kind(FP64, LANE)
+    assert factor.lane_info(FP64)["slots"] <= 64
+    rhs = system.rhs[:512]
+    factor.time_lane(True)
+    x = factor.solve_many(rhs)
+    assert factor.lane_times()["launches"] > 0
+    factor.time_lane(False)
+    factor.check_error()
+    assert worst_relative_difference(x, orc.solve_many_lu(system.lu, rhs, threads=8, transpose=True)) < BAR
+
+
 def test_the_autotuner_finds_a_faster_solve_for_the_jacobian(gpu, system):
     # at 1,024 right-hand sides (32 lane blocks) the Jacobian's domain tiles hold one column in
     # shared memory; the autotuner also times the lane and the global-scratch solves and keeps what
